@@ -1,0 +1,199 @@
+/*
+ * mtb.h -- C ABI of the B200-native W-projection imaging path.
+ *
+ * Drop-in boundary for mt-imager's W-projection hot path.  mt-imager wires its
+ * imaging dataflow out of GAFW operators (code/gafw/Implimentation/
+ * GPUImplimentation/GPUArrayOperator.h:27-43): each operator validates its
+ * inputs (validate(ValidationData&)) and enqueues work on the engine's stream
+ * (submitToGPU(GPUSubmissionData&), GPUSubmissionData.h:27-47) with buffers the
+ * engine owns.  The entry points below cover the three modules built out of
+ * those operators, with the same ownership rules: the caller owns and
+ * allocates every input, output and workspace buffer (device pointers), the
+ * library only enqueues work on the caller's stream, and every call returns a
+ * status code instead of throwing (0 = MTB_OK).
+ *
+ *   mtb_wkernel_*   WProjectionConvFunction::calculate
+ *                   (code/mt-imager/lib/components/ConvolutionFunctionsGenerator/
+ *                    WProjectionConvFunction.cpp:186-291) and its operators
+ *                   casagridsf, WProjPreFFTConvFunc, multiFFT2D,
+ *                   ZeroToCentre2DShift, SingleMultiply, ConvFunctionSupportFind,
+ *                   ConvFunctionReOrganize, ArraysToVector, SumConvolutionFunctions.
+ *   mtb_grid        one WImager chunk (code/mt-imager/lib/components/WImager.cpp:167-234):
+ *                   PreProcessUVW, Sum / GriddedPointsCalculator statistics,
+ *                   NormalizerCalculate, AccumulatedSum, CreateIndexAndReorder,
+ *                   ValueChangeDetect, CreateBlockDataIndex, NotSameSupportManipulate,
+ *                   CreateCompressionPlan, CompressVisibilities, ConvolutionGridder.
+ *   mtb_finalize    ImageFinalizer (code/mt-imager/lib/components/ImageFinalizer.cpp:31-44):
+ *                   PreIFFTUVCorrection, IFFT2D, ZeroToCentre2DShift, StokesConverter,
+ *                   casagridsf (lmPlanePostCorrection), SincCorrector.
+ *
+ * Array layouts are mt-imager's (dimensions slowest first, ArrayDimensions.h:62-83):
+ *   uvw        float   [3][R]        u, v, w rows in metres
+ *   freq       float   [R]           nu / c per record
+ *   vis        float2  [R][P]        pol-interleaved complex (XX, XY, YX, YY)
+ *   weights    float   [R][P]
+ *   flags      int     [R][P]        non-zero = flagged
+ *   table      float2  [sum_k T^2 S_k^2]  per plane [oy][ox][sy][sx], T = s (s odd) or s+1
+ *   conv_info  int     [wplanes][2]  {support, first element of the plane in table}
+ *   conv_sums  float   [wplanes][T*T]
+ *   grid       float2  [ny][nx][P]   (v rows, u columns, pol fastest), accumulated
+ *   normalizer float   [P]           accumulated
+ *   image      float   [P][ny][nx]   Stokes planes, row 0 = top of the FITS image
+ */
+#ifndef MTB_H
+#define MTB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* cudaStream_t without pulling in the CUDA headers */
+typedef struct CUstream_st *mtb_stream_t;
+
+/* Status codes; mirror the exception classes the reference throws
+ * (ValidationException, CudaException, FFTException, ImagerException:
+ * code/gafw/Implimentation/GPUImplimentation/GPUafw.h:28-33). */
+enum {
+    MTB_OK = 0,
+    MTB_ERR_BAD_PARAM = 1,     /* ValidationException: a parameter is out of range   */
+    MTB_ERR_BAD_SHAPE = 2,     /* ValidationException: sizes / pol count unsupported */
+    MTB_ERR_WORKSPACE = 3,     /* workspace smaller than the query said              */
+    MTB_ERR_CAPACITY = 4,      /* output buffer smaller than needed                  */
+    MTB_ERR_CUDA = 5,          /* CudaException                                      */
+    MTB_ERR_CUFFT = 6,         /* FFTException                                       */
+    MTB_ERR_KERNEL = 7,        /* ImagerException: w=0 origin not real / no support  */
+    MTB_ERR_NULL = 8           /* a required pointer is NULL                         */
+};
+
+/* ------------------------------------------------------------ w-kernels -- */
+typedef struct mtb_wkernel_params {
+    int nx, ny;              /* image.nx, image.ny (pixels)                            */
+    double l_increment;      /* image.lintervalsize in radians                         */
+    double m_increment;      /* image.mintervalsize in radians                         */
+    int wplanes;             /* wproj.wplanes                                          */
+    int sampling;            /* wproj.convFunction.sampling                            */
+    int trial_support;       /* 0: min(nx,ny)/sampling forced odd
+                                (WProjectionConvFunction.cpp:194-198)                  */
+    int max_support;         /* 0: trial_support-2 (WProjectionConvFunction.cpp:248)    */
+    double w_max;            /* 0: 0.25/l_increment (WProjectionConvFunction.cpp:105)  */
+} mtb_wkernel_params;
+
+typedef struct mtb_wkernel_info {
+    int trial_support;       /* odd S_t                                                */
+    int planesize;           /* S_t * sampling                                         */
+    int support_cap;         /* largest support a plane may get                        */
+    int T;                   /* oversampling offsets per axis (s or s+1)               */
+    double w_max;
+    double w_sq_increment;   /* w_k = k^2 * w_sq_increment (WProjectionConvFunction.cpp:112,238) */
+    double total_l, total_m; /* field size in radians (ConfigurationManager.cpp:190)   */
+    double u_increment, v_increment; /* 1/(dl*nx), 1/(dm*ny) (ConfigurationManager.cpp:177-178) */
+    size_t table_capacity;   /* float2 elements that always suffice for the table      */
+    size_t workspace_bytes;  /* workspace mtb_wkernel_build needs                      */
+} mtb_wkernel_info;
+
+/* Host-only: derived scalars and buffer sizes.  Replaces the parameter logic
+ * of WProjectionConvFunction's constructor (WProjectionConvFunction.cpp:90-160). */
+int mtb_wkernel_query(const mtb_wkernel_params *p, mtb_wkernel_info *info);
+
+/* Builds every w-plane kernel in one pass (all planes batched through cuFFT Z2Z,
+ * FP64 w-phase) into the reference's AmalgamatedConvFunction / convInfo /
+ * ConvSums outputs.  Replaces WProjectionConvFunction::calculate
+ * (WProjectionConvFunction.cpp:186-291).  Synchronises `stream` once, to bring
+ * the per-plane supports to the host (the reference does so once per plane,
+ * WPlaneConvFunctionCalculator.cpp:117-126).
+ *   d_table       out float2 [table_capacity]
+ *   d_conv_info   out int [wplanes][2] (device; may be NULL)
+ *   h_conv_info   out int [wplanes][2] (host; required)
+ *   d_conv_sums   out float [wplanes][T*T]
+ *   table_elems   out: float2 elements written */
+int mtb_wkernel_build(const mtb_wkernel_params *p, void *d_workspace, size_t workspace_bytes,
+                      void *d_table, size_t table_capacity, int *d_conv_info, int *h_conv_info,
+                      float *d_conv_sums, size_t *table_elems, mtb_stream_t stream);
+
+/* ------------------------------------------------------------- gridding -- */
+typedef struct mtb_grid_params {
+    int nx, ny;              /* uvImage.columns, uvImage.rows                          */
+    int npol;                /* 1, 2 or 4                                              */
+    int sampling;            /* ConvolutionFunction.sampling                           */
+    int wplanes;
+    double u_increment;      /* uvImage.u_increment                                    */
+    double v_increment;      /* uvImage.v_increment                                    */
+    double w_sq_increment;   /* ConvolutionFunction.wsquareincrement                   */
+    int initialize_output;   /* zero grid, grid_lo and normalizer first (ConvolutionGridder.cu:496-502) */
+    int tile;                /* 0: default; grid tile edge owned by one thread block   */
+    int support_bucket;      /* 0: default; supports are grouped in buckets this wide  */
+    int max_chunk;           /* 0: default; most records one block grids in one pass   */
+} mtb_grid_params;
+
+typedef struct mtb_grid_stats {
+    unsigned long long gridded_records;     /* Statistic:TotalGriddedRecords    (WImager.cpp:173) */
+    unsigned long long compressed_records;  /* Statistic:TotalCompressedRecords (WImager.cpp:174) */
+    unsigned long long gridded_points;      /* Statistic:TotalGriddedPoints     (WImager.cpp:175) */
+    unsigned long long compressed_points;   /* Statistic:TotalCompressedPoints  (WImager.cpp:176) */
+} mtb_grid_stats;
+
+/* Workspace for one mtb_grid call over `nrecords` records. */
+int mtb_grid_workspace_size(const mtb_grid_params *p, int nrecords, size_t *bytes);
+
+/* Grids one chunk of records into the accumulating grid: one WImager::calculate
+ * (WImager.cpp:271-290).  FP64 coordinates; FP32 tile accumulation in shared
+ * memory; each tile merged into the grid once.  With d_grid_lo non-NULL the merge
+ * is compensated: d_grid + d_grid_lo carries the running sum to about twice
+ * FP32 precision (pass the same d_grid_lo to mtb_finalize).  d_stats (device
+ * memory, may be NULL) accumulates the four record statistics.
+ *   h_conv_info   host int [wplanes][2] as returned by mtb_wkernel_build */
+int mtb_grid(const mtb_grid_params *p, const void *d_table, const int *d_conv_info,
+             const int *h_conv_info, const float *d_conv_sums,
+             const float *d_uvw, const float *d_freq, const void *d_vis, const float *d_weights,
+             const int *d_flags, int nrecords,
+             void *d_grid, void *d_grid_lo, float *d_normalizer, mtb_grid_stats *d_stats,
+             void *d_workspace, size_t workspace_bytes, mtb_stream_t stream);
+
+/* The PreProcessUVW operator alone, with its seven outputs in the reference's
+ * layout (code/mt-imager/lib/operators/WProjPreProcessUVW.cpp:66-85,
+ * WProjPreProcessUVW.cu:112-324), FP64 coordinates.  Workspace: as for
+ * mtb_grid with the same record count.
+ *   d_gridding_data   int [R][4] {cx, cy*nx+cx, -(cx%S), -(cy%S)}
+ *   d_conv_index      int [R]    first table element of the record's sub-kernel
+ *   d_to_grid         int [R]    1 = grid (after duplicate compression)
+ *   d_to_compress     int [R]    1 = merged into the previous record
+ *   d_support         int [R]
+ *   d_take_conjugate  float [R]  -1 when w < 0 (u, v negated, imaginary part negated)
+ *   d_conv_sum        float [P][R] ConvSums * weight * (1 - flag) */
+int mtb_preprocess_uvw(const mtb_grid_params *p, const int *d_conv_info, const int *h_conv_info,
+                       const float *d_conv_sums, const float *d_uvw, const float *d_freq,
+                       const float *d_weights, const int *d_flags, int nrecords, int *d_gridding_data,
+                       int *d_conv_index, int *d_to_grid, int *d_to_compress, int *d_support,
+                       float *d_take_conjugate, float *d_conv_sum, void *d_workspace,
+                       size_t workspace_bytes, mtb_stream_t stream);
+
+/* ------------------------------------------------------------- finalize -- */
+enum { MTB_POL_LINEAR = 0, MTB_POL_CIRCULAR = 1 };  /* PolarizationType (mtimager.h:30-37) */
+
+typedef struct mtb_finalize_params {
+    int nx, ny, npol;
+    int sampling;            /* SincCorrector "sampling" = wproj.convFunction.sampling */
+    int pol_type;            /* MTB_POL_LINEAR or MTB_POL_CIRCULAR                     */
+} mtb_finalize_params;
+
+int mtb_finalize_workspace_size(const mtb_finalize_params *p, size_t *bytes);
+
+/* Grid (+ optional compensation term) and normaliser to the corrected Stokes
+ * cube: ImageFinalizer::calculate (ImageFinalizer.cpp:60-65). */
+int mtb_finalize(const mtb_finalize_params *p, const void *d_grid, const void *d_grid_lo,
+                 const float *d_normalizer, float *d_image, void *d_workspace,
+                 size_t workspace_bytes, mtb_stream_t stream);
+
+/* ---------------------------------------------------------------- misc -- */
+const char *mtb_status_string(int status);
+int mtb_version(void);
+/* Releases cached cuFFT plans (plans are created on first use per shape). */
+void mtb_release_caches(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MTB_H */

@@ -1,0 +1,797 @@
+// Visibility preprocessing, binning and tile gridding for sm_100a.
+//
+// One mtb_grid call is one WImager chunk (code/mt-imager/lib/components/
+// WImager.cpp:167-234).  The reference runs ~14 operators per chunk:
+// PreProcessUVW, four statistics reductions, the normaliser sum, three
+// exclusive scans with compaction / run detection to build a plan of <=440
+// record runs of equal support, duplicate compression, and the Romein gridder
+// that flushes every cell change with float atomics into the global grid
+// (ConvolutionGridder.cu:325-444).
+//
+// Here:
+//   k_preprocess   one pass over the records in FP64: w-plane, grid corner,
+//                  oversampling offset, conv index, normaliser sums (FP64)
+//                  (WProjPreProcessUVW.cu:112-286 semantics).
+//   k_compress     duplicate detection exactly as the reference decides it
+//                  (WProjPreProcessUVW.cu:265-324), statistics, and the bin key
+//                  (support bucket, tile row, tile column) of every gridded record.
+//   CUB            stable radix sort of the keys (original order kept inside a
+//                  bin, so consecutive records of a baseline stay consecutive),
+//                  run-length encoding and a scan to cut bins into work items.
+//   k_gather       weighted, conjugation-corrected visibility of each gridded
+//                  record summed over its compressed duplicates
+//                  (CompressVisibilties.cu:41-74), stored in bin order.
+//   k_grid         persistent kernel per support bucket: each block takes work
+//                  items from a queue; a work item is up to max_chunk records of
+//                  one bin.  Threads own support-box positions (Romein's
+//                  assignment: cell x belongs to the thread with a == x mod M),
+//                  accumulate in registers while their cell is unchanged and
+//                  flush cell changes into a shared-memory tile window, which is
+//                  merged into the global grid once per work item with
+//                  compensated (two-float) vector atomics.  No global atomic per
+//                  sample.
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "mtb_internal.cuh"
+
+namespace mtb {
+
+static const unsigned kNoKey = 0xFFFFFFFFu;
+static const int kMaxBuckets = 128;
+static const int kStage = 64;          // records staged in shared memory per pass
+static const int kDefaultTile = 32;
+static const int kDefaultChunk = 2048;
+static const size_t kWindowSmemLimit = 200 * 1024;
+
+struct BucketTable {
+    int n;                       // number of buckets in use
+    int half;                    // odd supports per bucket
+    int M[kMaxBuckets];          // modulus (largest support) of each bucket, 0 = empty
+    int tile[kMaxBuckets];       // grid tile edge used for the bucket's keys
+};
+
+__device__ __forceinline__ int bucket_of(int S, int half) { return (S - 1) / (2 * half); }
+
+// ------------------------------------------------------------- preprocess --
+template <int P>
+__global__ void k_preprocess(int R, const float *__restrict__ uvw, const float *__restrict__ freq,
+                             const float *__restrict__ weights, const int *__restrict__ flags,
+                             const int *__restrict__ conv_info, const float *__restrict__ conv_sums,
+                             int nw, double w_inc, int s, int T, int nx, int ny, double du, double dv,
+                             int4 *__restrict__ pos, int *__restrict__ meta, double *__restrict__ norm_acc,
+                             float *__restrict__ convsum_out) {
+    double nsum[P];
+#pragma unroll
+    for (int p = 0; p < P; p++) nsum[p] = 0.0;
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < R; r += gridDim.x * blockDim.x) {
+        int fl[P];
+        float wt[P];
+        bool grid = false;
+#pragma unroll
+        for (int p = 0; p < P; p++) {
+            fl[p] = flags[(size_t)r * P + p];
+            wt[p] = weights[(size_t)r * P + p];
+            if (fl[p] == 0) grid = true;
+        }
+        int4 out = make_int4(0, 0, 0, 0);
+        int m = 0;
+        double cs = 0.0;
+        if (grid) {
+            double u = (double)uvw[r], v = (double)uvw[(size_t)R + r], w = (double)uvw[2 * (size_t)R + r];
+            double f = (double)freq[r];
+            bool neg = false;
+            if (w < 0.0) { u = -u; v = -v; neg = true; }
+            // WProjPreProcessUVW.cu:181-182
+            double wp = round(sqrt(fabs(__ddiv_rn(__dmul_rn(w, f), w_inc))));
+            if (!(wp == wp)) wp = 0.0;
+            int k = (wp > (double)(nw - 1)) ? nw - 1 : (int)wp;
+            int S = conv_info[2 * k];
+            int ci = conv_info[2 * k + 1];
+            // WProjPreProcessUVW.cu:188-199
+            double pos_v = __dadd_rn(__ddiv_rn(__dmul_rn(v, f), dv), (double)(ny / 2));
+            double pos_u = __dadd_rn(__ddiv_rn(__dmul_rn(u, f), du), (double)(nx / 2));
+            double lx = round(pos_u), ly = round(pos_v);
+            double cxd = lx - (double)(S / 2), cyd = ly - (double)(S / 2);
+            if (!(cyd >= 0.0) || cyd > (double)((ny - 1) - S) || !(cxd >= 0.0) || cxd > (double)(nx - 1 - S)) {
+                grid = false;
+            } else {
+                int cx = (int)cxd, cy = (int)cyd;
+                // WProjPreProcessUVW.cu:206-239
+                int ox = (int)round(__dmul_rn(__dadd_rn(lx, -pos_u), (double)s)) + s / 2;
+                int oy = (int)round(__dmul_rn(__dadd_rn(ly, -pos_v), (double)s)) + s / 2;
+                if (s & 1) {
+                    ox = ox < 0 ? 0 : (ox == s ? s - 1 : ox);
+                    oy = oy < 0 ? 0 : (oy == s ? s - 1 : oy);
+                }
+                cs = (double)conv_sums[(size_t)k * T * T + oy * T + ox];
+                ci += oy * S * S * T + ox * S * S;
+                out = make_int4(cx, cy, ci, S);
+                m = 1 | (neg ? 2 : 0);
+            }
+        }
+        pos[r] = out;
+        meta[r] = m;
+#pragma unroll
+        for (int p = 0; p < P; p++) {
+            double c = grid ? cs * (double)wt[p] * (1.0 - (double)fl[p]) : 0.0;
+            nsum[p] += c;
+            if (convsum_out) convsum_out[(size_t)p * R + r] = (float)c;
+        }
+    }
+    // normaliser: NormalizerCalculate = Sum over records (WImager.cpp:196-197)
+#pragma unroll
+    for (int p = 0; p < P; p++) {
+        double v = nsum[p];
+        for (int off = 16; off; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+        __shared__ double red[P][32];
+        if ((threadIdx.x & 31) == 0) red[p][threadIdx.x >> 5] = v;
+        __syncthreads();
+        if (threadIdx.x < 32) {
+            double t = (threadIdx.x < (blockDim.x >> 5)) ? red[p][threadIdx.x] : 0.0;
+            for (int off = 16; off; off >>= 1) t += __shfl_down_sync(0xffffffffu, t, off);
+            if (threadIdx.x == 0 && t != 0.0) atomicAdd(&norm_acc[p], t);
+        }
+        __syncthreads();
+    }
+}
+
+// Duplicate compression (a record whose corner row-index and conv index equal
+// the previous record's stored values is merged into it; a non-gridded
+// previous record stores zeros: WProjPreProcessUVW.cu:243-284, 316), the four
+// record statistics, and the bin key of every record left to grid.
+__global__ void k_compress(int R, int nx, const int4 *__restrict__ pos, int *__restrict__ meta,
+                           unsigned *__restrict__ keys, int *__restrict__ iota, BucketTable bt,
+                           unsigned long long *__restrict__ stats) {
+    unsigned long long st[4] = {0, 0, 0, 0};
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < R; r += gridDim.x * blockDim.x) {
+        int m = meta[r];
+        int4 q = pos[r];
+        bool comp = false;
+        if ((m & 1) && r > 0) {
+            int4 pq = pos[r - 1];   // zeros when the previous record is not gridded
+            comp = (q.z == pq.z) && (q.y * nx + q.x == pq.y * nx + pq.x);
+        }
+        unsigned key = kNoKey;
+        unsigned long long s2 = (unsigned long long)q.w * (unsigned long long)q.w;
+        if (comp) {
+            meta[r] = m | 4;
+            st[1] += 1;
+            st[3] += s2;
+        } else if (m & 1) {
+            int b = bucket_of(q.w, bt.half);
+            int t = bt.tile[b];
+            key = ((unsigned)b << 24) | ((unsigned)(q.y / t) << 12) | (unsigned)(q.x / t);
+            st[0] += 1;
+            st[2] += s2;
+        }
+        keys[r] = key;
+        iota[r] = r;
+    }
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        unsigned long long v = st[i];
+        for (int off = 16; off; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+        if ((threadIdx.x & 31) == 0 && v) atomicAdd(&stats[i], v);
+    }
+}
+
+// Per bin-run: number of work items (bins of the kNoKey run give none).
+__global__ void k_chunk_counts(const unsigned *__restrict__ ukeys, const int *__restrict__ counts,
+                               const int *__restrict__ num_runs, int cap, int chunk, int *__restrict__ nchunks) {
+    int n = *num_runs;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < cap; i += gridDim.x * blockDim.x) {
+        int c = 0;
+        if (i < n && ukeys[i] != kNoKey) c = (counts[i] + chunk - 1) / chunk;
+        nchunks[i] = c;
+    }
+}
+
+// Work items: {first record (bin order), record count, bin key}.
+__global__ void k_make_items(const unsigned *__restrict__ ukeys, const int *__restrict__ counts,
+                             const int *__restrict__ run_start, const int *__restrict__ item_start,
+                             const int *__restrict__ nchunks, const int *__restrict__ num_runs, int chunk,
+                             int4 *__restrict__ items) {
+    int n = *num_runs;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        int c = nchunks[i];
+        int base = item_start[i], s0 = run_start[i], cnt = counts[i];
+        for (int j = 0; j < c; j++) {
+            int a = s0 + j * chunk;
+            int len = min(chunk, s0 + cnt - a);
+            items[base + j] = make_int4(a, len, (int)ukeys[i], 0);
+        }
+    }
+}
+
+// Per bucket [begin, end) of the item list and the total item count.
+__global__ void k_bucket_bounds(const int4 *__restrict__ items, const int *__restrict__ item_start,
+                                const int *__restrict__ nchunks, const int *__restrict__ num_runs,
+                                int *__restrict__ bounds, int nb) {
+    int nr = *num_runs;
+    int total = nr > 0 ? item_start[nr - 1] + nchunks[nr - 1] : 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+        int b = (int)((unsigned)items[i].z >> 24);
+        int bp = i > 0 ? (int)((unsigned)items[i - 1].z >> 24) : -1;
+        int bn = i + 1 < total ? (int)((unsigned)items[i + 1].z >> 24) : -1;
+        if (b != bp) bounds[2 * b] = i;
+        if (b != bn) bounds[2 * b + 1] = i + 1;
+    }
+}
+
+// Gridded records in bin order: {cx, cy, conv index, support} and the
+// weighted, conjugation-corrected visibility summed over the run of records
+// compressed into it (CreateCompressionPlan.cu:32-67, CompressVisibilties.cu:41-74,
+// common.hcu:94-104).
+template <int P>
+__global__ void k_gather(int R, const unsigned *__restrict__ skeys, const int *__restrict__ sidx,
+                         const int4 *__restrict__ pos, const int *__restrict__ meta,
+                         const float2 *__restrict__ vis, const float *__restrict__ weights,
+                         const int *__restrict__ flags, int4 *__restrict__ wpos, float2 *__restrict__ wvis) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < R; i += gridDim.x * blockDim.x) {
+        if (skeys[i] == kNoKey) continue;
+        int g = sidx[i];
+        float2 acc[P];
+#pragma unroll
+        for (int p = 0; p < P; p++) acc[p] = make_float2(0.f, 0.f);
+        int r = g;
+        do {
+            int m = meta[r];
+            float im = (m & 2) ? -1.0f : 1.0f;
+#pragma unroll
+            for (int p = 0; p < P; p++) {
+                float2 v = vis[(size_t)r * P + p];
+                float wgt = weights[(size_t)r * P + p];
+                float keep = 1.0f - (float)flags[(size_t)r * P + p];
+                acc[p].x += v.x * wgt * keep;
+                acc[p].y += v.y * wgt * keep * im;
+            }
+            r++;
+        } while (r < R && (meta[r] & 4));
+        wpos[i] = pos[g];
+#pragma unroll
+        for (int p = 0; p < P; p++) wvis[(size_t)i * P + p] = acc[p];
+    }
+}
+
+__global__ void k_finish(int P, const double *__restrict__ norm_acc, float *__restrict__ normalizer,
+                         const unsigned long long *__restrict__ st, mtb_grid_stats *__restrict__ out) {
+    int t = threadIdx.x;
+    if (t < P) normalizer[t] += (float)norm_acc[t];
+    if (out && t == 0) {
+        out->gridded_records += st[0];
+        out->compressed_records += st[1];
+        out->gridded_points += st[2];
+        out->compressed_points += st[3];
+    }
+}
+
+// ---------------------------------------------------------------- gridder --
+struct GridArgs {
+    const int4 *items;
+    const int *bounds;          // [bucket][2]
+    int *counters;              // per bucket work counter
+    const int4 *wpos;
+    const float2 *wvis;
+    const float2 *table;
+    float *grid;                // float2 [ny][nx][P] as floats
+    float *grid_lo;             // may be null
+    int nx, ny;
+    int bucket, M, rows, nbands, tile, W;
+};
+
+// Two-float merge: hi += t with the rounding error of that add accumulated in lo.
+__device__ __forceinline__ void merge4(float *hi, float *lo, float4 t) {
+    if (lo) {
+        float4 old = atomicAdd((float4 *)hi, t);
+        float4 e;
+        float s, bp;
+        s = old.x + t.x; bp = s - old.x; e.x = (old.x - (s - bp)) + (t.x - bp);
+        s = old.y + t.y; bp = s - old.y; e.y = (old.y - (s - bp)) + (t.y - bp);
+        s = old.z + t.z; bp = s - old.z; e.z = (old.z - (s - bp)) + (t.z - bp);
+        s = old.w + t.w; bp = s - old.w; e.w = (old.w - (s - bp)) + (t.w - bp);
+        atomicAdd((float4 *)lo, e);
+    } else {
+        atomicAdd((float4 *)hi, t);
+    }
+}
+__device__ __forceinline__ void merge2(float *hi, float *lo, float2 t) {
+    if (lo) {
+        float2 old = atomicAdd((float2 *)hi, t);
+        float2 e;
+        float s, bp;
+        s = old.x + t.x; bp = s - old.x; e.x = (old.x - (s - bp)) + (t.x - bp);
+        s = old.y + t.y; bp = s - old.y; e.y = (old.y - (s - bp)) + (t.y - bp);
+        atomicAdd((float2 *)lo, e);
+    } else {
+        atomicAdd((float2 *)hi, t);
+    }
+}
+
+template <int P>
+__device__ __forceinline__ void merge_cell(float *hi, float *lo, const float *v) {
+    if (P == 1) {
+        merge2(hi, lo, make_float2(v[0], v[1]));
+    } else {
+#pragma unroll
+        for (int q = 0; q < 2 * P; q += 4) merge4(hi + q, lo ? lo + q : nullptr, make_float4(v[q], v[q + 1], v[q + 2], v[q + 3]));
+    }
+}
+
+// WINDOW: cell flushes go to the shared-memory window of the work item's
+// tile, merged into the grid at the end of the item.  !WINDOW (supports too
+// large for a window): flushes go straight to the grid.
+template <int P, int KMAX, bool WINDOW>
+__global__ void __launch_bounds__(KMAX >= 8 ? 576 : 1024) k_grid(GridArgs a) {
+    extern __shared__ float4 smem4[];
+    const int M = a.M, rows = a.rows, W = a.W;
+    const int nthreads = M * rows;
+    const int t = threadIdx.x;
+    float *win = (float *)smem4;
+    // padded to 16 bytes so the staging area after it stays int4-aligned
+    const size_t win_floats = WINDOW ? (((size_t)W * W * 2 * P + 3) & ~(size_t)3) : 0;
+    int4 *s_rec = (int4 *)(win + win_floats);                 // {base, (rxm | rym<<16), conv, S}
+    float *s_vis = (float *)(s_rec + kStage);                  // [kStage][2P]
+    __shared__ int s_item;
+
+    const int ta = t % M, tr = t / M;
+    const bool live = t < nthreads;
+    const int stride = WINDOW ? W : a.nx;
+
+    if (WINDOW) {
+        for (size_t i = t; i < (size_t)W * W * 2 * P; i += blockDim.x) win[i] = 0.f;
+    }
+    const int begin = a.bounds[2 * a.bucket], end = a.bounds[2 * a.bucket + 1];
+    const int nvirt = (end - begin) * a.nbands;
+
+    for (;;) {
+        __syncthreads();
+        if (t == 0) s_item = atomicAdd(&a.counters[a.bucket], 1);
+        __syncthreads();
+        const int v = s_item;
+        if (v >= nvirt) break;
+        const int item = begin + v / a.nbands, band = v % a.nbands;
+        const int4 it = a.items[item];
+        const unsigned key = (unsigned)it.z;
+        const int wx0 = (int)(key & 0xFFFu) * a.tile, wy0 = (int)((key >> 12) & 0xFFFu) * a.tile;
+        const int b0 = band * rows * KMAX + tr;               // first slot row of this thread
+
+        float acc[KMAX][2 * P];
+        int last[KMAX];
+#pragma unroll
+        for (int j = 0; j < KMAX; j++) {
+            last[j] = -1;
+#pragma unroll
+            for (int c = 0; c < 2 * P; c++) acc[j][c] = 0.f;
+        }
+
+        for (int r0 = 0; r0 < it.y; r0 += kStage) {
+            const int nrec = min(kStage, it.y - r0);
+            __syncthreads();
+            for (int i = t; i < nrec; i += blockDim.x) {
+                int4 p = a.wpos[it.x + r0 + i];
+                int rx = p.x - wx0, ry = p.y - wy0;
+                int rxm = (M - rx % M) % M, rym = (M - ry % M) % M;
+                int base = WINDOW ? ry * W + rx : (p.y * a.nx + p.x);
+                s_rec[i] = make_int4(base, rxm | (rym << 16), p.z, p.w);
+            }
+            for (int i = t; i < nrec * P; i += blockDim.x) {
+                float2 vv = a.wvis[(size_t)(it.x + r0) * P + i];
+                s_vis[2 * i] = vv.x;
+                s_vis[2 * i + 1] = vv.y;
+            }
+            __syncthreads();
+            if (!live) continue;
+            for (int i = 0; i < nrec; i++) {
+                const int4 rec = s_rec[i];
+                const int S = rec.w;
+                int sx = ta + (rec.y & 0xFFFF);
+                if (sx >= M) sx -= M;
+                if (sx >= S) continue;
+                int sy = b0 + (rec.y >> 16);
+                if (sy >= M) sy -= M;
+                float vr[P], vi[P];
+#pragma unroll
+                for (int p = 0; p < P; p++) {
+                    vr[p] = s_vis[i * 2 * P + 2 * p];
+                    vi[p] = s_vis[i * 2 * P + 2 * p + 1];
+                }
+                const int cbase = rec.x + sx, tbase = rec.z + sx;
+#pragma unroll
+                for (int j = 0; j < KMAX; j++) {
+                    const int b = b0 + j * rows;
+                    if (b < M && sy < S) {
+                        const int cell = cbase + sy * stride;
+                        const float2 cw = __ldg(&a.table[tbase + sy * S]);
+                        if (cell != last[j]) {
+                            if (last[j] >= 0) {
+                                if (WINDOW) {
+                                    float *wc = win + (size_t)last[j] * 2 * P;
+#pragma unroll
+                                    for (int c = 0; c < 2 * P; c++) wc[c] += acc[j][c];
+                                } else {
+                                    merge_cell<P>(a.grid + (size_t)last[j] * 2 * P,
+                                                  a.grid_lo ? a.grid_lo + (size_t)last[j] * 2 * P : nullptr, acc[j]);
+                                }
+                            }
+                            last[j] = cell;
+#pragma unroll
+                            for (int c = 0; c < 2 * P; c++) acc[j][c] = 0.f;
+                        }
+                        // ConvolutionGridder.cu:153-181: to += vis * wt (no conjugate)
+#pragma unroll
+                        for (int p = 0; p < P; p++) {
+                            acc[j][2 * p] += vr[p] * cw.x;
+                            acc[j][2 * p + 1] += vi[p] * cw.x;
+                            acc[j][2 * p] -= vi[p] * cw.y;
+                            acc[j][2 * p + 1] += vr[p] * cw.y;
+                        }
+                    }
+                    sy += rows;
+                    if (sy >= M) sy -= M;
+                }
+            }
+        }
+        // register flush
+        if (live) {
+#pragma unroll
+            for (int j = 0; j < KMAX; j++) {
+                if (last[j] >= 0) {
+                    if (WINDOW) {
+                        float *wc = win + (size_t)last[j] * 2 * P;
+#pragma unroll
+                        for (int c = 0; c < 2 * P; c++) wc[c] += acc[j][c];
+                    } else {
+                        merge_cell<P>(a.grid + (size_t)last[j] * 2 * P,
+                                      a.grid_lo ? a.grid_lo + (size_t)last[j] * 2 * P : nullptr, acc[j]);
+                    }
+                }
+            }
+        }
+        if (WINDOW) {
+            __syncthreads();
+            // one merge of the tile window into the grid; cells left at zero are skipped
+            for (int c = t; c < W * W; c += blockDim.x) {
+                float *wc = win + (size_t)c * 2 * P;
+                float vals[2 * P];
+                bool nz = false;
+#pragma unroll
+                for (int q = 0; q < 2 * P; q++) {
+                    vals[q] = wc[q];
+                    nz |= (vals[q] != 0.f);
+                    wc[q] = 0.f;
+                }
+                if (!nz) continue;
+                int y = wy0 + c / W, x = wx0 + c % W;
+                if (y >= a.ny || x >= a.nx) continue;
+                size_t g = ((size_t)y * a.nx + x) * 2 * P;
+                merge_cell<P>(a.grid + g, a.grid_lo ? a.grid_lo + g : nullptr, vals);
+            }
+        }
+    }
+}
+
+// ------------------------------------------------------------ host side --
+struct GridPlan {
+    BucketTable bt;
+    int chunk;
+    int ncap;      // record capacity of per-record arrays
+};
+
+struct GridSpace {
+    int4 *pos;
+    int *meta;
+    unsigned *keys, *skeys;
+    int *iota, *sidx;
+    unsigned *ukeys;
+    int *counts, *run_start, *nchunks, *item_start, *num_runs;
+    int4 *items;
+    int *bounds, *counters;
+    int4 *wpos;
+    float2 *wvis;
+    double *norm_acc;
+    unsigned long long *stats;
+    void *cub;
+    size_t cub_bytes;
+};
+
+static size_t cub_bytes(int n) {
+    size_t a = 0, b = 0, c = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, a, (unsigned *)nullptr, (unsigned *)nullptr, (int *)nullptr,
+                                    (int *)nullptr, n);
+    cub::DeviceRunLengthEncode::Encode(nullptr, b, (unsigned *)nullptr, (unsigned *)nullptr, (int *)nullptr,
+                                       (int *)nullptr, n);
+    cub::DeviceScan::ExclusiveSum(nullptr, c, (int *)nullptr, (int *)nullptr, n);
+    return std::max(a, std::max(b, c));
+}
+
+static void carve_grid(Arena &A, int R, int P, int chunk, GridSpace *s) {
+    size_t n = (size_t)(R > 0 ? R : 1);
+    size_t nitems = n + n / (size_t)chunk + 2;
+    s->pos = A.take<int4>(n);
+    s->meta = A.take<int>(n);
+    s->keys = A.take<unsigned>(n);
+    s->skeys = A.take<unsigned>(n);
+    s->iota = A.take<int>(n);
+    s->sidx = A.take<int>(n);
+    s->ukeys = A.take<unsigned>(n);
+    s->counts = A.take<int>(n);
+    s->run_start = A.take<int>(n);
+    s->nchunks = A.take<int>(n);
+    s->item_start = A.take<int>(n);
+    s->num_runs = A.take<int>(1);
+    s->items = A.take<int4>(nitems);
+    s->bounds = A.take<int>(2 * kMaxBuckets);
+    s->counters = A.take<int>(kMaxBuckets);
+    s->wpos = A.take<int4>(n);
+    s->wvis = A.take<float2>(n * P);
+    s->norm_acc = A.take<double>(4);
+    s->stats = A.take<unsigned long long>(4);
+    s->cub_bytes = cub_bytes((int)n);
+    s->cub = A.take<char>(s->cub_bytes);
+}
+
+static int check_params(const mtb_grid_params *p) {
+    if (!p) return MTB_ERR_NULL;
+    if (p->npol != 1 && p->npol != 2 && p->npol != 4) return MTB_ERR_BAD_SHAPE;
+    if (p->nx < 2 || p->ny < 2 || p->sampling < 1 || p->wplanes < 1) return MTB_ERR_BAD_PARAM;
+    if ((size_t)p->nx * p->ny > ((size_t)1 << 31)) return MTB_ERR_BAD_SHAPE;
+    if (!(p->u_increment > 0.0) || !(p->v_increment > 0.0) || !(p->w_sq_increment > 0.0)) return MTB_ERR_BAD_PARAM;
+    if (p->tile < 0 || p->support_bucket < 0 || p->max_chunk < 0) return MTB_ERR_BAD_PARAM;
+    return MTB_OK;
+}
+
+static int make_plan(const mtb_grid_params *p, const int *h_conv_info, GridPlan *g) {
+    int half = p->support_bucket > 0 ? p->support_bucket : 1;
+    int tile = p->tile > 0 ? p->tile : kDefaultTile;
+    g->chunk = p->max_chunk > 0 ? p->max_chunk : kDefaultChunk;
+    if (tile < 4 || p->nx / tile >= 4096 || p->ny / tile >= 4096) return MTB_ERR_BAD_PARAM;
+    std::memset(&g->bt, 0, sizeof(g->bt));
+    g->bt.half = half;
+    for (int k = 0; k < p->wplanes; k++) {
+        int S = h_conv_info[2 * k];
+        if (S < 1 || S % 2 == 0 || S > 4095 || S >= p->nx || S >= p->ny) return MTB_ERR_KERNEL;
+        int b = (S - 1) / (2 * half);
+        if (b >= kMaxBuckets) return MTB_ERR_BAD_PARAM;
+        g->bt.M[b] = std::max(g->bt.M[b], S);
+        g->bt.n = std::max(g->bt.n, b + 1);
+    }
+    for (int b = 0; b < kMaxBuckets; b++) g->bt.tile[b] = tile;
+    return MTB_OK;
+}
+
+struct Launch {
+    int kmax, rows, nbands, threads;
+    bool window;
+    size_t smem;
+};
+
+static Launch launch_shape(int M, int P, int tile) {
+    Launch L;
+    if (M <= 16) L.kmax = 1;
+    else if (M <= 32) L.kmax = 2;
+    else L.kmax = 8;
+    int rows = (M + L.kmax - 1) / L.kmax;
+    int maxrows = std::max(1, (L.kmax == 8 ? 576 : 1024) / M);
+    L.rows = std::min(rows, maxrows);
+    L.nbands = (M + L.rows * L.kmax - 1) / (L.rows * L.kmax);
+    L.threads = M * L.rows;
+    size_t stage = kStage * (sizeof(int4) + 2 * P * sizeof(float));
+    size_t W = (size_t)tile + M - 1;
+    size_t wbytes = ((W * W * 2 * P + 3) & ~(size_t)3) * sizeof(float);
+    L.window = (L.nbands == 1) && (wbytes + stage <= kWindowSmemLimit);
+    L.smem = (L.window ? wbytes : 0) + stage;
+    return L;
+}
+
+template <int P, int KMAX, bool WIN>
+static int launch_one(const GridArgs &a, const Launch &L, cudaStream_t st) {
+    auto kern = k_grid<P, KMAX, WIN>;
+    if (L.smem > 48 * 1024)
+        MTB_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem));
+    int per_sm = 0;
+    MTB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, L.threads, L.smem));
+    if (per_sm < 1) return MTB_ERR_BAD_SHAPE;
+    int blocks = per_sm * sm_count();
+    kern<<<blocks, L.threads, L.smem, st>>>(a);
+    MTB_CUDA_TRY(cudaGetLastError());
+    return MTB_OK;
+}
+
+template <int P>
+static int launch_bucket(GridArgs a, const Launch &L, cudaStream_t st) {
+    a.rows = L.rows;
+    a.nbands = L.nbands;
+    if (L.kmax == 1) return L.window ? launch_one<P, 1, true>(a, L, st) : launch_one<P, 1, false>(a, L, st);
+    if (L.kmax == 2) return L.window ? launch_one<P, 2, true>(a, L, st) : launch_one<P, 2, false>(a, L, st);
+    return L.window ? launch_one<P, 8, true>(a, L, st) : launch_one<P, 8, false>(a, L, st);
+}
+
+template <int P>
+static int run_grid(const mtb_grid_params *p, const GridPlan &plan, const float2 *table, const int *conv_info,
+                    const float *conv_sums, const float *uvw, const float *freq, const float2 *vis,
+                    const float *weights, const int *flags, int R, float *grid, float *grid_lo,
+                    float *normalizer, mtb_grid_stats *stats, GridSpace &s, cudaStream_t st) {
+    const int T = oversample_T(p->sampling);
+    const int sms = sm_count();
+    MTB_CUDA_TRY(cudaMemsetAsync(s.norm_acc, 0, 4 * sizeof(double), st));
+    MTB_CUDA_TRY(cudaMemsetAsync(s.stats, 0, 4 * sizeof(unsigned long long), st));
+    MTB_CUDA_TRY(cudaMemsetAsync(s.bounds, 0, 2 * kMaxBuckets * sizeof(int), st));
+    MTB_CUDA_TRY(cudaMemsetAsync(s.counters, 0, kMaxBuckets * sizeof(int), st));
+    int blocks = std::min((R + 255) / 256, sms * 8);
+    if (blocks < 1) blocks = 1;
+    k_preprocess<P><<<blocks, 256, 0, st>>>(R, uvw, freq, weights, flags, conv_info, conv_sums, p->wplanes,
+                                            p->w_sq_increment, p->sampling, T, p->nx, p->ny, p->u_increment,
+                                            p->v_increment, s.pos, s.meta, s.norm_acc, nullptr);
+    MTB_CUDA_TRY(cudaGetLastError());
+    k_compress<<<blocks, 256, 0, st>>>(R, p->nx, s.pos, s.meta, s.keys, s.iota, plan.bt, s.stats);
+    MTB_CUDA_TRY(cudaGetLastError());
+    int end_bit = 24;
+    while ((1 << (end_bit - 24)) < plan.bt.n) end_bit++;
+    // the kNoKey sentinel needs every bit: sort the full 32 bits
+    size_t cb = s.cub_bytes;
+    MTB_CUDA_TRY(cub::DeviceRadixSort::SortPairs(s.cub, cb, s.keys, s.skeys, s.iota, s.sidx, R, 0, 32, st));
+    cb = s.cub_bytes;
+    MTB_CUDA_TRY(cub::DeviceRunLengthEncode::Encode(s.cub, cb, s.skeys, s.ukeys, s.counts, s.num_runs, R, st));
+    cb = s.cub_bytes;
+    MTB_CUDA_TRY(cub::DeviceScan::ExclusiveSum(s.cub, cb, s.counts, s.run_start, R, st));
+    k_chunk_counts<<<blocks, 256, 0, st>>>(s.ukeys, s.counts, s.num_runs, R, plan.chunk, s.nchunks);
+    MTB_CUDA_TRY(cudaGetLastError());
+    cb = s.cub_bytes;
+    MTB_CUDA_TRY(cub::DeviceScan::ExclusiveSum(s.cub, cb, s.nchunks, s.item_start, R, st));
+    k_make_items<<<blocks, 256, 0, st>>>(s.ukeys, s.counts, s.run_start, s.item_start, s.nchunks, s.num_runs,
+                                         plan.chunk, s.items);
+    MTB_CUDA_TRY(cudaGetLastError());
+    k_bucket_bounds<<<blocks, 256, 0, st>>>(s.items, s.item_start, s.nchunks, s.num_runs, s.bounds, plan.bt.n);
+    MTB_CUDA_TRY(cudaGetLastError());
+    k_gather<P><<<blocks, 256, 0, st>>>(R, s.skeys, s.sidx, s.pos, s.meta, vis, weights, flags, s.wpos, s.wvis);
+    MTB_CUDA_TRY(cudaGetLastError());
+    (void)end_bit;
+
+    GridArgs a;
+    a.items = s.items;
+    a.bounds = s.bounds;
+    a.counters = s.counters;
+    a.wpos = s.wpos;
+    a.wvis = s.wvis;
+    a.table = table;
+    a.grid = grid;
+    a.grid_lo = grid_lo;
+    a.nx = p->nx;
+    a.ny = p->ny;
+    for (int b = 0; b < plan.bt.n; b++) {
+        int M = plan.bt.M[b];
+        if (M <= 0) continue;
+        a.bucket = b;
+        a.M = M;
+        a.tile = plan.bt.tile[b];
+        a.W = a.tile + M - 1;
+        Launch L = launch_shape(M, P, a.tile);
+        MTB_TRY(launch_bucket<P>(a, L, st));
+    }
+    k_finish<<<1, 32, 0, st>>>(P, s.norm_acc, normalizer, s.stats, stats);
+    MTB_CUDA_TRY(cudaGetLastError());
+    return MTB_OK;
+}
+
+// PreProcessUVW's seven outputs in the reference's layout
+// (WProjPreProcessUVW.cpp:66-85): GriddingData int4 {cx, cy*nx+cx,
+// -(cx%S), -(cy%S)}, conv index, ToGridIndicator (after compression),
+// ToCompressIndicator, support, TakeConjugateIndicator (+1/-1).
+__global__ void k_ref_outputs(int R, int nx, const int4 *__restrict__ pos, const int *__restrict__ meta,
+                              int4 *__restrict__ gdata, int *__restrict__ convidx, int *__restrict__ togrid,
+                              int *__restrict__ tocompress, int *__restrict__ support, float *__restrict__ imgmult) {
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < R; r += gridDim.x * blockDim.x) {
+        int4 q = pos[r];
+        int m = meta[r];
+        bool g = (m & 1) != 0;
+        gdata[r] = g ? make_int4(q.x, q.y * nx + q.x, -(q.x % q.w), -(q.y % q.w)) : make_int4(0, 0, 0, 0);
+        convidx[r] = q.z;
+        togrid[r] = (g && !(m & 4)) ? 1 : 0;
+        tocompress[r] = (m & 4) ? 1 : 0;
+        support[r] = q.w;
+        imgmult[r] = (m & 2) ? -1.0f : 1.0f;
+    }
+}
+
+}  // namespace mtb
+
+using namespace mtb;
+
+extern "C" int mtb_grid_workspace_size(const mtb_grid_params *p, int nrecords, size_t *bytes) {
+    if (!bytes) return MTB_ERR_NULL;
+    MTB_TRY(check_params(p));
+    if (nrecords < 0) return MTB_ERR_BAD_SHAPE;
+    int chunk = p->max_chunk > 0 ? p->max_chunk : kDefaultChunk;
+    Arena A;
+    GridSpace s;
+    carve_grid(A, nrecords, p->npol, chunk, &s);
+    *bytes = A.used;
+    return MTB_OK;
+}
+
+extern "C" int mtb_grid(const mtb_grid_params *p, const void *d_table, const int *d_conv_info,
+                        const int *h_conv_info, const float *d_conv_sums, const float *d_uvw,
+                        const float *d_freq, const void *d_vis, const float *d_weights, const int *d_flags,
+                        int nrecords, void *d_grid, void *d_grid_lo, float *d_normalizer,
+                        mtb_grid_stats *d_stats, void *d_workspace, size_t workspace_bytes,
+                        mtb_stream_t stream) {
+    MTB_TRY(check_params(p));
+    if (nrecords < 0) return MTB_ERR_BAD_SHAPE;
+    if (!d_grid || !d_normalizer || !h_conv_info) return MTB_ERR_NULL;
+    cudaStream_t st = (cudaStream_t)stream;
+    GridPlan plan;
+    MTB_TRY(make_plan(p, h_conv_info, &plan));
+    const int P = p->npol;
+    size_t gbytes = (size_t)p->nx * p->ny * P * sizeof(float2);
+    if (p->initialize_output) {
+        MTB_CUDA_TRY(cudaMemsetAsync(d_grid, 0, gbytes, st));
+        if (d_grid_lo) MTB_CUDA_TRY(cudaMemsetAsync(d_grid_lo, 0, gbytes, st));
+        MTB_CUDA_TRY(cudaMemsetAsync(d_normalizer, 0, P * sizeof(float), st));
+        if (d_stats) MTB_CUDA_TRY(cudaMemsetAsync(d_stats, 0, sizeof(mtb_grid_stats), st));
+    }
+    if (nrecords == 0) return MTB_OK;
+    if (!d_table || !d_conv_info || !d_conv_sums || !d_uvw || !d_freq || !d_vis || !d_weights || !d_flags ||
+        !d_workspace)
+        return MTB_ERR_NULL;
+    Arena A(d_workspace, workspace_bytes);
+    GridSpace s;
+    carve_grid(A, nrecords, P, plan.chunk, &s);
+    if (!A.ok()) return MTB_ERR_WORKSPACE;
+    const float2 *tb = (const float2 *)d_table;
+    const float2 *vis = (const float2 *)d_vis;
+    float *g = (float *)d_grid, *lo = (float *)d_grid_lo;
+    if (P == 1)
+        return run_grid<1>(p, plan, tb, d_conv_info, d_conv_sums, d_uvw, d_freq, vis, d_weights, d_flags,
+                           nrecords, g, lo, d_normalizer, d_stats, s, st);
+    if (P == 2)
+        return run_grid<2>(p, plan, tb, d_conv_info, d_conv_sums, d_uvw, d_freq, vis, d_weights, d_flags,
+                           nrecords, g, lo, d_normalizer, d_stats, s, st);
+    return run_grid<4>(p, plan, tb, d_conv_info, d_conv_sums, d_uvw, d_freq, vis, d_weights, d_flags, nrecords,
+                       g, lo, d_normalizer, d_stats, s, st);
+}
+
+extern "C" int mtb_preprocess_uvw(const mtb_grid_params *p, const int *d_conv_info, const int *h_conv_info,
+                                  const float *d_conv_sums, const float *d_uvw, const float *d_freq,
+                                  const float *d_weights, const int *d_flags, int nrecords, int *d_gridding_data,
+                                  int *d_conv_index, int *d_to_grid, int *d_to_compress, int *d_support,
+                                  float *d_take_conjugate, float *d_conv_sum, void *d_workspace,
+                                  size_t workspace_bytes, mtb_stream_t stream) {
+    MTB_TRY(check_params(p));
+    if (nrecords < 0) return MTB_ERR_BAD_SHAPE;
+    if (nrecords == 0) return MTB_OK;
+    if (!d_conv_info || !h_conv_info || !d_conv_sums || !d_uvw || !d_freq || !d_weights || !d_flags ||
+        !d_gridding_data || !d_conv_index || !d_to_grid || !d_to_compress || !d_support || !d_take_conjugate ||
+        !d_conv_sum || !d_workspace)
+        return MTB_ERR_NULL;
+    GridPlan plan;
+    MTB_TRY(make_plan(p, h_conv_info, &plan));
+    cudaStream_t st = (cudaStream_t)stream;
+    Arena A(d_workspace, workspace_bytes);
+    GridSpace s;
+    carve_grid(A, nrecords, p->npol, plan.chunk, &s);
+    if (!A.ok()) return MTB_ERR_WORKSPACE;
+    const int R = nrecords, T = oversample_T(p->sampling);
+    int blocks = std::min((R + 255) / 256, sm_count() * 8);
+    MTB_CUDA_TRY(cudaMemsetAsync(s.norm_acc, 0, 4 * sizeof(double), st));
+    MTB_CUDA_TRY(cudaMemsetAsync(s.stats, 0, 4 * sizeof(unsigned long long), st));
+#define MTB_PRE(PP)                                                                                           \
+    k_preprocess<PP><<<blocks, 256, 0, st>>>(R, d_uvw, d_freq, d_weights, d_flags, d_conv_info, d_conv_sums,   \
+                                             p->wplanes, p->w_sq_increment, p->sampling, T, p->nx, p->ny,     \
+                                             p->u_increment, p->v_increment, s.pos, s.meta, s.norm_acc,       \
+                                             d_conv_sum)
+    if (p->npol == 1) MTB_PRE(1);
+    else if (p->npol == 2) MTB_PRE(2);
+    else MTB_PRE(4);
+#undef MTB_PRE
+    MTB_CUDA_TRY(cudaGetLastError());
+    k_compress<<<blocks, 256, 0, st>>>(R, p->nx, s.pos, s.meta, s.keys, s.iota, plan.bt, s.stats);
+    MTB_CUDA_TRY(cudaGetLastError());
+    k_ref_outputs<<<blocks, 256, 0, st>>>(R, p->nx, s.pos, s.meta, (int4 *)d_gridding_data, d_conv_index,
+                                          d_to_grid, d_to_compress, d_support, d_take_conjugate);
+    MTB_CUDA_TRY(cudaGetLastError());
+    return MTB_OK;
+}

@@ -1,0 +1,99 @@
+"""ctypes binding of libmtb.so (the C ABI declared in include/mtb.h).
+
+The library is the product: there is no Python or CPU implementation of any
+kernel behind this module.  If libmtb.so is missing the import of the compute
+entry points fails loudly.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.dirname(HERE)
+LIB_PATH = os.path.join(PKG, "libmtb.so")
+
+MTB_OK = 0
+MTB_POL_LINEAR = 0
+MTB_POL_CIRCULAR = 1
+
+# every entry point include/mtb.h declares
+EXPORTS = (
+    "mtb_wkernel_query", "mtb_wkernel_build", "mtb_grid_workspace_size", "mtb_grid", "mtb_preprocess_uvw",
+    "mtb_finalize_workspace_size", "mtb_finalize", "mtb_status_string", "mtb_version",
+    "mtb_release_caches",
+)
+
+
+class MtbError(RuntimeError):
+    def __init__(self, status, where):
+        self.status = status
+        msg = _lib.mtb_status_string(status).decode() if _lib is not None else str(status)
+        super().__init__("%s failed: %s (status %d)" % (where, msg, status))
+
+
+class WKernelParams(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("l_increment", ctypes.c_double),
+                ("m_increment", ctypes.c_double), ("wplanes", ctypes.c_int), ("sampling", ctypes.c_int),
+                ("trial_support", ctypes.c_int), ("max_support", ctypes.c_int), ("w_max", ctypes.c_double)]
+
+
+class WKernelInfo(ctypes.Structure):
+    _fields_ = [("trial_support", ctypes.c_int), ("planesize", ctypes.c_int), ("support_cap", ctypes.c_int),
+                ("T", ctypes.c_int), ("w_max", ctypes.c_double), ("w_sq_increment", ctypes.c_double),
+                ("total_l", ctypes.c_double), ("total_m", ctypes.c_double), ("u_increment", ctypes.c_double),
+                ("v_increment", ctypes.c_double), ("table_capacity", ctypes.c_size_t),
+                ("workspace_bytes", ctypes.c_size_t)]
+
+
+class GridParams(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("npol", ctypes.c_int), ("sampling", ctypes.c_int),
+                ("wplanes", ctypes.c_int), ("u_increment", ctypes.c_double), ("v_increment", ctypes.c_double),
+                ("w_sq_increment", ctypes.c_double), ("initialize_output", ctypes.c_int), ("tile", ctypes.c_int),
+                ("support_bucket", ctypes.c_int), ("max_chunk", ctypes.c_int)]
+
+
+class GridStats(ctypes.Structure):
+    _fields_ = [("gridded_records", ctypes.c_ulonglong), ("compressed_records", ctypes.c_ulonglong),
+                ("gridded_points", ctypes.c_ulonglong), ("compressed_points", ctypes.c_ulonglong)]
+
+
+class FinalizeParams(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("npol", ctypes.c_int), ("sampling", ctypes.c_int),
+                ("pol_type", ctypes.c_int)]
+
+
+_lib = None
+
+
+def load(path: str = LIB_PATH):
+    """Load libmtb.so and declare the prototypes.  Raises if it is absent."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError("libmtb.so not found at %s: build it with python mt-imager_b200/build.py" % path)
+    L = ctypes.CDLL(path)
+    p, i, sz = ctypes.c_void_p, ctypes.c_int, ctypes.c_size_t
+    L.mtb_wkernel_query.argtypes = [ctypes.POINTER(WKernelParams), ctypes.POINTER(WKernelInfo)]
+    L.mtb_wkernel_build.argtypes = [ctypes.POINTER(WKernelParams), p, sz, p, sz, p, p, p,
+                                    ctypes.POINTER(sz), p]
+    L.mtb_grid_workspace_size.argtypes = [ctypes.POINTER(GridParams), i, ctypes.POINTER(sz)]
+    L.mtb_grid.argtypes = [ctypes.POINTER(GridParams), p, p, p, p, p, p, p, p, p, i, p, p, p, p, p, sz, p]
+    L.mtb_preprocess_uvw.argtypes = [ctypes.POINTER(GridParams), p, p, p, p, p, p, p, i] + [p] * 8 + [sz, p]
+    L.mtb_finalize_workspace_size.argtypes = [ctypes.POINTER(FinalizeParams), ctypes.POINTER(sz)]
+    L.mtb_finalize.argtypes = [ctypes.POINTER(FinalizeParams), p, p, p, p, p, sz, p]
+    for name in EXPORTS:
+        getattr(L, name).restype = i
+    L.mtb_status_string.restype = ctypes.c_char_p
+    L.mtb_status_string.argtypes = [i]
+    L.mtb_version.argtypes = []
+    L.mtb_release_caches.restype = None
+    L.mtb_release_caches.argtypes = []
+    _lib = L
+    return L
+
+
+def check(status: int, where: str):
+    if status != MTB_OK:
+        raise MtbError(status, where)

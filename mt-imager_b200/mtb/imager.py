@@ -1,0 +1,184 @@
+"""Host API of the W-projection imaging path over the C ABI.
+
+``WProjectionImager`` plays the part of mt-imager's three imaging modules on
+one GPU: WProjectionConvFunction (kernel table), WImager (per-chunk gridding
+into an accumulating grid and normaliser) and ImageFinalizer (Stokes cube),
+as wired by ``code/mt-imager/app/mtimager.cpp:138-199``.  Device memory and
+streams come from PyTorch; every computation is a call into libmtb.so.
+"""
+from __future__ import annotations
+
+import ctypes
+import dataclasses
+
+import numpy as np
+import torch
+
+from . import _lib as L
+
+
+def _ptr(t):
+    return ctypes.c_void_p(t.data_ptr()) if t is not None else ctypes.c_void_p(0)
+
+
+def _stream(stream=None):
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return ctypes.c_void_p(s.cuda_stream)
+
+
+def _dev(x, dtype, device):
+    if isinstance(x, torch.Tensor):
+        return x.to(device=device, dtype=dtype).contiguous()
+    return torch.from_numpy(np.ascontiguousarray(x)).to(device=device, dtype=dtype)
+
+
+@dataclasses.dataclass
+class KernelTable:
+    """AmalgamatedConvFunction, convInfo and ConvSums
+    (WProjectionConvFunction.cpp:297-301)."""
+    table: torch.Tensor          # complex64 [elems]
+    conv_info: np.ndarray        # int32 [wplanes][2] (host)
+    d_conv_info: torch.Tensor    # int32 [wplanes][2]
+    conv_sums: torch.Tensor      # float32 [wplanes][T*T]
+    info: L.WKernelInfo
+    params: L.WKernelParams
+
+    @property
+    def supports(self):
+        return self.conv_info[:, 0].copy()
+
+
+def wkernel_params(nx, ny, l_increment, m_increment, wplanes, sampling, trial_support=0, max_support=0,
+                   w_max=0.0) -> L.WKernelParams:
+    return L.WKernelParams(nx, ny, float(l_increment), float(m_increment), wplanes, sampling, trial_support,
+                           max_support, float(w_max))
+
+
+def query_wkernels(params: L.WKernelParams) -> L.WKernelInfo:
+    lib = L.load()
+    info = L.WKernelInfo()
+    L.check(lib.mtb_wkernel_query(ctypes.byref(params), ctypes.byref(info)), "mtb_wkernel_query")
+    return info
+
+
+def build_wkernels(params: L.WKernelParams, device="cuda", stream=None) -> KernelTable:
+    lib = L.load()
+    info = query_wkernels(params)
+    ws = torch.empty(max(1, info.workspace_bytes), dtype=torch.uint8, device=device)
+    table = torch.empty(max(1, info.table_capacity), dtype=torch.complex64, device=device)
+    nw = params.wplanes
+    d_ci = torch.empty((nw, 2), dtype=torch.int32, device=device)
+    h_ci = np.zeros((nw, 2), np.int32)
+    sums = torch.empty((nw, info.T * info.T), dtype=torch.float32, device=device)
+    n = ctypes.c_size_t(0)
+    L.check(lib.mtb_wkernel_build(ctypes.byref(params), _ptr(ws), info.workspace_bytes, _ptr(table),
+                                  info.table_capacity, _ptr(d_ci), h_ci.ctypes.data_as(ctypes.c_void_p),
+                                  _ptr(sums), ctypes.byref(n), _stream(stream)), "mtb_wkernel_build")
+    del ws
+    return KernelTable(table=table[: n.value].clone(), conv_info=h_ci, d_conv_info=d_ci, conv_sums=sums,
+                       info=info, params=params)
+
+
+class WProjectionImager:
+    """One image (one channel) on one GPU: kernel table, resident grid and
+    normaliser, chunked gridding and finalisation."""
+
+    def __init__(self, nx, ny, l_increment, m_increment=None, wplanes=32, sampling=8, npol=4,
+                 trial_support=0, max_support=0, w_max=0.0, pol_type=L.MTB_POL_LINEAR, compensated=True,
+                 tile=0, support_bucket=0, max_chunk=0, device="cuda", kernels: KernelTable | None = None):
+        self.lib = L.load()
+        self.device = torch.device(device)
+        self.nx, self.ny, self.npol = nx, ny, npol
+        m_increment = l_increment if m_increment is None else m_increment
+        self.params = wkernel_params(nx, ny, l_increment, m_increment, wplanes, sampling, trial_support,
+                                     max_support, w_max)
+        self.kernels = kernels
+        self.compensated = compensated
+        self.pol_type = pol_type
+        self.tuning = dict(tile=tile, support_bucket=support_bucket, max_chunk=max_chunk)
+        self.grid = torch.zeros((ny, nx, npol), dtype=torch.complex64, device=self.device)
+        self.grid_lo = torch.zeros_like(self.grid) if compensated else None
+        self.normalizer = torch.zeros(npol, dtype=torch.float32, device=self.device)
+        self.stats = torch.zeros(4, dtype=torch.int64, device=self.device)
+        self._ws = None
+        self._fin_ws = None
+        self._fresh = True
+
+    # -- WProjectionConvFunction
+    def build_kernels(self, stream=None) -> KernelTable:
+        if self.kernels is None:
+            self.kernels = build_wkernels(self.params, self.device, stream)
+        return self.kernels
+
+    def grid_params(self, initialize: bool) -> L.GridParams:
+        k = self.build_kernels()
+        return L.GridParams(self.nx, self.ny, self.npol, self.params.sampling, self.params.wplanes,
+                            k.info.u_increment, k.info.v_increment, k.info.w_sq_increment, int(initialize),
+                            self.tuning["tile"], self.tuning["support_bucket"], self.tuning["max_chunk"])
+
+    def _workspace(self, nrec, gp):
+        need = ctypes.c_size_t(0)
+        L.check(self.lib.mtb_grid_workspace_size(ctypes.byref(gp), nrec, ctypes.byref(need)),
+                "mtb_grid_workspace_size")
+        if self._ws is None or self._ws.numel() < need.value:
+            self._ws = torch.empty(max(1, need.value), dtype=torch.uint8, device=self.device)
+        return self._ws, need.value
+
+    def reset(self):
+        self._fresh = True
+
+    # -- WImager
+    def grid_chunk(self, uvw, freq, vis, weights, flags, stream=None):
+        """Grid one chunk: uvw [3][R] float32 metres, freq [R] nu/c, vis [R][P]
+        complex64, weights [R][P] float32, flags [R][P] int32 (numpy or torch)."""
+        dev = self.device
+        uvw = _dev(uvw, torch.float32, dev)
+        freq = _dev(freq, torch.float32, dev)
+        vis = _dev(vis, torch.complex64, dev)
+        weights = _dev(weights, torch.float32, dev)
+        flags = _dev(flags, torch.int32, dev)
+        R = int(freq.numel())
+        if vis.shape != (R, self.npol) or weights.shape != (R, self.npol) or flags.shape != (R, self.npol):
+            raise ValueError("record arrays must be [R][npol]")
+        if uvw.shape != (3, R):
+            raise ValueError("uvw must be [3][R]")
+        return self.grid_device(uvw, freq, vis, weights, flags, stream)
+
+    def grid_device(self, uvw, freq, vis, weights, flags, stream=None):
+        k = self.build_kernels()
+        R = int(freq.numel())
+        gp = self.grid_params(self._fresh)
+        ws, nbytes = self._workspace(R, gp)
+        st = L.check(self.lib.mtb_grid(ctypes.byref(gp), _ptr(k.table), _ptr(k.d_conv_info),
+                                       k.conv_info.ctypes.data_as(ctypes.c_void_p), _ptr(k.conv_sums),
+                                       _ptr(uvw), _ptr(freq), _ptr(vis), _ptr(weights), _ptr(flags), R,
+                                       _ptr(self.grid), _ptr(self.grid_lo), _ptr(self.normalizer),
+                                       _ptr(self.stats), _ptr(ws), nbytes, _stream(stream)), "mtb_grid")
+        self._fresh = False
+        return st
+
+    # -- ImageFinalizer
+    def finalize(self, out=None, stream=None):
+        fp = L.FinalizeParams(self.nx, self.ny, self.npol, self.params.sampling, self.pol_type)
+        need = ctypes.c_size_t(0)
+        L.check(self.lib.mtb_finalize_workspace_size(ctypes.byref(fp), ctypes.byref(need)),
+                "mtb_finalize_workspace_size")
+        if self._fin_ws is None or self._fin_ws.numel() < need.value:
+            self._fin_ws = torch.empty(max(1, need.value), dtype=torch.uint8, device=self.device)
+        if out is None:
+            out = torch.empty((self.npol, self.ny, self.nx), dtype=torch.float32, device=self.device)
+        L.check(self.lib.mtb_finalize(ctypes.byref(fp), _ptr(self.grid), _ptr(self.grid_lo), _ptr(self.normalizer),
+                                      _ptr(out), _ptr(self._fin_ws), need.value, _stream(stream)), "mtb_finalize")
+        return out
+
+    def grid_sum(self):
+        """Grid value the finaliser uses (hi + compensation term)."""
+        g = self.grid.clone()
+        if self.grid_lo is not None:
+            g += self.grid_lo
+        return g
+
+    def statistics(self):
+        s = self.stats.cpu().numpy()
+        return dict(gridded_records=int(s[0]), compressed_records=int(s[1]), gridded_points=int(s[2]),
+                    compressed_points=int(s[3]))
