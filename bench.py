@@ -1,0 +1,514 @@
+#!/usr/bin/env python
+"""Benchmark of the W-projection imaging path: vis·pol samples gridded per second.
+
+Workload (default, one GPU): the mid-size plain W-projection configuration --
+64 antennas within 4 km, 16 channels over 1.3-1.5 GHz, an 8 h track at 2 s
+(2016 baselines x 14,400 integrations = 29,030,400 records per channel,
+4.64e8 visibilities), 4 complex64 polarisations, 200 power-law point sources,
+25 % of records flagged, 4096 x 4096 image, 128 w-planes, oversampling 8,
+supports 7-65.  Synthetic, seeded data stand in for a MeasurementSet.
+
+One step images every channel: mtb_grid (preprocess, bin, tile gridder) into a
+fresh grid, then mtb_finalize (IFFT, Stokes, corrections).  The w-kernel table
+is built once and shared (the reference also builds it once per run).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl mtb|reference]
+                    [--channels C] [--hours H] [--config mid|small]
+
+Under torchrun each rank runs an independent replica (the path has no
+cross-GPU exchange); rank 0 prints one JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import math
+import os
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "mt-imager_b200")
+for _p in (ROOT, PKG):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+import numpy as np  # noqa: E402
+
+METRIC = "vis·pol samples/s gridded; p50/p99 image latency vs plain GPU path at ≤1e-5 RMS"
+C_LIGHT = 299792458.0
+ARCSEC = math.pi / (180.0 * 3600.0)
+
+
+# ------------------------------------------------------------- workload ----
+def workload_spec(args):
+    if args.config == "small":
+        return dict(name="small", n_ant=27, radius=1000.0, f_lo=1.4e9, f_hi=1.4e9, nchan=1, hours=1.0, dt=10.0,
+                    nsrc=10, powerlaw=None, flux=(0.1, 1.0), flag=0.0, nx=256, cell_arcsec=2.0, wplanes=32,
+                    sampling=8, trial_support=0, max_support=0, lat=-30.0, dec=-45.0)
+    return dict(name="mid", n_ant=64, radius=4000.0, f_lo=1.3e9, f_hi=1.5e9, nchan=args.channels,
+                hours=args.hours, dt=2.0, nsrc=200, powerlaw=-1.5, flux=(1e-3, 1.0), flag=0.25, nx=4096,
+                cell_arcsec=None, wplanes=128, sampling=8, trial_support=67, max_support=65, lat=-30.0,
+                dec=-45.0)
+
+
+def make_uvw(spec, device, torch, rng, nbl_limit=None, nt_limit=None):
+    from mtb import synth
+    enu = synth.antenna_layout(spec["n_ant"], spec["radius"], rng)
+    pairs = synth.baseline_order(spec["n_ant"])
+    if nbl_limit:
+        pairs = pairs[:nbl_limit]
+    nt = int(round(spec["hours"] * 3600.0 / spec["dt"]))
+    if nt_limit:
+        nt = min(nt, nt_limit)
+    lat, dec = math.radians(spec["lat"]), math.radians(spec["dec"])
+    a1 = torch.tensor([p[0] for p in pairs], device=device)
+    a2 = torch.tensor([p[1] for p in pairs], device=device)
+    e = torch.tensor(enu, dtype=torch.float64, device=device)
+    d = e[a2] - e[a1]
+    lx = (-d[:, 1] * math.sin(lat) + d[:, 2] * math.cos(lat))[:, None]
+    ly = d[:, 0][:, None]
+    lz = (d[:, 1] * math.cos(lat) + d[:, 2] * math.sin(lat))[:, None]
+    ha = ((torch.arange(nt, device=device, dtype=torch.float64) - (nt - 1) / 2.0) * spec["dt"]
+          * (2 * math.pi / 86164.0905))[None, :]
+    sh, ch = torch.sin(ha), torch.cos(ha)
+    uvw = torch.empty((3, len(pairs), nt), dtype=torch.float32, device=device)
+    uvw[0] = (sh * lx + ch * ly).float()
+    uvw[1] = (-math.sin(dec) * ch * lx + math.sin(dec) * sh * ly + math.cos(dec) * lz).float()
+    uvw[2] = (math.cos(dec) * ch * lx - math.cos(dec) * sh * ly + math.sin(dec) * lz).float()
+    return uvw.reshape(3, -1).contiguous(), len(pairs), nt
+
+
+def channel_freqs(spec):
+    if spec["nchan"] == 1:
+        return np.array([spec["f_lo"]])
+    return np.linspace(spec["f_lo"], spec["f_hi"], spec["nchan"])
+
+
+def cell_for(spec, uvw_max_m, torch):
+    """Largest cell with max|u|/du + 65/2 < N/2 at the highest frequency."""
+    if spec["cell_arcsec"]:
+        return spec["cell_arcsec"] * ARCSEC
+    n = spec["nx"]
+    uv_max = uvw_max_m * spec["f_hi"] / C_LIGHT
+    du = uv_max / (n / 2 - (spec["max_support"] / 2 + 1))
+    return 1.0 / (n * du)
+
+
+def make_vis(uvw, freq_hz, sources, torch, generator):
+    """Point-source visibilities complex64 [R][4] (XX, XY, YX, YY)."""
+    R = uvw.shape[1]
+    k = 2 * math.pi * freq_hz / C_LIGHT
+    out = torch.zeros((R, 4), dtype=torch.complex64, device=uvw.device)
+    for l, m, si, sq, su, sv in sources:
+        n1 = math.sqrt(1 - l * l - m * m) - 1
+        ph = (uvw[0] * l + uvw[1] * m + uvw[2] * n1) * (-k)
+        e = torch.polar(torch.ones_like(ph), ph)
+        out[:, 0] += (si + sq) * e
+        out[:, 1] += complex(su, sv) * e
+        out[:, 2] += complex(su, -sv) * e
+        out[:, 3] += (si - sq) * e
+    return out
+
+
+def sources_for(spec, fov, rng):
+    from mtb import synth
+    return synth.random_sources(spec["nsrc"], fov, rng, flux=spec["flux"], powerlaw=spec["powerlaw"])
+
+
+# ----------------------------------------------------------------- clocks --
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.proc = None
+        self.gpu = gpu_index
+        self.path = os.path.join(ROOT, "gpurun_out", "clocks_rank%d.csv" % gpu_index)
+
+    def start(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.fh,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.fh.close()
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except ValueError:
+                continue
+            for nme, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nme)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------- reference arm --
+def run_reference(args, rank, world):
+    """The reference's gridding semantics on the host cores: the FP32 OpenMP
+    transcription (oracle/cpu_port.c), each step a bounded sample of the same
+    workload (one channel, a block of baselines over the full track)."""
+    if rank != 0:
+        return
+    import torch
+    from oracle import oracle as O
+    spec = workload_spec(args)
+    rng = np.random.default_rng(2)
+    nbl = args.ref_baselines if spec["name"] == "mid" else None
+    uvw, _, _ = make_uvw(spec, "cpu", torch, rng, nbl_limit=nbl)
+    full, _, _ = make_uvw(spec, "cpu", torch, np.random.default_rng(2), nbl_limit=None, nt_limit=8)
+    dl = cell_for(spec, float(full[:2].abs().max()), torch)
+    freqs = channel_freqs(spec)
+    f = freqs[len(freqs) // 2]
+    gen = torch.Generator().manual_seed(3)
+    srcs = sources_for(spec, spec["nx"] * dl, rng)
+    vis = make_vis(uvw.double(), f, srcs, torch, gen).numpy()
+    R = uvw.shape[1]
+    flags = (torch.rand(R, generator=gen) < spec["flag"]).int()[:, None].repeat(1, 4).numpy()
+    weights = np.ones((R, 4), np.float32)
+    freq = np.full(R, f / C_LIGHT, np.float32)
+    geo = O.kernel_geometry(spec["nx"], spec["nx"], dl, dl, spec["wplanes"], spec["sampling"],
+                            spec["trial_support"], spec["max_support"])
+    kern = O.wkernels(geo)
+    table = kern["table"].astype(np.complex64)
+    sums = kern["conv_sums"].astype(np.float32)
+    P = O.port()
+    cores = P.port_threads()
+    grid = np.zeros((spec["nx"], spec["nx"], 4), np.complex64)
+    norm = np.zeros(4, np.float32)
+    uvw_np = uvw.numpy()
+
+    def step():
+        grid[:] = 0
+        st = np.zeros(4, np.int64)
+        P.port_grid_chunk(R, 4, O._p(uvw_np), O._p(freq), O._p(vis), O._p(weights), O._p(flags),
+                          spec["wplanes"], geo["w_inc"], O._p(kern["conv_info"]), O._p(sums), O._p(table),
+                          spec["sampling"], spec["nx"], spec["nx"], geo["du"], geo["dv"], O._p(grid),
+                          O._p(norm), O._p(st))
+        return int(st[0] + st[1]) * 4
+    for _ in range(args.warmup):
+        step()
+    t0 = time.perf_counter()
+    samples = 0
+    for _ in range(args.steps):
+        samples += step()
+    dt = time.perf_counter() - t0
+    v = samples / dt
+    sample = "%d records of one %s channel (%d of %d baselines, full track), FP32 OpenMP port" % (
+        R, spec["name"], nbl or 0, spec["n_ant"] * (spec["n_ant"] - 1) // 2)
+    line = {"metric": METRIC, "value": v, "unit": "samples/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "impl": "reference", "config": {"workload": workload_name(spec), "sample": sample},
+            "cpu_baseline": {"value": v, "unit": "samples/s", "cores": cores, "kind": "port", "sample": sample},
+            "e2e": {"value": v, "unit": "samples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def workload_name(spec):
+    if spec["name"] == "small":
+        return ("plain small W-projection image: 27 antennas / 1 km, 1 channel at 1.4 GHz, 1 h at 10 s "
+                "(126,360 records), 4 pol, 256^2 at 2 arcsec, 32 w-planes, oversampling 8")
+    return ("mid-size plain GPU path: 64 antennas / 4 km, %d channels over 1.3-1.5 GHz, %.3g h at 2 s, 4 pol, "
+            "200 power-law sources, 25%% flagged, 4096^2, 128 w-planes, oversampling 8, support 7-65"
+            % (spec["nchan"], spec["hours"]))
+
+
+# ------------------------------------------------------------------ main ----
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="mtb", choices=["mtb", "reference"])
+    ap.add_argument("--config", default="mid", choices=["mid", "small"])
+    ap.add_argument("--channels", type=int, default=16)
+    ap.add_argument("--hours", type=float, default=8.0)
+    ap.add_argument("--e2e-steps", type=int, default=1)
+    ap.add_argument("--cpu-records", type=int, default=0, help="records for the CPU baseline sample")
+    ap.add_argument("--ref-baselines", type=int, default=140)
+    ap.add_argument("--tile", type=int, default=0)
+    ap.add_argument("--support-bucket", type=int, default=0)
+    ap.add_argument("--max-chunk", type=int, default=0)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+
+    import torch
+    import torch.distributed as dist
+    from mtb import _lib as L
+    from mtb.imager import WProjectionImager, build_wkernels, wkernel_params
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    spec = workload_spec(args)
+    lib = L.load()
+
+    # ---- data (seeded; every replica images the same cube)
+    t_gen = time.perf_counter()
+    rng = np.random.default_rng(2)
+    uvw, nbl, nt = make_uvw(spec, dev, torch, rng)
+    R = uvw.shape[1]
+    dl = cell_for(spec, float(uvw[:2].abs().max()), torch)
+    fov = spec["nx"] * dl
+    srcs = sources_for(spec, fov, rng)
+    freqs = channel_freqs(spec)
+    gen = torch.Generator(device=dev).manual_seed(7 + rank)
+    chans = []
+    for c, f in enumerate(freqs):
+        vis = make_vis(uvw, f, srcs, torch, gen)
+        flags = (torch.rand(R, device=dev, generator=gen) < spec["flag"]).int()[:, None].repeat(1, 4).contiguous()
+        weights = torch.ones((R, 4), dtype=torch.float32, device=dev)
+        freq = torch.full((R,), f / C_LIGHT, dtype=torch.float32, device=dev)
+        chans.append((freq, vis, weights, flags))
+    torch.cuda.synchronize()
+    t_gen = time.perf_counter() - t_gen
+
+    # ---- w-kernels (once) and one imager per channel
+    n = spec["nx"]
+    kp = wkernel_params(n, n, dl, dl, spec["wplanes"], spec["sampling"], spec["trial_support"],
+                        spec["max_support"])
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    kern = build_wkernels(kp, dev)
+    torch.cuda.synchronize()
+    wk_ms = (time.perf_counter() - t0) * 1e3
+    imagers = [WProjectionImager(n, n, dl, wplanes=spec["wplanes"], sampling=spec["sampling"],
+                                 trial_support=spec["trial_support"], max_support=spec["max_support"],
+                                 kernels=kern, device=dev, tile=args.tile, support_bucket=args.support_bucket,
+                                 max_chunk=args.max_chunk) for _ in freqs]
+    images = [torch.empty((4, n, n), dtype=torch.float32, device=dev) for _ in freqs]
+    gev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in freqs]
+    for im, ev in zip(imagers, gev):
+        for e in ev:          # torch creates the CUDA event on first record
+            e.record()
+        im.gridder_events = ev
+    torch.cuda.synchronize()
+    lat_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in freqs]
+
+    def step(record_latency=True):
+        for c, (im, (freq, vis, weights, flags)) in enumerate(zip(imagers, chans)):
+            if record_latency:
+                lat_ev[c][0].record()
+            im.reset()
+            im.grid_device(uvw, freq, vis, weights, flags)
+            im.finalize(out=images[c])
+            if record_latency:
+                lat_ev[c][1].record()
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    torch.cuda.synchronize()
+    stats = [im.statistics() for im in imagers]
+    samples_per_step = sum((s["gridded_records"] + s["compressed_records"]) * 4 for s in stats)
+    flops_per_step = sum(8.0 * 4 * s["gridded_points"] for s in stats)
+
+    clocks = ClockSampler(local)
+    launches0 = lib.mtb_kernel_launch_count()
+    lat, gms = [], []
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    t_start.record()
+    for _ in range(args.steps):
+        step()
+        torch.cuda.synchronize()
+        lat += [a.elapsed_time(b) for a, b in lat_ev]
+        gms.append(sum(a.elapsed_time(b) for a, b in gev))
+    t_end.record()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    launches = (lib.mtb_kernel_launch_count() - launches0) // max(1, args.steps)
+    ms = t_start.elapsed_time(t_end)
+    if world > 1:
+        tt = torch.tensor([ms], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+    ms_per_step = ms / args.steps
+    value = samples_per_step * world / (ms_per_step * 1e-3)
+
+    # ---- roofline of the gridder (FP32 FMA pipe; peak measured on this GPU)
+    peak = ctypes.c_double(0)
+    L.check(lib.mtb_calibrate_fp32(ctypes.byref(peak), ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)),
+            "mtb_calibrate_fp32")
+    gridder_ms = float(np.mean(gms))
+    achieved = flops_per_step / (gridder_ms * 1e-3) / 1e12
+    roof = {"bound": "fp32", "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
+            "frac": achieved / peak.value if peak.value else None, "traffic": None,
+            "kernel": "k_grid (all support buckets of one mtb_grid call, span timed by events)",
+            "peak_source": "measured: mtb_calibrate_fp32 (packed f32x2 FMA chains, this GPU)"}
+
+    # ---- end to end: host buffers, H2D per channel overlapped with compute
+    e2e = None
+    if not args.no_e2e:
+        e2e = run_e2e(args, torch, dev, uvw, chans, imagers, images, samples_per_step, world, dist)
+
+    # ---- CPU baseline (rank 0, one GPU)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_baseline(args, spec, uvw, chans, kern, dl, torch)
+
+    if rank == 0:
+        sup = kern.supports
+        line = {
+            "metric": METRIC, "value": value, "unit": "samples/s", "n_gpus": world, "steps": args.steps,
+            "warmup": max(3, args.warmup), "ms_per_step": ms_per_step, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 (FP64 coordinates and w-phase)",
+            "data": "synthetic (seeded earth-rotation tracks, point-source sky)",
+            "config": {"workload": workload_name(spec), "records_per_channel": R, "channels": len(freqs),
+                       "image": n, "cell_arcsec": dl / ARCSEC, "wplanes": spec["wplanes"],
+                       "sampling": spec["sampling"], "supports": [int(sup.min()), int(sup.max())],
+                       "samples_per_step": samples_per_step, "l2": "inputs larger than L2 (2 GB per channel)",
+                       "parallelism": "replicas" if world > 1 else "single GPU"},
+            "images_per_s": len(freqs) * world / (ms_per_step * 1e-3),
+            "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
+            "roofline": roof, "gpu_launches": int(launches), "wkernel_ms": wk_ms,
+            "gridder_ms_per_step": gridder_ms, "datagen_s": t_gen,
+        }
+        if e2e:
+            line["e2e"] = e2e
+        if cpu:
+            line["cpu_baseline"] = cpu
+        if clk:
+            line["clocks"] = clk
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def run_e2e(args, torch, dev, uvw_d, chans, imagers, images, samples_per_step, world, dist):
+    """Same metric through the public API from pinned host buffers: per step
+    the H2D copy of every channel's records and the D2H of every image are
+    inside the timed region.  Copies run on a side stream, double-buffered
+    against the compute of the previous channel."""
+    host_uvw = torch.empty(uvw_d.shape, dtype=uvw_d.dtype, pin_memory=True)
+    host_uvw.copy_(uvw_d)
+    host = []
+    for (freq, vis, weights, flags) in chans:
+        hc = []
+        for t in (freq, vis, weights, flags):
+            h = torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
+            h.copy_(t)
+            hc.append(h)
+        host.append(hc)
+    out_host = [torch.empty(im.shape, dtype=im.dtype, pin_memory=True) for im in images]
+    bufs = [[torch.empty_like(t) for t in chans[0]] for _ in range(2)]
+    uvw_buf = torch.empty_like(uvw_d)
+    copy = torch.cuda.Stream(device=dev)
+    comp = torch.cuda.current_stream(dev)
+    h2d = host_uvw.numel() * 4 + sum(sum(t.numel() * t.element_size() for t in hc) for hc in host)
+    d2h = sum(o.numel() * 4 for o in out_host)
+
+    def step():
+        ready = [torch.cuda.Event() for _ in host]
+        free = [torch.cuda.Event() for _ in range(2)]
+        with torch.cuda.stream(copy):
+            uvw_buf.copy_(host_uvw, non_blocking=True)
+        for c, hc in enumerate(host):
+            b = bufs[c % 2]
+            with torch.cuda.stream(copy):
+                if c >= 2:
+                    copy.wait_event(free[c % 2])
+                for dst, src in zip(b, hc):
+                    dst.copy_(src, non_blocking=True)
+                ready[c].record(copy)
+            comp.wait_event(ready[c])
+            im = imagers[c]
+            im.reset()
+            im.grid_device(uvw_buf, *b)
+            free[c % 2].record(comp)
+            im.finalize(out=images[c])
+            out_host[c].copy_(images[c], non_blocking=True)
+        torch.cuda.synchronize()
+
+    step()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(args.e2e_steps):
+        step()
+    b.record()
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / args.e2e_steps
+    if world > 1:
+        tt = torch.tensor([ms], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+    return {"value": samples_per_step * world / (ms * 1e-3), "unit": "samples/s", "h2d_bytes_per_step": int(h2d),
+            "d2h_bytes_per_step": int(d2h), "ms_per_step": ms}
+
+
+def cpu_baseline(args, spec, uvw_d, chans, kern, dl, torch):
+    """FP32 OpenMP port of the reference's gridding on the host cores, on a
+    bounded sample: the first records of one channel."""
+    from oracle import oracle as O
+    R = uvw_d.shape[1]
+    n_rec = args.cpu_records or min(R, 2_000_000)
+    freq, vis, weights, flags = chans[len(chans) // 2]
+    u = np.ascontiguousarray(uvw_d[:, :n_rec].cpu().numpy())
+    fq = np.ascontiguousarray(freq[:n_rec].cpu().numpy())
+    vs = np.ascontiguousarray(vis[:n_rec].cpu().numpy())
+    wt = np.ascontiguousarray(weights[:n_rec].cpu().numpy())
+    fl = np.ascontiguousarray(flags[:n_rec].cpu().numpy())
+    table = kern.table.cpu().numpy()
+    sums = kern.conv_sums.cpu().numpy()
+    ci = kern.conv_info
+    n = spec["nx"]
+    P = O.port()
+    grid = np.zeros((n, n, 4), np.complex64)
+    norm = np.zeros(4, np.float32)
+    st = np.zeros(4, np.int64)
+    t0 = time.perf_counter()
+    P.port_grid_chunk(n_rec, 4, O._p(u), O._p(fq), O._p(vs), O._p(wt), O._p(fl), spec["wplanes"],
+                      kern.info.w_sq_increment, O._p(ci), O._p(sums), O._p(table), spec["sampling"], n, n,
+                      kern.info.u_increment, kern.info.v_increment, O._p(grid), O._p(norm), O._p(st))
+    dt = time.perf_counter() - t0
+    samples = int(st[0] + st[1]) * 4
+    return {"value": samples / dt, "unit": "samples/s", "cores": P.port_threads(), "kind": "port",
+            "sample": "first %d records of one channel (%d samples gridded in %.2f s), FP32 OpenMP port"
+                      % (n_rec, samples, dt)}
+
+
+if __name__ == "__main__":
+    main()

@@ -126,6 +126,10 @@ typedef struct mtb_grid_params {
     int tile;                /* 0: default; grid tile edge owned by one thread block   */
     int support_bucket;      /* 0: default; supports are grouped in buckets this wide  */
     int max_chunk;           /* 0: default; most records one block grids in one pass   */
+    void *gridder_start_event; /* cudaEvent_t or NULL: recorded before the gridder kernels */
+    void *gridder_end_event;   /* cudaEvent_t or NULL: recorded after them (the span of the
+                                  ConvolutionGridder operator, like GPUSubmissionData's
+                                  startEvent/endEvent, GPUSubmissionData.h:27-47)          */
 } mtb_grid_params;
 
 typedef struct mtb_grid_stats {
@@ -192,6 +196,13 @@ const char *mtb_status_string(int status);
 int mtb_version(void);
 /* Releases cached cuFFT plans (plans are created on first use per shape). */
 void mtb_release_caches(void);
+/* Number of this library's own kernels launched so far in the process
+ * (cuFFT and CUB launches are not counted). */
+unsigned long long mtb_kernel_launch_count(void);
+/* Measures the FP32 FMA throughput of the current GPU (TFLOP/s, packed
+ * f32x2 FMA chains on every SM): the roofline denominator of the gridder.
+ * Synchronises `stream`. */
+int mtb_calibrate_fp32(double *tflops, mtb_stream_t stream);
 
 #ifdef __cplusplus
 }

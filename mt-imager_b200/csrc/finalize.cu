@@ -3,21 +3,25 @@
 //
 //   k_pre_ifft     PreIFFTUVCorrection (PreIFFTUVCorrection.cu:28-90): grid
 //                  [v][u][pol] -> planes [pol][v][u] with the origin moved to
-//                  the corner, adding the compensation term of the grid.
-//   cuFFT C2C      IFFT2D INVERSE, unnormalised (IFFT2D.cpp:86-111), all
-//                  polarisation planes in one batched plan on the caller's stream.
+//                  the corner.  The two-float grid (hi + lo) becomes one FP64
+//                  value, exactly.
+//   cuFFT Z2Z      IFFT2D INVERSE, unnormalised (IFFT2D.cpp:86-111), all
+//                  polarisation planes in one batched plan on the caller's
+//                  stream.  FP64: the taper correction below divides by
+//                  grdsf(nu)^2, about 1.6e-5 at the image corners, so a float
+//                  FFT's rounding would be amplified ~6e4x there.
 //   k_stokes       ZeroToCentre2DShift + StokesConverter (PostIFFTStokesConverter.cu:
 //                  42-180, including the m-axis flip of :172) + casagridsf taper
 //                  correction (CasaGridSF.cu:174-199) + SincCorrector
-//                  (SincCorrector.cu:29-58) fused into one pass; the two
-//                  corrections are separable and come from per-axis factor
-//                  tables computed in FP64.
+//                  (SincCorrector.cu:29-58) fused into one pass in FP64; the
+//                  two corrections are separable and come from per-axis factor
+//                  tables.  Output float (the reference's FinalImage type).
 #include "fft_plans.cuh"
 #include "mtb_internal.cuh"
 
 namespace mtb {
 
-__global__ void k_pre_ifft(const float2 *__restrict__ grid, const float2 *__restrict__ lo, float2 *__restrict__ out,
+__global__ void k_pre_ifft(const float2 *__restrict__ grid, const float2 *__restrict__ lo, double2 *__restrict__ out,
                            int nx, int ny, int P) {
     const size_t plane = (size_t)nx * ny;
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < plane * P;
@@ -26,76 +30,78 @@ __global__ void k_pre_ifft(const float2 *__restrict__ grid, const float2 *__rest
         int p = (int)(i % P);
         size_t c = i / P;
         int y = (int)(c / nx), x = (int)(c - (size_t)y * nx);
-        float2 v = grid[i];
+        float2 h = grid[i];
+        double2 v = make_double2((double)h.x, (double)h.y);
         if (lo) {
             float2 e = lo[i];
-            v.x += e.x;
-            v.y += e.y;
+            v.x += (double)e.x;
+            v.y += (double)e.y;
         }
         out[(size_t)p * plane + (size_t)origin_to_corner(y, ny) * nx + origin_to_corner(x, nx)] = v;
     }
 }
 
 // f[j] = invsinc((j - n/2)/(n*s)) / grdsf(|j - n/2| / (n/2)) per axis
-__global__ void k_axis_factors(float *fx, int nx, float *fy, int ny, int s) {
+__global__ void k_axis_factors(double *fx, int nx, double *fy, int ny, int s) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     int n = (i < nx) ? nx : ny;
-    float *f = (i < nx) ? fx : fy;
+    double *f = (i < nx) ? fx : fy;
     int j = (i < nx) ? i : i - nx;
     if (i >= nx + ny) return;
     double nu = fabs((double)(j - n / 2) / (double)(n / 2));
     double x = (double)(j - n / 2) / ((double)n * (double)s);
     double inv = (x == 0.0) ? 1.0 : (M_PI * x) / sin(M_PI * x);
-    f[j] = (float)(inv / grdsf(nu));
+    f[j] = inv / grdsf(nu);
 }
 
 // One output pixel (all Stokes planes) per thread.  Output row j holds the
 // shifted row ny-1-j; shifted (y, x) reads unshifted (centre_to_origin(y),
 // centre_to_origin(x)) of the FFT output.
 template <int P, int CIRC>
-__global__ void k_stokes(const float2 *__restrict__ img, const float *__restrict__ norm, const float *__restrict__ fx,
-                         const float *__restrict__ fy, float *__restrict__ out, int nx, int ny) {
+__global__ void k_stokes(const double2 *__restrict__ img, const float *__restrict__ norm,
+                         const double *__restrict__ fx, const double *__restrict__ fy, float *__restrict__ out,
+                         int nx, int ny) {
     const size_t plane = (size_t)nx * ny;
-    float nrm[P];
+    double nrm[P];
 #pragma unroll
-    for (int p = 0; p < P; p++) nrm[p] = norm[p];
+    for (int p = 0; p < P; p++) nrm[p] = (double)norm[p];
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < plane; i += (size_t)gridDim.x * blockDim.x) {
         int j = (int)(i / nx), x = (int)(i - (size_t)j * nx);
         int y = ny - 1 - j;
         size_t src = (size_t)centre_to_origin(y, ny) * nx + centre_to_origin(x, nx);
-        float2 d[P];
+        double2 d[P];
 #pragma unroll
         for (int p = 0; p < P; p++) {
             d[p] = img[(size_t)p * plane + src];
             d[p].x /= nrm[p];
             d[p].y /= nrm[p];
         }
-        float st[P];
+        double st[P];
         if (P == 4 && !CIRC) {
-            st[0] = (d[0].x + d[3].x) * 0.5f;
-            st[1] = (d[0].x - d[3].x) * 0.5f;
-            st[2] = (d[1].x + d[2].x) * 0.5f;
-            st[3] = (d[1].y - d[2].y) * 0.5f;
+            st[0] = (d[0].x + d[3].x) * 0.5;
+            st[1] = (d[0].x - d[3].x) * 0.5;
+            st[2] = (d[1].x + d[2].x) * 0.5;
+            st[3] = (d[1].y - d[2].y) * 0.5;
         } else if (P == 4) {
-            st[0] = (d[0].x + d[3].x) * 0.5f;
-            st[1] = (d[1].x + d[2].x) * 0.5f;
-            st[2] = (d[2].y - d[1].y) * 0.5f;
-            st[3] = (d[0].x - d[3].x) * 0.5f;
+            st[0] = (d[0].x + d[3].x) * 0.5;
+            st[1] = (d[1].x + d[2].x) * 0.5;
+            st[2] = (d[2].y - d[1].y) * 0.5;
+            st[3] = (d[0].x - d[3].x) * 0.5;
         } else if (P == 2) {
-            st[0] = (d[0].x + d[1].x) * 0.5f;
-            st[P - 1] = (d[0].x - d[1].x) * 0.5f;
+            st[0] = (d[0].x + d[1].x) * 0.5;
+            st[P - 1] = (d[0].x - d[1].x) * 0.5;
         } else {
             st[0] = d[0].x;
         }
-        float f = fy[j] * fx[x];
+        double f = fy[j] * fx[x];
 #pragma unroll
-        for (int p = 0; p < P; p++) out[(size_t)p * plane + i] = st[p] * f;
+        for (int p = 0; p < P; p++) out[(size_t)p * plane + i] = (float)(st[p] * f);
     }
 }
 
 struct FSpace {
-    float2 *planes;
-    float *fx, *fy;
+    double2 *planes;
+    double *fx, *fy;
     void *work;
     size_t work_bytes;
 };
@@ -103,11 +109,11 @@ struct FSpace {
 static int carve_fin(const mtb_finalize_params *p, void *ws, size_t bytes, FSpace *f, size_t *need) {
     cufftHandle h;
     size_t fw = 0;
-    MTB_TRY(fft_plan(CUFFT_C2C, p->ny, p->nx, p->npol, &h, &fw));
+    MTB_TRY(fft_plan(CUFFT_Z2Z, p->ny, p->nx, p->npol, &h, &fw));
     Arena A(ws, bytes);
-    f->planes = A.take<float2>((size_t)p->nx * p->ny * p->npol);
-    f->fx = A.take<float>(p->nx);
-    f->fy = A.take<float>(p->ny);
+    f->planes = A.take<double2>((size_t)p->nx * p->ny * p->npol);
+    f->fx = A.take<double>(p->nx);
+    f->fy = A.take<double>(p->ny);
     f->work = A.take<char>(fw ? fw : 1);
     f->work_bytes = fw;
     *need = A.used;
@@ -148,10 +154,10 @@ extern "C" int mtb_finalize(const mtb_finalize_params *p, const void *d_grid, co
     size_t cells = (size_t)nx * ny * P;
     int blocks = (int)std::min<size_t>((cells + 255) / 256, (size_t)sm_count() * 16);
     k_pre_ifft<<<blocks, 256, 0, st>>>((const float2 *)d_grid, (const float2 *)d_grid_lo, f.planes, nx, ny, P);
-    MTB_CUDA_TRY(cudaGetLastError());
-    MTB_TRY(fft_exec(CUFFT_C2C, ny, nx, P, f.planes, f.planes, CUFFT_INVERSE, f.work, f.work_bytes, st));
+    MTB_LAUNCHED();
+    MTB_TRY(fft_exec(CUFFT_Z2Z, ny, nx, P, f.planes, f.planes, CUFFT_INVERSE, f.work, f.work_bytes, st));
     k_axis_factors<<<(nx + ny + 255) / 256, 256, 0, st>>>(f.fx, nx, f.fy, ny, p->sampling);
-    MTB_CUDA_TRY(cudaGetLastError());
+    MTB_LAUNCHED();
     size_t px = (size_t)nx * ny;
     blocks = (int)std::min<size_t>((px + 255) / 256, (size_t)sm_count() * 16);
     bool circ = p->pol_type == MTB_POL_CIRCULAR;
@@ -163,6 +169,6 @@ extern "C" int mtb_finalize(const mtb_finalize_params *p, const void *d_grid, co
     } else {
         k_stokes<1, 0><<<blocks, 256, 0, st>>>(f.planes, d_normalizer, f.fx, f.fy, d_image, nx, ny);
     }
-    MTB_CUDA_TRY(cudaGetLastError());
+    MTB_LAUNCHED();
     return MTB_OK;
 }

@@ -83,8 +83,9 @@ __global__ void k_preprocess(int R, const float *__restrict__ uvw, const float *
         if (grid) {
             double u = (double)uvw[r], v = (double)uvw[(size_t)R + r], w = (double)uvw[2 * (size_t)R + r];
             double f = (double)freq[r];
-            bool neg = false;
-            if (w < 0.0) { u = -u; v = -v; neg = true; }
+            // TakeConjugateIndicator is set before the bounds test, so a
+            // rejected w < 0 record still reports -1 (WProjPreProcessUVW.cu:170-175)
+            if (w < 0.0) { u = -u; v = -v; m = 2; }
             // WProjPreProcessUVW.cu:181-182
             double wp = round(sqrt(fabs(__ddiv_rn(__dmul_rn(w, f), w_inc))));
             if (!(wp == wp)) wp = 0.0;
@@ -110,7 +111,7 @@ __global__ void k_preprocess(int R, const float *__restrict__ uvw, const float *
                 cs = (double)conv_sums[(size_t)k * T * T + oy * T + ox];
                 ci += oy * S * S * T + ox * S * S;
                 out = make_int4(cx, cy, ci, S);
-                m = 1 | (neg ? 2 : 0);
+                m |= 1;
             }
         }
         pos[r] = out;
@@ -597,7 +598,7 @@ static int launch_one(const GridArgs &a, const Launch &L, cudaStream_t st) {
     if (per_sm < 1) return MTB_ERR_BAD_SHAPE;
     int blocks = per_sm * sm_count();
     kern<<<blocks, L.threads, L.smem, st>>>(a);
-    MTB_CUDA_TRY(cudaGetLastError());
+    MTB_LAUNCHED();
     return MTB_OK;
 }
 
@@ -626,9 +627,9 @@ static int run_grid(const mtb_grid_params *p, const GridPlan &plan, const float2
     k_preprocess<P><<<blocks, 256, 0, st>>>(R, uvw, freq, weights, flags, conv_info, conv_sums, p->wplanes,
                                             p->w_sq_increment, p->sampling, T, p->nx, p->ny, p->u_increment,
                                             p->v_increment, s.pos, s.meta, s.norm_acc, nullptr);
-    MTB_CUDA_TRY(cudaGetLastError());
+    MTB_LAUNCHED();
     k_compress<<<blocks, 256, 0, st>>>(R, p->nx, s.pos, s.meta, s.keys, s.iota, plan.bt, s.stats);
-    MTB_CUDA_TRY(cudaGetLastError());
+    MTB_LAUNCHED();
     int end_bit = 24;
     while ((1 << (end_bit - 24)) < plan.bt.n) end_bit++;
     // the kNoKey sentinel needs every bit: sort the full 32 bits
@@ -639,16 +640,16 @@ static int run_grid(const mtb_grid_params *p, const GridPlan &plan, const float2
     cb = s.cub_bytes;
     MTB_CUDA_TRY(cub::DeviceScan::ExclusiveSum(s.cub, cb, s.counts, s.run_start, R, st));
     k_chunk_counts<<<blocks, 256, 0, st>>>(s.ukeys, s.counts, s.num_runs, R, plan.chunk, s.nchunks);
-    MTB_CUDA_TRY(cudaGetLastError());
+    MTB_LAUNCHED();
     cb = s.cub_bytes;
     MTB_CUDA_TRY(cub::DeviceScan::ExclusiveSum(s.cub, cb, s.nchunks, s.item_start, R, st));
     k_make_items<<<blocks, 256, 0, st>>>(s.ukeys, s.counts, s.run_start, s.item_start, s.nchunks, s.num_runs,
                                          plan.chunk, s.items);
-    MTB_CUDA_TRY(cudaGetLastError());
+    MTB_LAUNCHED();
     k_bucket_bounds<<<blocks, 256, 0, st>>>(s.items, s.item_start, s.nchunks, s.num_runs, s.bounds, plan.bt.n);
-    MTB_CUDA_TRY(cudaGetLastError());
+    MTB_LAUNCHED();
     k_gather<P><<<blocks, 256, 0, st>>>(R, s.skeys, s.sidx, s.pos, s.meta, vis, weights, flags, s.wpos, s.wvis);
-    MTB_CUDA_TRY(cudaGetLastError());
+    MTB_LAUNCHED();
     (void)end_bit;
 
     GridArgs a;
@@ -662,6 +663,7 @@ static int run_grid(const mtb_grid_params *p, const GridPlan &plan, const float2
     a.grid_lo = grid_lo;
     a.nx = p->nx;
     a.ny = p->ny;
+    if (p->gridder_start_event) MTB_CUDA_TRY(cudaEventRecord((cudaEvent_t)p->gridder_start_event, st));
     for (int b = 0; b < plan.bt.n; b++) {
         int M = plan.bt.M[b];
         if (M <= 0) continue;
@@ -672,8 +674,9 @@ static int run_grid(const mtb_grid_params *p, const GridPlan &plan, const float2
         Launch L = launch_shape(M, P, a.tile);
         MTB_TRY(launch_bucket<P>(a, L, st));
     }
+    if (p->gridder_end_event) MTB_CUDA_TRY(cudaEventRecord((cudaEvent_t)p->gridder_end_event, st));
     k_finish<<<1, 32, 0, st>>>(P, s.norm_acc, normalizer, s.stats, stats);
-    MTB_CUDA_TRY(cudaGetLastError());
+    MTB_LAUNCHED();
     return MTB_OK;
 }
 
@@ -787,11 +790,11 @@ extern "C" int mtb_preprocess_uvw(const mtb_grid_params *p, const int *d_conv_in
     else if (p->npol == 2) MTB_PRE(2);
     else MTB_PRE(4);
 #undef MTB_PRE
-    MTB_CUDA_TRY(cudaGetLastError());
+    MTB_LAUNCHED();
     k_compress<<<blocks, 256, 0, st>>>(R, p->nx, s.pos, s.meta, s.keys, s.iota, plan.bt, s.stats);
-    MTB_CUDA_TRY(cudaGetLastError());
+    MTB_LAUNCHED();
     k_ref_outputs<<<blocks, 256, 0, st>>>(R, p->nx, s.pos, s.meta, (int4 *)d_gridding_data, d_conv_index,
                                           d_to_grid, d_to_compress, d_support, d_take_conjugate);
-    MTB_CUDA_TRY(cudaGetLastError());
+    MTB_LAUNCHED();
     return MTB_OK;
 }

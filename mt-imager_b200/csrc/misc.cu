@@ -1,6 +1,16 @@
 // Status strings, version and cache release of the C ABI.
+#include <algorithm>
+#include <atomic>
+
 #include "fft_plans.cuh"
 #include "mtb_internal.cuh"
+
+namespace mtb {
+static std::atomic<unsigned long long> g_launches{0};
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+}  // namespace mtb
+
+extern "C" unsigned long long mtb_kernel_launch_count(void) { return mtb::g_launches.load(); }
 
 extern "C" const char *mtb_status_string(int status) {
     switch (status) {
@@ -20,3 +30,60 @@ extern "C" const char *mtb_status_string(int status) {
 extern "C" int mtb_version(void) { return 100; }
 
 extern "C" void mtb_release_caches(void) { mtb::fft_release_all(); }
+
+// FP32 FMA-pipe calibration: a register-resident chain of packed f32x2 FMAs
+// (fma.rn.f32x2, sm_100a) over every SM, timed with events on `stream`.  It
+// gives the denominator of the gridder's FP32 roofline fraction on the GPU the
+// measurement runs on.  The result is written through a volatile store so the
+// chain cannot be removed.
+namespace mtb {
+__device__ __forceinline__ unsigned long long f2pack(float a, float b) {
+    unsigned long long r;
+    asm("mov.b64 %0, {%1,%2};" : "=l"(r) : "f"(a), "f"(b));
+    return r;
+}
+__global__ void k_ffma2_chain(float *sink, int iters, float seed) {
+    unsigned long long acc[8];
+#pragma unroll
+    for (int j = 0; j < 8; j++) acc[j] = f2pack(seed + j, seed - j);
+    const unsigned long long m = f2pack(0.999999f, 1.000001f), c = f2pack(1e-7f, -1e-7f);
+    for (int i = 0; i < iters; i++) {
+#pragma unroll
+        for (int j = 0; j < 8; j++) asm volatile("fma.rn.f32x2 %0, %0, %1, %2;" : "+l"(acc[j]) : "l"(m), "l"(c));
+    }
+    float t = 0.f;
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+        float lo, hi;
+        asm("mov.b64 {%0,%1}, %2;" : "=f"(lo), "=f"(hi) : "l"(acc[j]));
+        t += lo + hi;
+    }
+    if (t == 12345.678f) *(volatile float *)sink = t;
+}
+}  // namespace mtb
+
+extern "C" int mtb_calibrate_fp32(double *tflops, mtb_stream_t stream) {
+    if (!tflops) return MTB_ERR_NULL;
+    cudaStream_t st = (cudaStream_t)stream;
+    float *sink = nullptr;
+    cudaEvent_t a, b;
+    MTB_CUDA_TRY(cudaEventCreate(&a));
+    MTB_CUDA_TRY(cudaEventCreate(&b));
+    const int threads = 256, blocks = mtb::sm_count() * 8, iters = 1 << 16;
+    double best = 0.0;
+    for (int rep = 0; rep < 4; rep++) {
+        MTB_CUDA_TRY(cudaEventRecord(a, st));
+        mtb::k_ffma2_chain<<<blocks, threads, 0, st>>>(sink, iters, 1.0f + rep);
+        MTB_LAUNCHED();
+        MTB_CUDA_TRY(cudaEventRecord(b, st));
+        MTB_CUDA_TRY(cudaEventSynchronize(b));
+        float ms = 0.f;
+        MTB_CUDA_TRY(cudaEventElapsedTime(&ms, a, b));
+        double flops = 2.0 * 2.0 * 8.0 * (double)iters * threads * blocks;
+        if (rep > 0 && ms > 0) best = std::max(best, flops / (ms * 1e-3) / 1e12);
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    *tflops = best;
+    return MTB_OK;
+}

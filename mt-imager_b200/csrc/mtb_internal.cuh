@@ -13,6 +13,16 @@ namespace mtb {
         if (_e != cudaSuccess) return MTB_ERR_CUDA;          \
     } while (0)
 
+// every launch of this library's own kernels goes through here so the
+// process-wide launch count stays exact
+void count_launch();
+#define MTB_LAUNCHED()                                       \
+    do {                                                     \
+        ::mtb::count_launch();                               \
+        cudaError_t _e = cudaGetLastError();                 \
+        if (_e != cudaSuccess) return MTB_ERR_CUDA;          \
+    } while (0)
+
 #define MTB_TRY(expr)                                        \
     do {                                                     \
         int _s = (expr);                                     \

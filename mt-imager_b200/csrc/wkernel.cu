@@ -208,7 +208,7 @@ static int launch_screen_fft(const WGeom &g, const WSpace &w, int k0, int nb, cu
     if (blocks > cap) blocks = cap;
     k_wscreen<<<blocks, 256, 0, st>>>(w.planes, nb, k0, g.St, g.ps, g.total_l / (double)g.St,
                                       g.total_m / (double)g.St, g.w_inc);
-    MTB_CUDA_TRY(cudaGetLastError());
+    MTB_LAUNCHED();
     return fft_exec(CUFFT_Z2Z, g.ps, g.ps, nb, w.planes, w.planes, CUFFT_FORWARD, w.fftwork,
                     w.fftbytes, st);
 }
@@ -260,10 +260,10 @@ extern "C" int mtb_wkernel_build(const mtb_wkernel_params *p, void *d_workspace,
         MTB_TRY(launch_screen_fft(g, w, k0, n, st));
         if (k0 == 0) {
             k_copy_divisor<<<1, 1, 0, st>>>(w.planes, w.divisor);
-            MTB_CUDA_TRY(cudaGetLastError());
+            MTB_LAUNCHED();
         }
         k_support_find<<<n, 256, 0, st>>>(w.planes, k0, g.ps, g.s, w.divisor, g.cap, w.supports);
-        MTB_CUDA_TRY(cudaGetLastError());
+        MTB_LAUNCHED();
     }
     std::vector<int> sup(g.nw);
     double2 div;
@@ -295,12 +295,12 @@ extern "C" int mtb_wkernel_build(const mtb_wkernel_params *p, void *d_workspace,
         dim3 grid(64, n < 65535 ? n : 65535);
         k_reorganize<<<grid, 256, 0, st>>>(w.planes, n, k0, g.ps, g.s, g.T, w.conv_info, w.divisor,
                                            (float2 *)d_table);
-        MTB_CUDA_TRY(cudaGetLastError());
+        MTB_LAUNCHED();
     }
     int warps = g.nw * g.T * g.T;
     k_conv_sums<<<(warps * 32 + 255) / 256, 256, 0, st>>>((const float2 *)d_table, w.conv_info, g.nw, g.T,
                                                          d_conv_sums);
-    MTB_CUDA_TRY(cudaGetLastError());
+    MTB_LAUNCHED();
     // the host copy of conv_info is read by the caller right away; make sure the
     // H2D above has consumed it before returning
     MTB_CUDA_TRY(cudaStreamSynchronize(st));

@@ -21,7 +21,7 @@ MTB_POL_CIRCULAR = 1
 EXPORTS = (
     "mtb_wkernel_query", "mtb_wkernel_build", "mtb_grid_workspace_size", "mtb_grid", "mtb_preprocess_uvw",
     "mtb_finalize_workspace_size", "mtb_finalize", "mtb_status_string", "mtb_version",
-    "mtb_release_caches",
+    "mtb_release_caches", "mtb_kernel_launch_count", "mtb_calibrate_fp32",
 )
 
 
@@ -50,7 +50,8 @@ class GridParams(ctypes.Structure):
     _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("npol", ctypes.c_int), ("sampling", ctypes.c_int),
                 ("wplanes", ctypes.c_int), ("u_increment", ctypes.c_double), ("v_increment", ctypes.c_double),
                 ("w_sq_increment", ctypes.c_double), ("initialize_output", ctypes.c_int), ("tile", ctypes.c_int),
-                ("support_bucket", ctypes.c_int), ("max_chunk", ctypes.c_int)]
+                ("support_bucket", ctypes.c_int), ("max_chunk", ctypes.c_int),
+                ("gridder_start_event", ctypes.c_void_p), ("gridder_end_event", ctypes.c_void_p)]
 
 
 class GridStats(ctypes.Structure):
@@ -90,6 +91,9 @@ def load(path: str = LIB_PATH):
     L.mtb_version.argtypes = []
     L.mtb_release_caches.restype = None
     L.mtb_release_caches.argtypes = []
+    L.mtb_kernel_launch_count.restype = ctypes.c_ulonglong
+    L.mtb_kernel_launch_count.argtypes = []
+    L.mtb_calibrate_fp32.argtypes = [ctypes.POINTER(ctypes.c_double), p]
     _lib = L
     return L
 

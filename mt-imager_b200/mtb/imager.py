@@ -102,6 +102,9 @@ class WProjectionImager:
         self.stats = torch.zeros(4, dtype=torch.int64, device=self.device)
         self._ws = None
         self._fin_ws = None
+        # optional (start, end) torch.cuda.Event pair recorded around the
+        # gridder kernels of every mtb_grid call
+        self.gridder_events = None
         self._fresh = True
 
     # -- WProjectionConvFunction
@@ -112,9 +115,13 @@ class WProjectionImager:
 
     def grid_params(self, initialize: bool) -> L.GridParams:
         k = self.build_kernels()
-        return L.GridParams(self.nx, self.ny, self.npol, self.params.sampling, self.params.wplanes,
-                            k.info.u_increment, k.info.v_increment, k.info.w_sq_increment, int(initialize),
-                            self.tuning["tile"], self.tuning["support_bucket"], self.tuning["max_chunk"])
+        gp = L.GridParams(self.nx, self.ny, self.npol, self.params.sampling, self.params.wplanes,
+                          k.info.u_increment, k.info.v_increment, k.info.w_sq_increment, int(initialize),
+                          self.tuning["tile"], self.tuning["support_bucket"], self.tuning["max_chunk"])
+        if self.gridder_events is not None:
+            gp.gridder_start_event = self.gridder_events[0].cuda_event
+            gp.gridder_end_event = self.gridder_events[1].cuda_event
+        return gp
 
     def _workspace(self, nrec, gp):
         need = ctypes.c_size_t(0)

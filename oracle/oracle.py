@@ -83,6 +83,21 @@ def lib():
     return _lib
 
 
+def port():
+    """FP32 OpenMP transcription of the reference's gridding (cpu_port.c),
+    the CPU baseline bench.py times."""
+    global _port
+    if _port is None:
+        path = _compile(PORT_SRC, os.path.join(BUILD, "libcpu_port.so"), extra=("-O3", "-march=native"))
+        P = ctypes.CDLL(path)
+        i, p, f = ctypes.c_int, ctypes.c_void_p, ctypes.c_float
+        P.port_threads.restype = i
+        P.port_grid_chunk.restype = i
+        P.port_grid_chunk.argtypes = [i, i, p, p, p, p, p, i, f, p, p, p, i, i, i, f, f, p, p, p]
+        _port = P
+    return _port
+
+
 def _p(a):
     return a.ctypes.data_as(ctypes.c_void_p)
 
