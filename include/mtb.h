@@ -126,6 +126,9 @@ typedef struct mtb_grid_params {
     int tile;                /* 0: default; grid tile edge owned by one thread block   */
     int support_bucket;      /* 0: default; supports are grouped in buckets this wide  */
     int max_chunk;           /* 0: default; most records one block grids in one pass   */
+    int merge;               /* 0: default; 1: cell flushes go to a shared-memory tile
+                                window merged once per work item; 2: cell flushes merge
+                                straight into the grid                                 */
     void *gridder_start_event; /* cudaEvent_t or NULL: recorded before the gridder kernels */
     void *gridder_end_event;   /* cudaEvent_t or NULL: recorded after them (the span of the
                                   ConvolutionGridder operator, like GPUSubmissionData's

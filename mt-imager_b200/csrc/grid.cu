@@ -211,9 +211,10 @@ __global__ void k_make_items(const unsigned *__restrict__ ukeys, const int *__re
 // Per bucket [begin, end) of the item list and the total item count.
 __global__ void k_bucket_bounds(const int4 *__restrict__ items, const int *__restrict__ item_start,
                                 const int *__restrict__ nchunks, const int *__restrict__ num_runs,
-                                int *__restrict__ bounds, int nb) {
+                                int *__restrict__ bounds, int nb, int *__restrict__ n_items) {
     int nr = *num_runs;
     int total = nr > 0 ? item_start[nr - 1] + nchunks[nr - 1] : 0;
+    if (blockIdx.x == 0 && threadIdx.x == 0) *n_items = total;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
         int b = (int)((unsigned)items[i].z >> 24);
         int bp = i > 0 ? (int)((unsigned)items[i - 1].z >> 24) : -1;
@@ -475,6 +476,177 @@ __global__ void __launch_bounds__(KMAX >= 8 ? 576 : 1024) k_grid(GridArgs a) {
     }
 }
 
+// ------------------------------------------------------- direct gridder --
+// One persistent launch for every support bucket.  A block of kG2Threads
+// threads takes a work item (up to max_chunk records of one (support bucket,
+// tile) bin, original record order) and walks the M x M support box in passes
+// of kG2Threads*KS slots: slot q -> (a, b) = (q % M, q / M).  For a record with
+// corner (cx, cy) the slot touches cell (cx + sx, cy + sy), sx = (a - cx) mod M,
+// sy = (b - cy) mod M (Romein's assignment: a slot keeps its cell while the
+// record moves less than a cell, and no two slots of a pass share a cell).
+// Each slot accumulates V * C for all polarisations in registers with packed
+// f32x2 FMAs and merges into the grid (two-float, vector atomics) only when its
+// cell changes and at the end of a pass.  The next record's kernel values are
+// loaded while the current record's FMAs run.
+static const int kG2Threads = 256;
+static const int kG2Stage = 128;
+
+struct Grid2Args {
+    const int4 *items;
+    const int *n_items;
+    int *counter;
+    const int4 *wpos;
+    const float2 *wvis;
+    const float2 *table;
+    float *grid;
+    float *grid_lo;
+    int nx;
+    BucketTable bt;
+};
+
+typedef unsigned long long u64;
+__device__ __forceinline__ u64 pk2(float a, float b) {
+    u64 r;
+    asm("mov.b64 %0, {%1,%2};" : "=l"(r) : "f"(a), "f"(b));
+    return r;
+}
+__device__ __forceinline__ float2 upk2(u64 v) {
+    float2 r;
+    asm("mov.b64 {%0,%1}, %2;" : "=f"(r.x), "=f"(r.y) : "l"(v));
+    return r;
+}
+__device__ __forceinline__ void ffma2(u64 &acc, u64 a, u64 b) {
+    asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(acc) : "l"(a), "l"(b));
+}
+
+template <int P>
+__device__ __forceinline__ void flush2(float *grid, float *lo, int cell, const u64 *acc) {
+    float v[2 * P];
+#pragma unroll
+    for (int p = 0; p < P; p++) {
+        float2 f = upk2(acc[p]);
+        v[2 * p] = f.x;
+        v[2 * p + 1] = f.y;
+    }
+    size_t g = (size_t)cell * 2 * P;
+    merge_cell<P>(grid + g, lo ? lo + g : nullptr, v);
+}
+
+template <int P, int KS>
+__global__ void __launch_bounds__(kG2Threads, (KS <= 2) ? 4 : 2) k_grid2(Grid2Args a) {
+    __shared__ int4 s_rec[kG2Stage];              // {grid index of corner, rxm | rym << 16, conv, S}
+    __shared__ ulonglong2 s_v[kG2Stage][P];       // per pol {(re, im), (-im, re)}
+    __shared__ int s_item;
+    const int t = threadIdx.x;
+    const int nitems = *a.n_items;
+    for (;;) {
+        __syncthreads();
+        if (t == 0) s_item = atomicAdd(a.counter, 1);
+        __syncthreads();
+        const int v = s_item;
+        if (v >= nitems) break;
+        const int4 it = a.items[v];
+        const int M = a.bt.M[(unsigned)it.z >> 24];
+        const int MM = M * M;
+        for (int pass0 = 0; pass0 < MM; pass0 += kG2Threads * KS) {
+            int sa[KS], sb[KS], last[KS];
+            u64 acc[KS][P];
+#pragma unroll
+            for (int j = 0; j < KS; j++) {
+                int q = pass0 + j * kG2Threads + t;
+                // an idle slot (q >= M*M) gets a = 2M: after one wrap sx is
+                // still >= M >= S, so it never touches a cell
+                sa[j] = (q < MM) ? q % M : 2 * M;
+                sb[j] = (q < MM) ? q / M : 0;
+                last[j] = -1;
+#pragma unroll
+                for (int p = 0; p < P; p++) acc[j][p] = 0ull;
+            }
+            for (int r0 = 0; r0 < it.y; r0 += kG2Stage) {
+                const int nrec = min(kG2Stage, it.y - r0);
+                __syncthreads();
+                for (int i = t; i < nrec; i += kG2Threads) {
+                    int4 q = a.wpos[it.x + r0 + i];
+                    int rxm = (M - q.x % M) % M, rym = (M - q.y % M) % M;
+                    s_rec[i] = make_int4(q.y * a.nx + q.x, rxm | (rym << 16), q.z, q.w);
+                }
+                for (int i = t; i < nrec * P; i += kG2Threads) {
+                    float2 vv = a.wvis[(size_t)(it.x + r0) * P + i];
+                    s_v[i / P][i % P] = make_ulonglong2(pk2(vv.x, vv.y), pk2(-vv.y, vv.x));
+                }
+                __syncthreads();
+                // software pipeline: the geometry and kernel values of record
+                // i+1 are fetched before record i is accumulated
+                int cellN[KS];
+                float2 cN[KS];
+                auto fetch = [&](int i) {
+                    const int4 rec = s_rec[i];
+                    const int S = rec.w;
+#pragma unroll
+                    for (int j = 0; j < KS; j++) {
+                        int sx = sa[j] + (rec.y & 0xFFFF);
+                        sx -= (sx >= M) ? M : 0;
+                        int sy = sb[j] + (rec.y >> 16);
+                        sy -= (sy >= M) ? M : 0;
+                        bool ok = (sx < S) && (sy < S);
+                        cellN[j] = ok ? rec.x + sy * a.nx + sx : -1;
+                        cN[j] = ok ? __ldg(&a.table[rec.z + sy * S + sx]) : make_float2(0.f, 0.f);
+                    }
+                };
+                fetch(0);
+                for (int i = 0; i < nrec; i++) {
+                    int cell[KS];
+                    float2 c[KS];
+#pragma unroll
+                    for (int j = 0; j < KS; j++) {
+                        cell[j] = cellN[j];
+                        c[j] = cN[j];
+                    }
+                    if (i + 1 < nrec) fetch(i + 1);
+                    u64 vp[P], wp[P];
+#pragma unroll
+                    for (int p = 0; p < P; p++) {
+                        ulonglong2 q = s_v[i][p];
+                        vp[p] = q.x;
+                        wp[p] = q.y;
+                    }
+#pragma unroll
+                    for (int j = 0; j < KS; j++) {
+                        if (cell[j] < 0) continue;
+                        if (cell[j] != last[j]) {
+                            if (last[j] >= 0) flush2<P>(a.grid, a.grid_lo, last[j], acc[j]);
+                            last[j] = cell[j];
+#pragma unroll
+                            for (int p = 0; p < P; p++) acc[j][p] = 0ull;
+                        }
+                        const u64 cr = pk2(c[j].x, c[j].x), ci = pk2(c[j].y, c[j].y);
+                        // ConvolutionGridder.cu:153-181: to += vis * wt (no conjugate)
+#pragma unroll
+                        for (int p = 0; p < P; p++) {
+                            ffma2(acc[j][p], cr, vp[p]);
+                            ffma2(acc[j][p], ci, wp[p]);
+                        }
+                    }
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < KS; j++)
+                if (last[j] >= 0) flush2<P>(a.grid, a.grid_lo, last[j], acc[j]);
+        }
+    }
+}
+
+template <int P, int KS>
+static int launch_grid2(const Grid2Args &a, cudaStream_t st) {
+    auto kern = k_grid2<P, KS>;
+    int per_sm = 0;
+    MTB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kG2Threads, 0));
+    if (per_sm < 1) return MTB_ERR_BAD_SHAPE;
+    kern<<<per_sm * sm_count(), kG2Threads, 0, st>>>(a);
+    MTB_LAUNCHED();
+    return MTB_OK;
+}
+
 // ------------------------------------------------------------ host side --
 struct GridPlan {
     BucketTable bt;
@@ -488,7 +660,7 @@ struct GridSpace {
     unsigned *keys, *skeys;
     int *iota, *sidx;
     unsigned *ukeys;
-    int *counts, *run_start, *nchunks, *item_start, *num_runs;
+    int *counts, *run_start, *nchunks, *item_start, *num_runs, *n_items;
     int4 *items;
     int *bounds, *counters;
     int4 *wpos;
@@ -524,6 +696,7 @@ static void carve_grid(Arena &A, int R, int P, int chunk, GridSpace *s) {
     s->nchunks = A.take<int>(n);
     s->item_start = A.take<int>(n);
     s->num_runs = A.take<int>(1);
+    s->n_items = A.take<int>(1);
     s->items = A.take<int4>(nitems);
     s->bounds = A.take<int>(2 * kMaxBuckets);
     s->counters = A.take<int>(kMaxBuckets);
@@ -542,6 +715,7 @@ static int check_params(const mtb_grid_params *p) {
     if ((size_t)p->nx * p->ny > ((size_t)1 << 31)) return MTB_ERR_BAD_SHAPE;
     if (!(p->u_increment > 0.0) || !(p->v_increment > 0.0) || !(p->w_sq_increment > 0.0)) return MTB_ERR_BAD_PARAM;
     if (p->tile < 0 || p->support_bucket < 0 || p->max_chunk < 0) return MTB_ERR_BAD_PARAM;
+    if (p->merge < 0 || p->merge > 2) return MTB_ERR_BAD_PARAM;
     return MTB_OK;
 }
 
@@ -570,7 +744,7 @@ struct Launch {
     size_t smem;
 };
 
-static Launch launch_shape(int M, int P, int tile) {
+static Launch launch_shape(int M, int P, int tile, int merge) {
     Launch L;
     if (M <= 16) L.kmax = 1;
     else if (M <= 32) L.kmax = 2;
@@ -583,7 +757,7 @@ static Launch launch_shape(int M, int P, int tile) {
     size_t stage = kStage * (sizeof(int4) + 2 * P * sizeof(float));
     size_t W = (size_t)tile + M - 1;
     size_t wbytes = ((W * W * 2 * P + 3) & ~(size_t)3) * sizeof(float);
-    L.window = (L.nbands == 1) && (wbytes + stage <= kWindowSmemLimit);
+    L.window = (merge == 1) && (L.nbands == 1) && (wbytes + stage <= kWindowSmemLimit);
     L.smem = (L.window ? wbytes : 0) + stage;
     return L;
 }
@@ -646,7 +820,8 @@ static int run_grid(const mtb_grid_params *p, const GridPlan &plan, const float2
     k_make_items<<<blocks, 256, 0, st>>>(s.ukeys, s.counts, s.run_start, s.item_start, s.nchunks, s.num_runs,
                                          plan.chunk, s.items);
     MTB_LAUNCHED();
-    k_bucket_bounds<<<blocks, 256, 0, st>>>(s.items, s.item_start, s.nchunks, s.num_runs, s.bounds, plan.bt.n);
+    k_bucket_bounds<<<blocks, 256, 0, st>>>(s.items, s.item_start, s.nchunks, s.num_runs, s.bounds, plan.bt.n,
+                                            s.n_items);
     MTB_LAUNCHED();
     k_gather<P><<<blocks, 256, 0, st>>>(R, s.skeys, s.sidx, s.pos, s.meta, vis, weights, flags, s.wpos, s.wvis);
     MTB_LAUNCHED();
@@ -664,6 +839,27 @@ static int run_grid(const mtb_grid_params *p, const GridPlan &plan, const float2
     a.nx = p->nx;
     a.ny = p->ny;
     if (p->gridder_start_event) MTB_CUDA_TRY(cudaEventRecord((cudaEvent_t)p->gridder_start_event, st));
+    if (p->merge != 1) {
+        Grid2Args g2;
+        g2.items = s.items;
+        g2.n_items = s.n_items;
+        g2.counter = s.counters;
+        g2.wpos = s.wpos;
+        g2.wvis = s.wvis;
+        g2.table = table;
+        g2.grid = grid;
+        g2.grid_lo = grid_lo;
+        g2.nx = p->nx;
+        g2.bt = plan.bt;
+        int Mmax = 0;
+        for (int b = 0; b < plan.bt.n; b++) Mmax = std::max(Mmax, plan.bt.M[b]);
+        int ls = (Mmax * Mmax <= kG2Threads * 2) ? launch_grid2<P, 2>(g2, st) : launch_grid2<P, 4>(g2, st);
+        if (ls != MTB_OK) return ls;
+        if (p->gridder_end_event) MTB_CUDA_TRY(cudaEventRecord((cudaEvent_t)p->gridder_end_event, st));
+        k_finish<<<1, 32, 0, st>>>(P, s.norm_acc, normalizer, s.stats, stats);
+        MTB_LAUNCHED();
+        return MTB_OK;
+    }
     for (int b = 0; b < plan.bt.n; b++) {
         int M = plan.bt.M[b];
         if (M <= 0) continue;
@@ -671,7 +867,7 @@ static int run_grid(const mtb_grid_params *p, const GridPlan &plan, const float2
         a.M = M;
         a.tile = plan.bt.tile[b];
         a.W = a.tile + M - 1;
-        Launch L = launch_shape(M, P, a.tile);
+        Launch L = launch_shape(M, P, a.tile, p->merge);
         MTB_TRY(launch_bucket<P>(a, L, st));
     }
     if (p->gridder_end_event) MTB_CUDA_TRY(cudaEventRecord((cudaEvent_t)p->gridder_end_event, st));

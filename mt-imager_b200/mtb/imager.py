@@ -85,7 +85,8 @@ class WProjectionImager:
 
     def __init__(self, nx, ny, l_increment, m_increment=None, wplanes=32, sampling=8, npol=4,
                  trial_support=0, max_support=0, w_max=0.0, pol_type=L.MTB_POL_LINEAR, compensated=True,
-                 tile=0, support_bucket=0, max_chunk=0, device="cuda", kernels: KernelTable | None = None):
+                 tile=0, support_bucket=0, max_chunk=0, merge=0, device="cuda",
+                 kernels: KernelTable | None = None):
         self.lib = L.load()
         self.device = torch.device(device)
         self.nx, self.ny, self.npol = nx, ny, npol
@@ -95,7 +96,7 @@ class WProjectionImager:
         self.kernels = kernels
         self.compensated = compensated
         self.pol_type = pol_type
-        self.tuning = dict(tile=tile, support_bucket=support_bucket, max_chunk=max_chunk)
+        self.tuning = dict(tile=tile, support_bucket=support_bucket, max_chunk=max_chunk, merge=merge)
         self.grid = torch.zeros((ny, nx, npol), dtype=torch.complex64, device=self.device)
         self.grid_lo = torch.zeros_like(self.grid) if compensated else None
         self.normalizer = torch.zeros(npol, dtype=torch.float32, device=self.device)
@@ -117,7 +118,8 @@ class WProjectionImager:
         k = self.build_kernels()
         gp = L.GridParams(self.nx, self.ny, self.npol, self.params.sampling, self.params.wplanes,
                           k.info.u_increment, k.info.v_increment, k.info.w_sq_increment, int(initialize),
-                          self.tuning["tile"], self.tuning["support_bucket"], self.tuning["max_chunk"])
+                          self.tuning["tile"], self.tuning["support_bucket"], self.tuning["max_chunk"],
+                          self.tuning["merge"])
         if self.gridder_events is not None:
             gp.gridder_start_event = self.gridder_events[0].cuda_event
             gp.gridder_end_event = self.gridder_events[1].cuda_event

@@ -158,7 +158,8 @@ def test_chunked_equals_single(cfg1):
     assert sa["gridded_records"] + sa["compressed_records"] == sb["gridded_records"] + sb["compressed_records"]
 
 
-@pytest.mark.parametrize("tuning", [dict(tile=16), dict(tile=64), dict(support_bucket=3), dict(max_chunk=37)])
+@pytest.mark.parametrize("tuning", [dict(tile=16), dict(tile=64), dict(support_bucket=3), dict(max_chunk=37),
+                                    dict(merge=1), dict(merge=2), dict(merge=1, tile=16)])
 def test_tuning_does_not_change_result(cfg1, tuning):
     obs, setup, geo, kern, img_o, grid_o, norm_o = cfg1
     im, img = run_gpu(obs, setup, **tuning)
@@ -167,17 +168,18 @@ def test_tuning_does_not_change_result(cfg1, tuning):
     assert rel_rms(img[0], img_o[0]) <= IMAGE_RMS_TOL
 
 
-@pytest.mark.parametrize("kw", [dict(), dict(tile=64), dict(nx=320, s=3)])
+@pytest.mark.parametrize("kw", [dict(), dict(tile=64), dict(nx=320, s=3), dict(merge=1)])
 def test_large_supports(oracle, kw):
     """Supports up to 55 (and 105 with odd sampling): register-tile widths 1,
     2 and 8, the shared-memory window and the direct-merge variants, and
     support bands split across blocks."""
     tile = kw.pop("tile", 0)
+    merge = kw.pop("merge", 0)
     obs, setup = wide_case(**kw)
     geo = oracle.geometry_for(setup)
     kern = oracle.wkernels(geo)
     img_o, grid_o, norm_o = oracle.image_channel(obs, 0, setup, kern, geo)
-    im, img = run_gpu(obs, setup, tile=tile)
+    im, img = run_gpu(obs, setup, tile=tile, merge=merge)
     assert np.array_equal(im.kernels.conv_info, kern["conv_info"])
     assert np.abs(im.kernels.table.cpu().numpy() - kern["table"]).max() <= KERNEL_TOL
     g = im.grid_sum().cpu().numpy()
