@@ -142,8 +142,9 @@ typedef struct mtb_grid_stats {
     unsigned long long compressed_points;   /* Statistic:TotalCompressedPoints  (WImager.cpp:176) */
 } mtb_grid_stats;
 
-/* Workspace for one mtb_grid call over `nrecords` records. */
-int mtb_grid_workspace_size(const mtb_grid_params *p, int nrecords, size_t *bytes);
+/* Workspace for one mtb_grid call over `nrecords` records with the kernel
+ * table described by h_conv_info (host int [wplanes][2]). */
+int mtb_grid_workspace_size(const mtb_grid_params *p, const int *h_conv_info, int nrecords, size_t *bytes);
 
 /* Grids one chunk of records into the accumulating grid: one WImager::calculate
  * (WImager.cpp:271-290).  FP64 coordinates; FP32 tile accumulation in shared

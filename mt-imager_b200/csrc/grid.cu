@@ -498,6 +498,7 @@ struct Grid2Args {
     const int4 *wpos;
     const float2 *wvis;
     const float2 *table;
+    const float4 *table2;
     float *grid;
     float *grid_lo;
     int nx;
@@ -532,13 +533,43 @@ __device__ __forceinline__ void flush2(float *grid, float *lo, int cell, const u
     merge_cell<P>(grid + g, lo ? lo + g : nullptr, v);
 }
 
+// Thread layout for modulus M (KS slots per thread, all in one support-box
+// column so the column offset is computed once per record):
+//   G  = ceil(M / KS) row groups; a thread of row group g owns rows g + j*G.
+//   Gp = row groups one pass covers (<= kG2Threads / M); passes = ceil(G / Gp).
+//   With a single pass, kG2Threads / (M*G) independent streams split the
+//   item's records into contiguous runs (small supports fill the block that
+//   way; every flush is an atomic merge, so streams may share cells).
+struct Layout {
+    int G, Gp, npass, nstream;
+};
+__device__ __forceinline__ Layout layout_for(int M, int KS) {
+    Layout L;
+    L.G = (M + KS - 1) / KS;
+    int gmax = kG2Threads / M;
+    L.Gp = L.G < gmax ? L.G : gmax;
+    L.npass = (L.G + L.Gp - 1) / L.Gp;
+    L.nstream = (L.npass == 1) ? kG2Threads / (M * L.G) : 1;
+    return L;
+}
+
+// {re, re, im, im} copy of the table: one 128-bit load gives both packed
+// operands of the f32x2 complex multiply-add
+__global__ void k_expand_table(const float2 *__restrict__ t, float4 *__restrict__ t2, size_t n) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        float2 c = t[i];
+        t2[i] = make_float4(c.x, c.x, c.y, c.y);
+    }
+}
+
 template <int P, int KS>
-__global__ void __launch_bounds__(kG2Threads, (KS <= 2) ? 4 : 2) k_grid2(Grid2Args a) {
+__global__ void __launch_bounds__(kG2Threads, 2) k_grid2(Grid2Args a) {
     __shared__ int4 s_rec[kG2Stage];              // {grid index of corner, rxm | rym << 16, conv, S}
     __shared__ ulonglong2 s_v[kG2Stage][P];       // per pol {(re, im), (-im, re)}
     __shared__ int s_item;
     const int t = threadIdx.x;
     const int nitems = *a.n_items;
+    const ulonglong2 *tab = (const ulonglong2 *)a.table2;
     for (;;) {
         __syncthreads();
         if (t == 0) s_item = atomicAdd(a.counter, 1);
@@ -547,18 +578,23 @@ __global__ void __launch_bounds__(kG2Threads, (KS <= 2) ? 4 : 2) k_grid2(Grid2Ar
         if (v >= nitems) break;
         const int4 it = a.items[v];
         const int M = a.bt.M[(unsigned)it.z >> 24];
-        const int MM = M * M;
-        for (int pass0 = 0; pass0 < MM; pass0 += kG2Threads * KS) {
-            int sa[KS], sb[KS], last[KS];
+        const Layout L = layout_for(M, KS);
+        const int per_stream = M * L.Gp;
+        const int stream = t / per_stream;
+        const int r = t - stream * per_stream;
+        const int col = r % M;
+        const int gl = r / M;
+        const bool live = stream < L.nstream;
+        for (int pass = 0; pass < L.npass; pass++) {
+            const int g = pass * L.Gp + gl;
+            // rows g + j*G that exist: j < nrow
+            const int nrow = (live && g < L.G) ? (M - g + L.G - 1) / L.G : 0;
+            int last[KS], toff[KS];
             u64 acc[KS][P];
 #pragma unroll
             for (int j = 0; j < KS; j++) {
-                int q = pass0 + j * kG2Threads + t;
-                // an idle slot (q >= M*M) gets a = 2M: after one wrap sx is
-                // still >= M >= S, so it never touches a cell
-                sa[j] = (q < MM) ? q % M : 2 * M;
-                sb[j] = (q < MM) ? q / M : 0;
                 last[j] = -1;
+                toff[j] = -1;
 #pragma unroll
                 for (int p = 0; p < P; p++) acc[j][p] = 0ull;
             }
@@ -575,34 +611,74 @@ __global__ void __launch_bounds__(kG2Threads, (KS <= 2) ? 4 : 2) k_grid2(Grid2Ar
                     s_v[i / P][i % P] = make_ulonglong2(pk2(vv.x, vv.y), pk2(-vv.y, vv.x));
                 }
                 __syncthreads();
-                // software pipeline: the geometry and kernel values of record
-                // i+1 are fetched before record i is accumulated
-                int cellN[KS];
-                float2 cN[KS];
-                auto fetch = [&](int i) {
-                    const int4 rec = s_rec[i];
+                if (nrow == 0) continue;
+                // this stream's contiguous share of the staged records
+                const int i0 = (int)(((long)nrec * stream) / L.nstream);
+                const int i1 = (int)(((long)nrec * (stream + 1)) / L.nstream);
+                if (i0 >= i1) continue;
+                // Slot geometry depends only on the record's corner and support:
+                // it is recomputed (and the cell-change flushes done) only when
+                // those change.  toff = sy*S + sx of the slot's tap, -1 if the
+                // slot lies outside the record's support box.
+                int cellN[KS], toffN[KS];
+                auto geometry = [&](const int4 &rec) {
                     const int S = rec.w;
+                    int sx = col + (rec.y & 0xFFFF);
+                    sx -= (sx >= M) ? M : 0;
+                    int sy = g + (rec.y >> 16);
+                    sy -= (sy >= M) ? M : 0;
+                    const bool xok = sx < S;
 #pragma unroll
                     for (int j = 0; j < KS; j++) {
-                        int sx = sa[j] + (rec.y & 0xFFFF);
-                        sx -= (sx >= M) ? M : 0;
-                        int sy = sb[j] + (rec.y >> 16);
+                        const bool ok = xok && (j < nrow) && (sy < S);
+                        cellN[j] = rec.x + sy * a.nx + sx;
+                        toffN[j] = ok ? sy * S + sx : -1;
+                        sy += L.G;
                         sy -= (sy >= M) ? M : 0;
-                        bool ok = (sx < S) && (sy < S);
-                        cellN[j] = ok ? rec.x + sy * a.nx + sx : -1;
-                        cN[j] = ok ? __ldg(&a.table[rec.z + sy * S + sx]) : make_float2(0.f, 0.f);
                     }
                 };
-                fetch(0);
-                for (int i = 0; i < nrec; i++) {
-                    int cell[KS];
-                    float2 c[KS];
+                // flush the slots whose cell changes and adopt the new geometry
+                auto settle = [&]() {
 #pragma unroll
                     for (int j = 0; j < KS; j++) {
-                        cell[j] = cellN[j];
-                        c[j] = cN[j];
+                        if (toffN[j] >= 0 && cellN[j] != last[j]) {
+                            if (last[j] >= 0) flush2<P>(a.grid, a.grid_lo, last[j], acc[j]);
+                            last[j] = cellN[j];
+#pragma unroll
+                            for (int p = 0; p < P; p++) acc[j][p] = 0ull;
+                        }
+                        toff[j] = toffN[j];
                     }
-                    if (i + 1 < nrec) fetch(i + 1);
+                };
+                int4 rec = s_rec[i0];
+                geometry(rec);
+                settle();
+                ulonglong2 cN[KS];
+#pragma unroll
+                for (int j = 0; j < KS; j++)
+                    cN[j] = (toff[j] >= 0) ? __ldg(&tab[rec.z + toff[j]]) : make_ulonglong2(0ull, 0ull);
+                for (int i = i0; i < i1; i++) {
+                    ulonglong2 c[KS];
+                    int tcur[KS];
+#pragma unroll
+                    for (int j = 0; j < KS; j++) {
+                        c[j] = cN[j];
+                        tcur[j] = toff[j];
+                    }
+                    bool moved = false;
+                    int4 nrec4 = rec;
+                    if (i + 1 < i1) {
+                        nrec4 = s_rec[i + 1];
+                        moved = (nrec4.x != rec.x) || (nrec4.w != rec.w);
+                        if (moved) geometry(nrec4);
+                        // kernel values of the next record, fetched before this
+                        // record's FMAs
+#pragma unroll
+                        for (int j = 0; j < KS; j++) {
+                            int to = moved ? toffN[j] : toff[j];
+                            cN[j] = (to >= 0) ? __ldg(&tab[nrec4.z + to]) : make_ulonglong2(0ull, 0ull);
+                        }
+                    }
                     u64 vp[P], wp[P];
 #pragma unroll
                     for (int p = 0; p < P; p++) {
@@ -612,21 +688,16 @@ __global__ void __launch_bounds__(kG2Threads, (KS <= 2) ? 4 : 2) k_grid2(Grid2Ar
                     }
 #pragma unroll
                     for (int j = 0; j < KS; j++) {
-                        if (cell[j] < 0) continue;
-                        if (cell[j] != last[j]) {
-                            if (last[j] >= 0) flush2<P>(a.grid, a.grid_lo, last[j], acc[j]);
-                            last[j] = cell[j];
-#pragma unroll
-                            for (int p = 0; p < P; p++) acc[j][p] = 0ull;
-                        }
-                        const u64 cr = pk2(c[j].x, c[j].x), ci = pk2(c[j].y, c[j].y);
+                        if (tcur[j] < 0) continue;
                         // ConvolutionGridder.cu:153-181: to += vis * wt (no conjugate)
 #pragma unroll
                         for (int p = 0; p < P; p++) {
-                            ffma2(acc[j][p], cr, vp[p]);
-                            ffma2(acc[j][p], ci, wp[p]);
+                            ffma2(acc[j][p], c[j].x, vp[p]);
+                            ffma2(acc[j][p], c[j].y, wp[p]);
                         }
                     }
+                    if (moved) settle();
+                    rec = nrec4;
                 }
             }
 #pragma unroll
@@ -669,6 +740,7 @@ struct GridSpace {
     unsigned long long *stats;
     void *cub;
     size_t cub_bytes;
+    float4 *table2;      // gridder copy of the table: {re, re, im, im} per tap
 };
 
 static size_t cub_bytes(int n) {
@@ -681,7 +753,7 @@ static size_t cub_bytes(int n) {
     return std::max(a, std::max(b, c));
 }
 
-static void carve_grid(Arena &A, int R, int P, int chunk, GridSpace *s) {
+static void carve_grid(Arena &A, int R, int P, int chunk, size_t table_elems, GridSpace *s) {
     size_t n = (size_t)(R > 0 ? R : 1);
     size_t nitems = n + n / (size_t)chunk + 2;
     s->pos = A.take<int4>(n);
@@ -706,6 +778,17 @@ static void carve_grid(Arena &A, int R, int P, int chunk, GridSpace *s) {
     s->stats = A.take<unsigned long long>(4);
     s->cub_bytes = cub_bytes((int)n);
     s->cub = A.take<char>(s->cub_bytes);
+    s->table2 = A.take<float4>(table_elems ? table_elems : 1);
+}
+
+// float2 elements of the kernel table described by conv_info
+static size_t table_elems_of(const mtb_grid_params *p, const int *h_conv_info) {
+    size_t T = (size_t)oversample_T(p->sampling), n = 0;
+    for (int k = 0; k < p->wplanes; k++) {
+        size_t S = (size_t)(h_conv_info[2 * k] > 0 ? h_conv_info[2 * k] : 0);
+        n = std::max(n, (size_t)(h_conv_info[2 * k + 1] > 0 ? h_conv_info[2 * k + 1] : 0) + T * T * S * S);
+    }
+    return n;
 }
 
 static int check_params(const mtb_grid_params *p) {
@@ -786,7 +869,8 @@ static int launch_bucket(GridArgs a, const Launch &L, cudaStream_t st) {
 }
 
 template <int P>
-static int run_grid(const mtb_grid_params *p, const GridPlan &plan, const float2 *table, const int *conv_info,
+static int run_grid(const mtb_grid_params *p, const GridPlan &plan, const float2 *table, size_t table_elems,
+                    const int *conv_info,
                     const float *conv_sums, const float *uvw, const float *freq, const float2 *vis,
                     const float *weights, const int *flags, int R, float *grid, float *grid_lo,
                     float *normalizer, mtb_grid_stats *stats, GridSpace &s, cudaStream_t st) {
@@ -847,13 +931,17 @@ static int run_grid(const mtb_grid_params *p, const GridPlan &plan, const float2
         g2.wpos = s.wpos;
         g2.wvis = s.wvis;
         g2.table = table;
+        g2.table2 = s.table2;
+        {
+            int eb = (int)std::min<size_t>((table_elems + 255) / 256, (size_t)sms * 16);
+            k_expand_table<<<eb > 0 ? eb : 1, 256, 0, st>>>(table, s.table2, table_elems);
+            MTB_LAUNCHED();
+        }
         g2.grid = grid;
         g2.grid_lo = grid_lo;
         g2.nx = p->nx;
         g2.bt = plan.bt;
-        int Mmax = 0;
-        for (int b = 0; b < plan.bt.n; b++) Mmax = std::max(Mmax, plan.bt.M[b]);
-        int ls = (Mmax * Mmax <= kG2Threads * 2) ? launch_grid2<P, 2>(g2, st) : launch_grid2<P, 4>(g2, st);
+        int ls = launch_grid2<P, 4>(g2, st);
         if (ls != MTB_OK) return ls;
         if (p->gridder_end_event) MTB_CUDA_TRY(cudaEventRecord((cudaEvent_t)p->gridder_end_event, st));
         k_finish<<<1, 32, 0, st>>>(P, s.norm_acc, normalizer, s.stats, stats);
@@ -900,14 +988,15 @@ __global__ void k_ref_outputs(int R, int nx, const int4 *__restrict__ pos, const
 
 using namespace mtb;
 
-extern "C" int mtb_grid_workspace_size(const mtb_grid_params *p, int nrecords, size_t *bytes) {
-    if (!bytes) return MTB_ERR_NULL;
+extern "C" int mtb_grid_workspace_size(const mtb_grid_params *p, const int *h_conv_info, int nrecords,
+                                       size_t *bytes) {
+    if (!bytes || !h_conv_info) return MTB_ERR_NULL;
     MTB_TRY(check_params(p));
     if (nrecords < 0) return MTB_ERR_BAD_SHAPE;
     int chunk = p->max_chunk > 0 ? p->max_chunk : kDefaultChunk;
     Arena A;
     GridSpace s;
-    carve_grid(A, nrecords, p->npol, chunk, &s);
+    carve_grid(A, nrecords, p->npol, chunk, table_elems_of(p, h_conv_info), &s);
     *bytes = A.used;
     return MTB_OK;
 }
@@ -938,18 +1027,18 @@ extern "C" int mtb_grid(const mtb_grid_params *p, const void *d_table, const int
         return MTB_ERR_NULL;
     Arena A(d_workspace, workspace_bytes);
     GridSpace s;
-    carve_grid(A, nrecords, P, plan.chunk, &s);
+    carve_grid(A, nrecords, P, plan.chunk, table_elems_of(p, h_conv_info), &s);
     if (!A.ok()) return MTB_ERR_WORKSPACE;
     const float2 *tb = (const float2 *)d_table;
     const float2 *vis = (const float2 *)d_vis;
     float *g = (float *)d_grid, *lo = (float *)d_grid_lo;
     if (P == 1)
-        return run_grid<1>(p, plan, tb, d_conv_info, d_conv_sums, d_uvw, d_freq, vis, d_weights, d_flags,
+        return run_grid<1>(p, plan, tb, table_elems_of(p, h_conv_info), d_conv_info, d_conv_sums, d_uvw, d_freq, vis, d_weights, d_flags,
                            nrecords, g, lo, d_normalizer, d_stats, s, st);
     if (P == 2)
-        return run_grid<2>(p, plan, tb, d_conv_info, d_conv_sums, d_uvw, d_freq, vis, d_weights, d_flags,
+        return run_grid<2>(p, plan, tb, table_elems_of(p, h_conv_info), d_conv_info, d_conv_sums, d_uvw, d_freq, vis, d_weights, d_flags,
                            nrecords, g, lo, d_normalizer, d_stats, s, st);
-    return run_grid<4>(p, plan, tb, d_conv_info, d_conv_sums, d_uvw, d_freq, vis, d_weights, d_flags, nrecords,
+    return run_grid<4>(p, plan, tb, table_elems_of(p, h_conv_info), d_conv_info, d_conv_sums, d_uvw, d_freq, vis, d_weights, d_flags, nrecords,
                        g, lo, d_normalizer, d_stats, s, st);
 }
 
@@ -971,7 +1060,7 @@ extern "C" int mtb_preprocess_uvw(const mtb_grid_params *p, const int *d_conv_in
     cudaStream_t st = (cudaStream_t)stream;
     Arena A(d_workspace, workspace_bytes);
     GridSpace s;
-    carve_grid(A, nrecords, p->npol, plan.chunk, &s);
+    carve_grid(A, nrecords, p->npol, plan.chunk, 0, &s);
     if (!A.ok()) return MTB_ERR_WORKSPACE;
     const int R = nrecords, T = oversample_T(p->sampling);
     int blocks = std::min((R + 255) / 256, sm_count() * 8);

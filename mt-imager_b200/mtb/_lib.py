@@ -79,7 +79,7 @@ def load(path: str = LIB_PATH):
     L.mtb_wkernel_query.argtypes = [ctypes.POINTER(WKernelParams), ctypes.POINTER(WKernelInfo)]
     L.mtb_wkernel_build.argtypes = [ctypes.POINTER(WKernelParams), p, sz, p, sz, p, p, p,
                                     ctypes.POINTER(sz), p]
-    L.mtb_grid_workspace_size.argtypes = [ctypes.POINTER(GridParams), i, ctypes.POINTER(sz)]
+    L.mtb_grid_workspace_size.argtypes = [ctypes.POINTER(GridParams), p, i, ctypes.POINTER(sz)]
     L.mtb_grid.argtypes = [ctypes.POINTER(GridParams), p, p, p, p, p, p, p, p, p, i, p, p, p, p, p, sz, p]
     L.mtb_preprocess_uvw.argtypes = [ctypes.POINTER(GridParams), p, p, p, p, p, p, p, i] + [p] * 8 + [sz, p]
     L.mtb_finalize_workspace_size.argtypes = [ctypes.POINTER(FinalizeParams), ctypes.POINTER(sz)]

@@ -127,7 +127,9 @@ class WProjectionImager:
 
     def _workspace(self, nrec, gp):
         need = ctypes.c_size_t(0)
-        L.check(self.lib.mtb_grid_workspace_size(ctypes.byref(gp), nrec, ctypes.byref(need)),
+        ci = self.build_kernels().conv_info
+        L.check(self.lib.mtb_grid_workspace_size(ctypes.byref(gp), ci.ctypes.data_as(ctypes.c_void_p), nrec,
+                                                 ctypes.byref(need)),
                 "mtb_grid_workspace_size")
         if self._ws is None or self._ws.numel() < need.value:
             self._ws = torch.empty(max(1, need.value), dtype=torch.uint8, device=self.device)

@@ -254,7 +254,8 @@ def test_status_codes(oracle):
     gp = im.grid_params(True)
     gp.npol = 3
     n = ctypes.c_size_t(0)
-    assert lib.mtb_grid_workspace_size(ctypes.byref(gp), 10, ctypes.byref(n)) == 2
+    ci = im.build_kernels().conv_info.ctypes.data_as(ctypes.c_void_p)
+    assert lib.mtb_grid_workspace_size(ctypes.byref(gp), ci, 10, ctypes.byref(n)) == 2
     im2 = imager_for(setup)
     k = im2.build_kernels()
     gp = im2.grid_params(True)
