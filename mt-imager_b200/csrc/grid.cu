@@ -224,15 +224,20 @@ __global__ void k_bucket_bounds(const int4 *__restrict__ items, const int *__res
     }
 }
 
-// Gridded records in bin order: {cx, cy, conv index, support} and the
-// weighted, conjugation-corrected visibility summed over the run of records
-// compressed into it (CreateCompressionPlan.cu:32-67, CompressVisibilties.cu:41-74,
-// common.hcu:94-104).
-template <int P>
+// Gridded records in bin order with the weighted, conjugation-corrected
+// visibility summed over the run of records compressed into it
+// (CreateCompressionPlan.cu:32-67, CompressVisibilties.cu:41-74,
+// common.hcu:94-104).  Two layouts:
+//   DIRECT = false  {cx, cy, conv index, support} and float2 [P] (window gridder)
+//   DIRECT = true   {cy*nx+cx, rxm | rym << 16, conv index, support} with
+//                   rxm = (-cx) mod M, rym = (-cy) mod M for the record's bucket
+//                   modulus M, and per pol {re, im, -im, re} (direct gridder)
+template <int P, bool DIRECT>
 __global__ void k_gather(int R, const unsigned *__restrict__ skeys, const int *__restrict__ sidx,
                          const int4 *__restrict__ pos, const int *__restrict__ meta,
                          const float2 *__restrict__ vis, const float *__restrict__ weights,
-                         const int *__restrict__ flags, int4 *__restrict__ wpos, float2 *__restrict__ wvis) {
+                         const int *__restrict__ flags, int4 *__restrict__ wpos, void *__restrict__ wvis,
+                         BucketTable bt, int nx) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < R; i += gridDim.x * blockDim.x) {
         if (skeys[i] == kNoKey) continue;
         int g = sidx[i];
@@ -253,9 +258,20 @@ __global__ void k_gather(int R, const unsigned *__restrict__ skeys, const int *_
             }
             r++;
         } while (r < R && (meta[r] & 4));
-        wpos[i] = pos[g];
+        const int4 q = pos[g];
+        if (DIRECT) {
+            const int M = bt.M[bucket_of(q.w, bt.half)];
+            const int rxm = (M - q.x % M) % M, rym = (M - q.y % M) % M;
+            wpos[i] = make_int4(q.y * nx + q.x, rxm | (rym << 16), q.z, q.w);
+            float4 *o = (float4 *)wvis + (size_t)i * P;
 #pragma unroll
-        for (int p = 0; p < P; p++) wvis[(size_t)i * P + p] = acc[p];
+            for (int p = 0; p < P; p++) o[p] = make_float4(acc[p].x, acc[p].y, -acc[p].y, acc[p].x);
+        } else {
+            wpos[i] = q;
+            float2 *o = (float2 *)wvis + (size_t)i * P;
+#pragma unroll
+            for (int p = 0; p < P; p++) o[p] = acc[p];
+        }
     }
 }
 
@@ -485,11 +501,13 @@ __global__ void __launch_bounds__(KMAX >= 8 ? 576 : 1024) k_grid(GridArgs a) {
 // sy = (b - cy) mod M (Romein's assignment: a slot keeps its cell while the
 // record moves less than a cell, and no two slots of a pass share a cell).
 // Each slot accumulates V * C for all polarisations in registers with packed
-// f32x2 FMAs and merges into the grid (two-float, vector atomics) only when its
-// cell changes and at the end of a pass.  The next record's kernel values are
-// loaded while the current record's FMAs run.
+// f32x2 FMAs and merges into the grid (vector reductions) only when its cell
+// changes and at the end of a pass.
 static const int kG2Threads = 256;
-static const int kG2Stage = 128;
+static const int kG3Threads = kG2Threads;   // block size (layout_for assumes it)
+static const int kG3Chunk = 512;            // records of one work item, staged at once
+static const int kG3Depth = 4;              // records of kernel values fetched ahead
+static const int kG3KS = 4;                 // support-box slots per thread
 
 struct Grid2Args {
     const int4 *items;
@@ -497,6 +515,7 @@ struct Grid2Args {
     int *counter;
     const int4 *wpos;
     const float2 *wvis;
+    const float4 *wvis4;
     const float2 *table;
     const float4 *table2;
     float *grid;
@@ -518,6 +537,16 @@ __device__ __forceinline__ float2 upk2(u64 v) {
 }
 __device__ __forceinline__ void ffma2(u64 &acc, u64 a, u64 b) {
     asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(acc) : "l"(a), "l"(b));
+}
+
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+    unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
 template <int P>
@@ -562,14 +591,26 @@ __global__ void k_expand_table(const float2 *__restrict__ t, float4 *__restrict_
     }
 }
 
-template <int P, int KS>
-__global__ void __launch_bounds__(kG2Threads, 2) k_grid2(Grid2Args a) {
-    __shared__ int4 s_rec[kG2Stage];              // {grid index of corner, rxm | rym << 16, conv, S}
-    __shared__ ulonglong2 s_v[kG2Stage][P];       // per pol {(re, im), (-im, re)}
+// Direct gridder with asynchronous staging.  A work item's records (already in
+// the gridder layout) are copied to shared memory with 16-byte cp.async; each
+// thread then fetches the kernel values of its slots kG3Depth records ahead
+// into its own entries of a shared-memory ring (cp.async, completion tracked
+// per thread with commit/wait groups, so no block barrier per record).  A slot
+// outside a record's support box gets zeros in its ring entry, which keeps the
+// accumulation loop free of per-slot branches.
+template <int P>
+__global__ void __launch_bounds__(kG3Threads, 2) k_grid3(Grid2Args a) {
+    extern __shared__ uint4 smem3[];
+    int4 *s_rec = (int4 *)smem3;                                  // [kG3Chunk]
+    ulonglong2 *s_v = (ulonglong2 *)(s_rec + kG3Chunk);           // [kG3Chunk][P]
+    ulonglong2 *ring = s_v + (size_t)kG3Chunk * P;                // [kG3Depth][kG3KS][kG3Threads]
     __shared__ int s_item;
     const int t = threadIdx.x;
-    const int nitems = *a.n_items;
+    const int nitems = a.n_items[0];
     const ulonglong2 *tab = (const ulonglong2 *)a.table2;
+    const int4 *grec = a.wpos;
+    const uint4 *gvis = (const uint4 *)a.wvis4;
+    constexpr int KS = kG3KS, D = kG3Depth;
     for (;;) {
         __syncthreads();
         if (t == 0) s_item = atomicAdd(a.counter, 1);
@@ -577,6 +618,12 @@ __global__ void __launch_bounds__(kG2Threads, 2) k_grid2(Grid2Args a) {
         const int v = s_item;
         if (v >= nitems) break;
         const int4 it = a.items[v];
+        // stage the item's records (gridder layout, 16-byte pieces)
+        for (int k = t; k < it.y; k += kG3Threads) cp_async16(&s_rec[k], &grec[it.x + k]);
+        for (int k = t; k < it.y * P; k += kG3Threads) cp_async16(&s_v[k], &gvis[(size_t)it.x * P + k]);
+        cp_async_commit();
+        cp_async_wait<0>();
+        __syncthreads();
         const int M = a.bt.M[(unsigned)it.z >> 24];
         const Layout L = layout_for(M, KS);
         const int per_stream = M * L.Gp;
@@ -585,121 +632,102 @@ __global__ void __launch_bounds__(kG2Threads, 2) k_grid2(Grid2Args a) {
         const int col = r % M;
         const int gl = r / M;
         const bool live = stream < L.nstream;
+        const int i0 = live ? (int)(((long)it.y * stream) / L.nstream) : 0;
+        const int i1 = live ? (int)(((long)it.y * (stream + 1)) / L.nstream) : 0;
         for (int pass = 0; pass < L.npass; pass++) {
             const int g = pass * L.Gp + gl;
             // rows g + j*G that exist: j < nrow
             const int nrow = (live && g < L.G) ? (M - g + L.G - 1) / L.G : 0;
-            int last[KS], toff[KS];
+            if (nrow == 0 || i0 >= i1) continue;
+            // Slot geometry depends only on the record's corner and support;
+            // vmul = 0 marks a slot outside the record's box.
+            auto geometry = [&](const int4 &rec, int *cell, int *toff, int *vmul) {
+                const int S = rec.w;
+                int sx = col + (rec.y & 0xFFFF);
+                sx -= (sx >= M) ? M : 0;
+                int sy = g + (rec.y >> 16);
+                sy -= (sy >= M) ? M : 0;
+                const bool xok = sx < S;
+#pragma unroll
+                for (int j = 0; j < KS; j++) {
+                    const bool ok = xok && (j < nrow) && (sy < S);
+                    cell[j] = ok ? rec.x + sy * a.nx + sx : -1;
+                    toff[j] = ok ? sy * S + sx : 0;
+                    vmul[j] = ok ? 1 : 0;
+                    sy += L.G;
+                    sy -= (sy >= M) ? M : 0;
+                }
+            };
+            // look-ahead: the kernel values of record k go to ring slot k % D
+            int keyLx = -1, keyLw = -1, toffL[KS], cellL[KS], vmulL[KS];
+            auto prefetch = [&](int k) {
+                const int4 rec = s_rec[k];
+                if (rec.x != keyLx || rec.w != keyLw) {
+                    geometry(rec, cellL, toffL, vmulL);
+                    keyLx = rec.x;
+                    keyLw = rec.w;
+                }
+                ulonglong2 *dst = ring + (size_t)(k % D) * KS * kG3Threads + t;
+#pragma unroll
+                for (int j = 0; j < KS; j++) {
+                    if (vmulL[j]) cp_async16(dst + j * kG3Threads, &tab[rec.z + toffL[j]]);
+                    else dst[j * kG3Threads] = make_ulonglong2(0ull, 0ull);
+                }
+            };
+#pragma unroll
+            for (int d = 0; d < D; d++) {
+                if (i0 + d < i1) prefetch(i0 + d);
+                cp_async_commit();
+            }
+            int last[KS], keyx = -1, keyw = -1;
             u64 acc[KS][P];
 #pragma unroll
             for (int j = 0; j < KS; j++) {
                 last[j] = -1;
-                toff[j] = -1;
 #pragma unroll
                 for (int p = 0; p < P; p++) acc[j][p] = 0ull;
             }
-            for (int r0 = 0; r0 < it.y; r0 += kG2Stage) {
-                const int nrec = min(kG2Stage, it.y - r0);
-                __syncthreads();
-                for (int i = t; i < nrec; i += kG2Threads) {
-                    int4 q = a.wpos[it.x + r0 + i];
-                    int rxm = (M - q.x % M) % M, rym = (M - q.y % M) % M;
-                    s_rec[i] = make_int4(q.y * a.nx + q.x, rxm | (rym << 16), q.z, q.w);
-                }
-                for (int i = t; i < nrec * P; i += kG2Threads) {
-                    float2 vv = a.wvis[(size_t)(it.x + r0) * P + i];
-                    s_v[i / P][i % P] = make_ulonglong2(pk2(vv.x, vv.y), pk2(-vv.y, vv.x));
-                }
-                __syncthreads();
-                if (nrow == 0) continue;
-                // this stream's contiguous share of the staged records
-                const int i0 = (int)(((long)nrec * stream) / L.nstream);
-                const int i1 = (int)(((long)nrec * (stream + 1)) / L.nstream);
-                if (i0 >= i1) continue;
-                // Slot geometry depends only on the record's corner and support:
-                // it is recomputed (and the cell-change flushes done) only when
-                // those change.  toff = sy*S + sx of the slot's tap, -1 if the
-                // slot lies outside the record's support box.
-                int cellN[KS], toffN[KS];
-                auto geometry = [&](const int4 &rec) {
-                    const int S = rec.w;
-                    int sx = col + (rec.y & 0xFFFF);
-                    sx -= (sx >= M) ? M : 0;
-                    int sy = g + (rec.y >> 16);
-                    sy -= (sy >= M) ? M : 0;
-                    const bool xok = sx < S;
+            for (int i = i0; i < i1; i++) {
+                const int4 rec = s_rec[i];
+                if (rec.x != keyx || rec.w != keyw) {
+                    // corner or support changed: flush the slots whose cell changes
+                    int cellN[KS], toffN[KS], vN[KS];
+                    geometry(rec, cellN, toffN, vN);
+                    keyx = rec.x;
+                    keyw = rec.w;
 #pragma unroll
                     for (int j = 0; j < KS; j++) {
-                        const bool ok = xok && (j < nrow) && (sy < S);
-                        cellN[j] = rec.x + sy * a.nx + sx;
-                        toffN[j] = ok ? sy * S + sx : -1;
-                        sy += L.G;
-                        sy -= (sy >= M) ? M : 0;
-                    }
-                };
-                // flush the slots whose cell changes and adopt the new geometry
-                auto settle = [&]() {
-#pragma unroll
-                    for (int j = 0; j < KS; j++) {
-                        if (toffN[j] >= 0 && cellN[j] != last[j]) {
+                        if (cellN[j] >= 0 && cellN[j] != last[j]) {
                             if (last[j] >= 0) flush2<P>(a.grid, a.grid_lo, last[j], acc[j]);
                             last[j] = cellN[j];
 #pragma unroll
                             for (int p = 0; p < P; p++) acc[j][p] = 0ull;
                         }
-                        toff[j] = toffN[j];
                     }
-                };
-                int4 rec = s_rec[i0];
-                geometry(rec);
-                settle();
-                ulonglong2 cN[KS];
+                }
+                cp_async_wait<D - 1>();     // this thread's copies for record i have landed
+                u64 vp[P], wp[P];
 #pragma unroll
-                for (int j = 0; j < KS; j++)
-                    cN[j] = (toff[j] >= 0) ? __ldg(&tab[rec.z + toff[j]]) : make_ulonglong2(0ull, 0ull);
-                for (int i = i0; i < i1; i++) {
-                    ulonglong2 c[KS];
-                    int tcur[KS];
+                for (int p = 0; p < P; p++) {
+                    ulonglong2 q = s_v[(size_t)i * P + p];
+                    vp[p] = q.x;
+                    wp[p] = q.y;
+                }
+                const ulonglong2 *src = ring + (size_t)(i % D) * KS * kG3Threads + t;
 #pragma unroll
-                    for (int j = 0; j < KS; j++) {
-                        c[j] = cN[j];
-                        tcur[j] = toff[j];
-                    }
-                    bool moved = false;
-                    int4 nrec4 = rec;
-                    if (i + 1 < i1) {
-                        nrec4 = s_rec[i + 1];
-                        moved = (nrec4.x != rec.x) || (nrec4.w != rec.w);
-                        if (moved) geometry(nrec4);
-                        // kernel values of the next record, fetched before this
-                        // record's FMAs
-#pragma unroll
-                        for (int j = 0; j < KS; j++) {
-                            int to = moved ? toffN[j] : toff[j];
-                            cN[j] = (to >= 0) ? __ldg(&tab[nrec4.z + to]) : make_ulonglong2(0ull, 0ull);
-                        }
-                    }
-                    u64 vp[P], wp[P];
+                for (int j = 0; j < KS; j++) {
+                    const ulonglong2 c = src[j * kG3Threads];
+                    // ConvolutionGridder.cu:153-181: to += vis * wt (no conjugate)
 #pragma unroll
                     for (int p = 0; p < P; p++) {
-                        ulonglong2 q = s_v[i][p];
-                        vp[p] = q.x;
-                        wp[p] = q.y;
+                        ffma2(acc[j][p], c.x, vp[p]);
+                        ffma2(acc[j][p], c.y, wp[p]);
                     }
-#pragma unroll
-                    for (int j = 0; j < KS; j++) {
-                        if (tcur[j] < 0) continue;
-                        // ConvolutionGridder.cu:153-181: to += vis * wt (no conjugate)
-#pragma unroll
-                        for (int p = 0; p < P; p++) {
-                            ffma2(acc[j][p], c[j].x, vp[p]);
-                            ffma2(acc[j][p], c[j].y, wp[p]);
-                        }
-                    }
-                    if (moved) settle();
-                    rec = nrec4;
                 }
+                if (i + D < i1) prefetch(i + D);
+                cp_async_commit();
             }
+            cp_async_wait<0>();
 #pragma unroll
             for (int j = 0; j < KS; j++)
                 if (last[j] >= 0) flush2<P>(a.grid, a.grid_lo, last[j], acc[j]);
@@ -707,15 +735,45 @@ __global__ void __launch_bounds__(kG2Threads, 2) k_grid2(Grid2Args a) {
     }
 }
 
-template <int P, int KS>
-static int launch_grid2(const Grid2Args &a, cudaStream_t st) {
-    auto kern = k_grid2<P, KS>;
+template <int P>
+static int launch_grid3(const Grid2Args &a, cudaStream_t st) {
+    auto kern = k_grid3<P>;
+    const size_t smem = (size_t)kG3Chunk * 16 * (1 + P) + (size_t)kG3Depth * kG3KS * kG3Threads * 16;
+    MTB_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
-    MTB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kG2Threads, 0));
+    MTB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kG3Threads, smem));
     if (per_sm < 1) return MTB_ERR_BAD_SHAPE;
-    kern<<<per_sm * sm_count(), kG2Threads, 0, st>>>(a);
+    kern<<<per_sm * sm_count(), kG3Threads, smem, st>>>(a);
     MTB_LAUNCHED();
     return MTB_OK;
+}
+
+// Compensated merge of one call's contribution into the two-float grid:
+// hi + lo += delta with the rounding error of hi + delta kept in lo.  One pass
+// over the cells, no atomics; cells the call did not touch are skipped.
+__global__ void k_merge_delta(float4 *__restrict__ hi, float4 *__restrict__ lo, const float4 *__restrict__ delta,
+                              size_t n4) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n4; i += (size_t)gridDim.x * blockDim.x) {
+        const float4 d = delta[i];
+        if (d.x == 0.f && d.y == 0.f && d.z == 0.f && d.w == 0.f) continue;
+        float4 h = hi[i], e = lo[i];
+        float sx, bp;
+        sx = h.x + d.x; bp = sx - h.x; e.x += (h.x - (sx - bp)) + (d.x - bp); h.x = sx;
+        sx = h.y + d.y; bp = sx - h.y; e.y += (h.y - (sx - bp)) + (d.y - bp); h.y = sx;
+        sx = h.z + d.z; bp = sx - h.z; e.z += (h.z - (sx - bp)) + (d.z - bp); h.z = sx;
+        sx = h.w + d.w; bp = sx - h.w; e.w += (h.w - (sx - bp)) + (d.w - bp); h.w = sx;
+        hi[i] = h;
+        lo[i] = e;
+    }
+}
+
+__global__ void k_merge_delta_tail(float *hi, float *lo, const float *delta, size_t nfloat) {
+    for (size_t i = nfloat & ~(size_t)3; i < nfloat; i++) {
+        float d = delta[i], h = hi[i];
+        float sx = h + d, bp = sx - h;
+        lo[i] += (h - (sx - bp)) + (d - bp);
+        hi[i] = sx;
+    }
 }
 
 // ------------------------------------------------------------ host side --
@@ -741,6 +799,7 @@ struct GridSpace {
     void *cub;
     size_t cub_bytes;
     float4 *table2;      // gridder copy of the table: {re, re, im, im} per tap
+    float *delta;        // this call's grid contribution (compensated mode)
 };
 
 static size_t cub_bytes(int n) {
@@ -753,7 +812,7 @@ static size_t cub_bytes(int n) {
     return std::max(a, std::max(b, c));
 }
 
-static void carve_grid(Arena &A, int R, int P, int chunk, size_t table_elems, GridSpace *s) {
+static void carve_grid(Arena &A, int R, int P, int chunk, size_t table_elems, size_t grid_cells, GridSpace *s) {
     size_t n = (size_t)(R > 0 ? R : 1);
     size_t nitems = n + n / (size_t)chunk + 2;
     s->pos = A.take<int4>(n);
@@ -773,12 +832,13 @@ static void carve_grid(Arena &A, int R, int P, int chunk, size_t table_elems, Gr
     s->bounds = A.take<int>(2 * kMaxBuckets);
     s->counters = A.take<int>(kMaxBuckets);
     s->wpos = A.take<int4>(n);
-    s->wvis = A.take<float2>(n * P);
+    s->wvis = A.take<float2>(n * P * 2);   // float4 per pol for the direct gridder
     s->norm_acc = A.take<double>(4);
     s->stats = A.take<unsigned long long>(4);
     s->cub_bytes = cub_bytes((int)n);
     s->cub = A.take<char>(s->cub_bytes);
     s->table2 = A.take<float4>(table_elems ? table_elems : 1);
+    s->delta = A.take<float>(grid_cells ? grid_cells * 2 * P : 1);
 }
 
 // float2 elements of the kernel table described by conv_info
@@ -789,6 +849,13 @@ static size_t table_elems_of(const mtb_grid_params *p, const int *h_conv_info) {
         n = std::max(n, (size_t)(h_conv_info[2 * k + 1] > 0 ? h_conv_info[2 * k + 1] : 0) + T * T * S * S);
     }
     return n;
+}
+
+// records per work item: the direct gridder stages a whole item in shared memory
+static int effective_chunk(const mtb_grid_params *p) {
+    int c = p->max_chunk > 0 ? p->max_chunk : kDefaultChunk;
+    if (p->merge != 1 && c > kG3Chunk) c = kG3Chunk;
+    return c;
 }
 
 static int check_params(const mtb_grid_params *p) {
@@ -805,7 +872,7 @@ static int check_params(const mtb_grid_params *p) {
 static int make_plan(const mtb_grid_params *p, const int *h_conv_info, GridPlan *g) {
     int half = p->support_bucket > 0 ? p->support_bucket : 1;
     int tile = p->tile > 0 ? p->tile : kDefaultTile;
-    g->chunk = p->max_chunk > 0 ? p->max_chunk : kDefaultChunk;
+    g->chunk = effective_chunk(p);
     if (tile < 4 || p->nx / tile >= 4096 || p->ny / tile >= 4096) return MTB_ERR_BAD_PARAM;
     std::memset(&g->bt, 0, sizeof(g->bt));
     g->bt.half = half;
@@ -907,7 +974,12 @@ static int run_grid(const mtb_grid_params *p, const GridPlan &plan, const float2
     k_bucket_bounds<<<blocks, 256, 0, st>>>(s.items, s.item_start, s.nchunks, s.num_runs, s.bounds, plan.bt.n,
                                             s.n_items);
     MTB_LAUNCHED();
-    k_gather<P><<<blocks, 256, 0, st>>>(R, s.skeys, s.sidx, s.pos, s.meta, vis, weights, flags, s.wpos, s.wvis);
+    if (p->merge == 1)
+        k_gather<P, false><<<blocks, 256, 0, st>>>(R, s.skeys, s.sidx, s.pos, s.meta, vis, weights, flags, s.wpos,
+                                                   s.wvis, plan.bt, p->nx);
+    else
+        k_gather<P, true><<<blocks, 256, 0, st>>>(R, s.skeys, s.sidx, s.pos, s.meta, vis, weights, flags, s.wpos,
+                                                  s.wvis, plan.bt, p->nx);
     MTB_LAUNCHED();
     (void)end_bit;
 
@@ -937,12 +1009,30 @@ static int run_grid(const mtb_grid_params *p, const GridPlan &plan, const float2
             k_expand_table<<<eb > 0 ? eb : 1, 256, 0, st>>>(table, s.table2, table_elems);
             MTB_LAUNCHED();
         }
-        g2.grid = grid;
-        g2.grid_lo = grid_lo;
+        // compensated mode: the call grids into a zeroed delta grid with plain
+        // vector reductions (no returned values, so no stall at a flush) and
+        // one pass merges it into (grid, grid_lo) afterwards
+        const size_t nfloat = (size_t)p->nx * p->ny * 2 * P;
+        if (grid_lo) MTB_CUDA_TRY(cudaMemsetAsync(s.delta, 0, nfloat * sizeof(float), st));
+        g2.wvis4 = (const float4 *)s.wvis;
+        g2.grid = grid_lo ? s.delta : grid;
+        g2.grid_lo = nullptr;
         g2.nx = p->nx;
         g2.bt = plan.bt;
-        int ls = launch_grid2<P, 4>(g2, st);
+        int ls = launch_grid3<P>(g2, st);
         if (ls != MTB_OK) return ls;
+        if (grid_lo) {
+            const size_t n4 = nfloat / 4;
+            int mb = (int)std::min<size_t>((n4 + 255) / 256, (size_t)sms * 16);
+            k_merge_delta<<<mb > 0 ? mb : 1, 256, 0, st>>>((float4 *)grid, (float4 *)grid_lo,
+                                                         (const float4 *)s.delta, n4);
+            MTB_LAUNCHED();
+            if (nfloat % 4) {
+                // odd cell count with one polarisation: the last cell alone
+                k_merge_delta_tail<<<1, 1, 0, st>>>(grid, grid_lo, s.delta, nfloat);
+                MTB_LAUNCHED();
+            }
+        }
         if (p->gridder_end_event) MTB_CUDA_TRY(cudaEventRecord((cudaEvent_t)p->gridder_end_event, st));
         k_finish<<<1, 32, 0, st>>>(P, s.norm_acc, normalizer, s.stats, stats);
         MTB_LAUNCHED();
@@ -993,10 +1083,10 @@ extern "C" int mtb_grid_workspace_size(const mtb_grid_params *p, const int *h_co
     if (!bytes || !h_conv_info) return MTB_ERR_NULL;
     MTB_TRY(check_params(p));
     if (nrecords < 0) return MTB_ERR_BAD_SHAPE;
-    int chunk = p->max_chunk > 0 ? p->max_chunk : kDefaultChunk;
+    int chunk = effective_chunk(p);
     Arena A;
     GridSpace s;
-    carve_grid(A, nrecords, p->npol, chunk, table_elems_of(p, h_conv_info), &s);
+    carve_grid(A, nrecords, p->npol, chunk, table_elems_of(p, h_conv_info), (size_t)p->nx * p->ny, &s);
     *bytes = A.used;
     return MTB_OK;
 }
@@ -1027,7 +1117,7 @@ extern "C" int mtb_grid(const mtb_grid_params *p, const void *d_table, const int
         return MTB_ERR_NULL;
     Arena A(d_workspace, workspace_bytes);
     GridSpace s;
-    carve_grid(A, nrecords, P, plan.chunk, table_elems_of(p, h_conv_info), &s);
+    carve_grid(A, nrecords, P, plan.chunk, table_elems_of(p, h_conv_info), (size_t)p->nx * p->ny, &s);
     if (!A.ok()) return MTB_ERR_WORKSPACE;
     const float2 *tb = (const float2 *)d_table;
     const float2 *vis = (const float2 *)d_vis;
@@ -1060,7 +1150,7 @@ extern "C" int mtb_preprocess_uvw(const mtb_grid_params *p, const int *d_conv_in
     cudaStream_t st = (cudaStream_t)stream;
     Arena A(d_workspace, workspace_bytes);
     GridSpace s;
-    carve_grid(A, nrecords, p->npol, plan.chunk, 0, &s);
+    carve_grid(A, nrecords, p->npol, plan.chunk, 0, 0, &s);
     if (!A.ok()) return MTB_ERR_WORKSPACE;
     const int R = nrecords, T = oversample_T(p->sampling);
     int blocks = std::min((R + 255) / 256, sm_count() * 8);
