@@ -65,7 +65,8 @@ enum {
     MTB_ERR_CUDA = 5,          /* CudaException                                      */
     MTB_ERR_CUFFT = 6,         /* FFTException                                       */
     MTB_ERR_KERNEL = 7,        /* ImagerException: w=0 origin not real / no support  */
-    MTB_ERR_NULL = 8           /* a required pointer is NULL                         */
+    MTB_ERR_NULL = 8,          /* a required pointer is NULL                         */
+    MTB_ERR_TOO_LARGE = 9      /* request exceeds a fixed-size entry point's capacity */
 };
 
 /* ------------------------------------------------------------ w-kernels -- */
@@ -177,6 +178,30 @@ int mtb_preprocess_uvw(const mtb_grid_params *p, const int *d_conv_info, const i
                        int *d_conv_index, int *d_to_grid, int *d_to_compress, int *d_support,
                        float *d_take_conjugate, float *d_conv_sum, void *d_workspace,
                        size_t workspace_bytes, mtb_stream_t stream);
+
+/* mtb_preprocess_uvw for callers that cannot allocate device memory.  No
+ * counterpart in the reference.  Some hosts may not call cudaMalloc at all:
+ * code running inside an allocator or memory-pool callback, a process whose
+ * device memory is partitioned up front by its framework, a plugin that may
+ * only use the buffers its host hands it.  This entry point takes no
+ * workspace: its scratch lives in a fixed array inside the library's device
+ * image (about 28 MB, held by every GPU that loads the library until the
+ * process exits), and it calls no allocating routine.  Inputs and outputs are
+ * those of mtb_preprocess_uvw and still belong to the caller.
+ *   - nrecords above mtb_preprocess_uvw_noalloc_capacity() (1,048,576) is
+ *     refused with MTB_ERR_TOO_LARGE; split larger chunks.
+ *   - The first call on a device looks up the array's device address
+ *     (cudaGetSymbolAddress); make that first call before any stream capture.
+ *   - Every call shares the one array, so calls whose work overlaps on the
+ *     GPU (different streams or host threads on one device) race and must be
+ *     serialised by the caller. */
+int mtb_preprocess_uvw_noalloc(const mtb_grid_params *p, const int *d_conv_info, const int *h_conv_info,
+                               const float *d_conv_sums, const float *d_uvw, const float *d_freq,
+                               const float *d_weights, const int *d_flags, int nrecords, int *d_gridding_data,
+                               int *d_conv_index, int *d_to_grid, int *d_to_compress, int *d_support,
+                               float *d_take_conjugate, float *d_conv_sum, mtb_stream_t stream);
+/* Largest nrecords mtb_preprocess_uvw_noalloc accepts. */
+int mtb_preprocess_uvw_noalloc_capacity(void);
 
 /* ------------------------------------------------------------- finalize -- */
 enum { MTB_POL_LINEAR = 0, MTB_POL_CIRCULAR = 1 };  /* PolarizationType (mtimager.h:30-37) */

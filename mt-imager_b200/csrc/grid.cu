@@ -34,6 +34,7 @@
 
 #include <algorithm>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "mtb_internal.cuh"
@@ -1170,6 +1171,93 @@ extern "C" int mtb_preprocess_uvw(const mtb_grid_params *p, const int *d_conv_in
     MTB_LAUNCHED();
     k_ref_outputs<<<blocks, 256, 0, st>>>(R, p->nx, s.pos, s.meta, (int4 *)d_gridding_data, d_conv_index,
                                           d_to_grid, d_to_compress, d_support, d_take_conjugate);
+    MTB_LAUNCHED();
+    return MTB_OK;
+}
+
+// ------------------------------------------------------ fixed-scratch path --
+// Some callers cannot allocate device memory: code running where cudaMalloc
+// is off limits (inside an allocator or memory-pool callback, a process whose
+// device memory is pre-partitioned by a host framework, or a plugin that may
+// only touch buffers its host hands it).  For them mtb_preprocess_uvw_noalloc
+// runs the PreProcessUVW operator with its scratch in the fixed array below
+// instead of a caller workspace.  The array is part of this library's device
+// image, so every GPU that loads the library holds it until the process exits.
+namespace mtb {
+static const int kNoAllocMaxRecords = 1 << 20;
+static const size_t kNoAllocPos = 0;
+static const size_t kNoAllocMeta = kNoAllocPos + sizeof(int4) * (size_t)kNoAllocMaxRecords;
+static const size_t kNoAllocKeys = kNoAllocMeta + sizeof(int) * (size_t)kNoAllocMaxRecords;
+static const size_t kNoAllocIota = kNoAllocKeys + sizeof(unsigned) * (size_t)kNoAllocMaxRecords;
+static const size_t kNoAllocNorm = kNoAllocIota + sizeof(int) * (size_t)kNoAllocMaxRecords;
+static const size_t kNoAllocStats = kNoAllocNorm + sizeof(double) * 4;
+static const size_t kNoAllocBytes = kNoAllocStats + sizeof(unsigned long long) * 4;
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+// Device address of g_noalloc_scratch on the current device, looked up once
+// per device (host code must not use the symbol itself as an address).
+static int noalloc_scratch(unsigned char **out) {
+    static std::mutex mu;
+    static unsigned char *addr[64] = {nullptr};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return MTB_ERR_CUDA;
+    std::lock_guard<std::mutex> lk(mu);
+    if (!addr[dev]) {
+        void *ptr = nullptr;
+        if (cudaGetSymbolAddress(&ptr, g_noalloc_scratch) != cudaSuccess || !ptr) return MTB_ERR_CUDA;
+        addr[dev] = (unsigned char *)ptr;
+    }
+    *out = addr[dev];
+    return MTB_OK;
+}
+}  // namespace mtb
+
+extern "C" int mtb_preprocess_uvw_noalloc_capacity(void) { return mtb::kNoAllocMaxRecords; }
+
+extern "C" int mtb_preprocess_uvw_noalloc(const mtb_grid_params *p, const int *d_conv_info, const int *h_conv_info,
+                                          const float *d_conv_sums, const float *d_uvw, const float *d_freq,
+                                          const float *d_weights, const int *d_flags, int nrecords,
+                                          int *d_gridding_data, int *d_conv_index, int *d_to_grid,
+                                          int *d_to_compress, int *d_support, float *d_take_conjugate,
+                                          float *d_conv_sum, mtb_stream_t stream) {
+    MTB_TRY(check_params(p));
+    if (nrecords < 0) return MTB_ERR_BAD_SHAPE;
+    if (nrecords > kNoAllocMaxRecords) return MTB_ERR_TOO_LARGE;
+    if (nrecords == 0) return MTB_OK;
+    if (!d_conv_info || !h_conv_info || !d_conv_sums || !d_uvw || !d_freq || !d_weights || !d_flags ||
+        !d_gridding_data || !d_conv_index || !d_to_grid || !d_to_compress || !d_support || !d_take_conjugate ||
+        !d_conv_sum)
+        return MTB_ERR_NULL;
+    GridPlan plan;
+    MTB_TRY(make_plan(p, h_conv_info, &plan));
+    unsigned char *base = nullptr;
+    MTB_TRY(noalloc_scratch(&base));
+    int4 *pos = (int4 *)(base + kNoAllocPos);
+    int *meta = (int *)(base + kNoAllocMeta);
+    unsigned *keys = (unsigned *)(base + kNoAllocKeys);
+    int *iota = (int *)(base + kNoAllocIota);
+    double *norm_acc = (double *)(base + kNoAllocNorm);
+    unsigned long long *stats = (unsigned long long *)(base + kNoAllocStats);
+    cudaStream_t st = (cudaStream_t)stream;
+    const int R = nrecords, T = oversample_T(p->sampling);
+    int blocks = std::min((R + 255) / 256, sm_count() * 8);
+    // the accumulators keep the previous call's values: clear them
+    MTB_CUDA_TRY(cudaMemsetAsync(norm_acc, 0, 4 * sizeof(double), st));
+    MTB_CUDA_TRY(cudaMemsetAsync(stats, 0, 4 * sizeof(unsigned long long), st));
+#define MTB_PRE(PP)                                                                                           \
+    k_preprocess<PP><<<blocks, 256, 0, st>>>(R, d_uvw, d_freq, d_weights, d_flags, d_conv_info, d_conv_sums,   \
+                                             p->wplanes, p->w_sq_increment, p->sampling, T, p->nx, p->ny,     \
+                                             p->u_increment, p->v_increment, pos, meta, norm_acc, d_conv_sum)
+    if (p->npol == 1) MTB_PRE(1);
+    else if (p->npol == 2) MTB_PRE(2);
+    else MTB_PRE(4);
+#undef MTB_PRE
+    MTB_LAUNCHED();
+    k_compress<<<blocks, 256, 0, st>>>(R, p->nx, pos, meta, keys, iota, plan.bt, stats);
+    MTB_LAUNCHED();
+    k_ref_outputs<<<blocks, 256, 0, st>>>(R, p->nx, pos, meta, (int4 *)d_gridding_data, d_conv_index, d_to_grid,
+                                          d_to_compress, d_support, d_take_conjugate);
     MTB_LAUNCHED();
     return MTB_OK;
 }

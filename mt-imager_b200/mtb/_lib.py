@@ -14,12 +14,14 @@ PKG = os.path.dirname(HERE)
 LIB_PATH = os.path.join(PKG, "libmtb.so")
 
 MTB_OK = 0
+MTB_ERR_TOO_LARGE = 9
 MTB_POL_LINEAR = 0
 MTB_POL_CIRCULAR = 1
 
 # every entry point include/mtb.h declares
 EXPORTS = (
     "mtb_wkernel_query", "mtb_wkernel_build", "mtb_grid_workspace_size", "mtb_grid", "mtb_preprocess_uvw",
+    "mtb_preprocess_uvw_noalloc", "mtb_preprocess_uvw_noalloc_capacity",
     "mtb_finalize_workspace_size", "mtb_finalize", "mtb_status_string", "mtb_version",
     "mtb_release_caches", "mtb_kernel_launch_count", "mtb_calibrate_fp32",
 )
@@ -82,6 +84,8 @@ def load(path: str = LIB_PATH):
     L.mtb_grid_workspace_size.argtypes = [ctypes.POINTER(GridParams), p, i, ctypes.POINTER(sz)]
     L.mtb_grid.argtypes = [ctypes.POINTER(GridParams), p, p, p, p, p, p, p, p, p, i, p, p, p, p, p, sz, p]
     L.mtb_preprocess_uvw.argtypes = [ctypes.POINTER(GridParams), p, p, p, p, p, p, p, i] + [p] * 8 + [sz, p]
+    L.mtb_preprocess_uvw_noalloc.argtypes = [ctypes.POINTER(GridParams), p, p, p, p, p, p, p, i] + [p] * 7 + [p]
+    L.mtb_preprocess_uvw_noalloc_capacity.argtypes = []
     L.mtb_finalize_workspace_size.argtypes = [ctypes.POINTER(FinalizeParams), ctypes.POINTER(sz)]
     L.mtb_finalize.argtypes = [ctypes.POINTER(FinalizeParams), p, p, p, p, p, sz, p]
     for name in EXPORTS:
