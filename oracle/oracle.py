@@ -9,11 +9,13 @@ The per-element work lives in ``wproj_oracle.c`` (compiled here with gcc,
 function names the reference step it restates (paths relative to the
 reference project's ``code/`` directory).
 
-Parity anchors: the reference ships no tests, fixtures or golden vectors, so
-this restatement is pinned by the known-answer tests in tests/ (w=0 kernel
-DC = 1, point sources imaged where the direct FP64 DFT puts them, chunk
-invariance, Hermitian conjugation of w<0 records) and by the committed
-golden vectors in tests/golden/.
+Parity anchors: the reference ships no tests, fixtures or golden vectors.
+This restatement is pinned (tests/test_golden.py) against outputs of
+mt-imager's own operator code -- its sources compiled unchanged by
+oracle/build_ref.py and run on a GPU by tests/golden/make_golden.py -- and by
+the known-answer tests in tests/test_oracle.py (w=0 kernel DC = 1, point
+sources imaged where the direct FP64 DFT puts them, chunk invariance,
+Hermitian conjugation of w<0 records).
 """
 from __future__ import annotations
 

@@ -1,0 +1,158 @@
+/*
+ * GPUafw.h -- TEST INFRASTRUCTURE, NOT PRODUCT CODE.
+ *
+ * A minimal stand-in for the GAFW engine headers, written for this project,
+ * so that mt-imager's own operator sources (their kernels and submitToGPU
+ * launch code) compile unchanged outside GAFW and can be driven by
+ * oracle/ref_harness.cu to produce reference outputs.  Only the names those
+ * sources use are provided; the interface mirrors GAFW's
+ * (gafw/Implimentation/GPUImplimentation/GPUafw.h:28-70,
+ *  GPUSubmissionData.h:27-47, GPUArrayOperator.h:27-43,
+ *  gafw/pil/ArrayDimensions.h:62-83) because the operator sources are
+ * written against it.  The engine itself (scheduling, memory, validation)
+ * is not reproduced: the harness allocates every buffer and calls
+ * submitToGPU directly.
+ */
+#ifndef MTREF_GPUAFW_STUB_H
+#define MTREF_GPUAFW_STUB_H
+
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <map>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+typedef unsigned int uint;
+
+class CudaException : public std::runtime_error {
+public:
+    CudaException(const std::string &msg, cudaError_t err)
+        : std::runtime_error(msg + ": " + cudaGetErrorString(err)), err(err) {}
+    cudaError_t err;
+};
+
+#define checkCudaError(x, msg)                                    \
+    {                                                             \
+        cudaError_t _mtref_err_ = (x);                            \
+        if (_mtref_err_ != cudaSuccess) throw CudaException(msg, _mtref_err_); \
+    }
+
+namespace GAFW {
+
+class GeneralException : public std::runtime_error {
+public:
+    explicit GeneralException(const std::string &msg) : std::runtime_error(msg) {}
+};
+
+// Dimensions listed slowest first; the last one is X (columns).
+class ArrayDimensions {
+public:
+    ArrayDimensions() {}
+    explicit ArrayDimensions(const std::vector<unsigned> &d) : dims(d) {}
+    int getNoOfDimensions() const { return (int)dims.size(); }
+    unsigned getNoOfColumns() const { return dims.empty() ? 0 : dims.back(); }
+    unsigned getNoOfRows() const { return dims.size() < 2 ? 1 : dims[dims.size() - 2]; }
+    unsigned getX() const { return getNoOfColumns(); }
+    unsigned getY() const { return getNoOfRows(); }
+    unsigned getTotalNoOfElements() const {
+        unsigned n = dims.empty() ? 0 : 1;
+        for (unsigned d : dims) n *= d;
+        return n;
+    }
+    std::vector<unsigned> dims;
+};
+
+namespace GeneralImplimentation {
+enum StoreType { real_int, real_uint, real_float, real_double, complex_float, complex_double, real_longint,
+                 real_ulongint, real_shortint, real_ushortint, StoreTypeUnknown };
+}
+
+namespace Tools { namespace CppProperties {
+class Properties {
+public:
+    int getIntProperty(const std::string &k) const { return (int)get(k); }
+    float getFloatProperty(const std::string &k) const { return (float)get(k); }
+    double getDoubleProperty(const std::string &k) const { return get(k); }
+    bool getBoolProperty(const std::string &k) const { return get(k) != 0.0; }
+    void set(const std::string &k, double v) { values[k] = v; }
+
+private:
+    double get(const std::string &k) const {
+        auto it = values.find(k);
+        if (it == values.end()) throw GeneralException("property not set: " + k);
+        return it->second;
+    }
+    std::map<std::string, double> values;
+};
+}}  // namespace Tools::CppProperties
+
+namespace GPU {
+class GPUFactory;
+
+namespace Buffer {
+enum BufferType { Buffer_Normal, Buffer_DeallocBeforeSubmit, Buffer_UnkownSize };
+}
+
+typedef struct {
+    void *pointer;
+    GAFW::ArrayDimensions dim;
+    GAFW::GeneralImplimentation::StoreType type;
+} GPUArrayDescriptor;
+
+// Launch shape covering a rows x columns array with 32 x 32 thread blocks.
+class GPUDeviceDescriptor {
+public:
+    int getBestThreadsAndBlocksDim(const int rows, const int columns, dim3 &blocks, dim3 &threads) {
+        threads = dim3(32, 32, 1);
+        blocks = dim3((unsigned)(columns + 31) / 32, (unsigned)(rows + 31) / 32, 1);
+        if (blocks.x == 0) blocks.x = 1;
+        if (blocks.y == 0) blocks.y = 1;
+        return 0;
+    }
+};
+
+class ValidationData {
+public:
+    Buffer::BufferType bufferMode = Buffer::Buffer_Normal;
+    size_t bufferSize = 0;
+};
+
+class GPUSubmissionData {
+public:
+    int noOfInputs = 0;
+    GPUArrayDescriptor *inputs = nullptr;
+    int noOfOutputs = 0;
+    GPUArrayDescriptor *outputs = nullptr;
+    cudaStream_t stream = 0;
+    void **postExecutePointer = nullptr;
+    cudaEvent_t *startEvent = nullptr;
+    cudaEvent_t *endEvent = nullptr;
+    bool endEventRecorded = false;
+    GAFW::Tools::CppProperties::Properties params;
+    void *bufferGPUPointer = nullptr;
+    int buffersize = 0;
+    GPUDeviceDescriptor *deviceDescriptor = nullptr;
+};
+
+class GPUArrayOperator {
+public:
+    enum LogCategory { other, execution_submission };
+    GPUArrayOperator(GPUFactory *, std::string nickname, std::string name = "GPUMatrixOperator")
+        : nickname(nickname), name(name) {}
+    virtual ~GPUArrayOperator() {}
+    virtual void validate() {}
+    virtual void validate(ValidationData &) {}
+    virtual void submitToGPU(GPUSubmissionData &data) = 0;
+    virtual void postRunExecute(void *) {}
+    void logDebug(int, const std::string &) {}
+    void logWarn(int, const std::string &) {}
+    void logInfo(int, const std::string &) {}
+    GAFW::Tools::CppProperties::Properties params;
+    std::string nickname, name;
+};
+}  // namespace GPU
+}  // namespace GAFW
+
+#endif

@@ -1,0 +1,133 @@
+"""Generate the golden fixtures in this directory from mt-imager itself.
+
+TEST INFRASTRUCTURE.  Runs mt-imager's own operator code (built by
+oracle/build_ref.py from the reference sources into oracle/_ref/libmtref.so;
+needs a GPU) on seeded synthetic chunks and stores inputs and outputs as
+compressed .npz files:
+
+  grid_<case>.npz   one or more WImager chunks (WImager.cpp:167-234):
+                    inputs (uvw, nu/c, vis, weights, flags), the kernel table
+                    they are gridded with (the FP64 oracle's, rounded to
+                    complex64, with its convInfo and ConvSums), the seven
+                    PreProcessUVW outputs of every chunk and the accumulated
+                    grid from ConvolutionGridder.
+
+    python tests/golden/make_golden.py [--out DIR]
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+for p in (ROOT, os.path.join(ROOT, "mt-imager_b200")):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+from mtb import synth  # noqa: E402
+from oracle import oracle as O  # noqa: E402
+
+# name: (observation and geometry, number of chunks, npol)
+CASES = {
+    # 45 baselines x 120 integrations, even oversampling, supports 7-9, two chunks
+    "even_s4": dict(obs=dict(seed=11, n_ant=10, ntimes=120, nx=128, cell_arcsec=60.0, wplanes=8, sampling=4,
+                             radius_m=300.0, flag_frac=0.1, dec_deg=-80.0, nsrc=4), chunks=2, npol=4),
+    # odd oversampling, two polarisations
+    "odd_s3_p2": dict(obs=dict(seed=12, n_ant=10, ntimes=120, nx=96, cell_arcsec=80.0, wplanes=6, sampling=3,
+                               radius_m=300.0, flag_frac=0.1, dec_deg=-85.0, nsrc=3), chunks=1, npol=2),
+    # wide field: supports 9-27, both of the reference's gridder kernels (S < 16 and S > 16)
+    "wide_s4": dict(obs=dict(seed=13, n_ant=12, ntimes=80, nx=128, cell_arcsec=400.0, wplanes=8, sampling=4,
+                             radius_m=150.0, flag_frac=0.1, dec_deg=-88.0, nsrc=3), chunks=1, npol=1,
+                    w_max_from_data=True),
+}
+
+
+def partial_flags(flags, rng, frac=0.05):
+    m = rng.random(flags.shape) < frac
+    flags[m] = 1
+
+
+def make_case(name, spec):
+    obs, setup = synth.small_config(**spec["obs"])
+    if spec.get("w_max_from_data"):
+        setup.w_max = float(np.abs(obs.uvw[2] * obs.freq_over_c(0)).max())
+    P = spec["npol"]
+    rng = np.random.default_rng(100 + spec["obs"]["seed"])
+    flags = np.ascontiguousarray(obs.flags[0][:, :P]).copy()
+    if P == 2:
+        # the reference's 2-pol ConvSum reads pol 0's flag for pol 1
+        # (WProjPreProcessUVW.cu:94): keep both pols' flags equal
+        m = rng.random(flags.shape[0]) < 0.05
+        flags[m, :] = 1
+    else:
+        partial_flags(flags, rng)
+    geo = O.geometry_for(setup)
+    kern = O.wkernels(geo)
+    return dict(uvw=np.ascontiguousarray(obs.uvw, np.float32),
+                freq=np.ascontiguousarray(obs.freq_over_c(0), np.float32),
+                vis=np.ascontiguousarray(obs.vis[0][:, :P], np.complex64),
+                weights=np.ascontiguousarray(obs.weights[0][:, :P], np.float32),
+                flags=np.ascontiguousarray(flags, np.int32),
+                table=kern["table"].astype(np.complex64), conv_info=kern["conv_info"].astype(np.int32),
+                conv_sums=kern["conv_sums"].astype(np.float32),
+                nx=setup.nx, ny=setup.ny, npol=P, sampling=setup.sampling, wplanes=setup.wplanes,
+                dl=setup.dl, trial_support=geo["trial_support"], support_cap=geo["support_cap"],
+                w_max=geo["w_max"], w_inc=geo["w_inc"], du=geo["du"], dv=geo["dv"], chunks=spec["chunks"])
+
+
+def run_reference(lib, c):
+    R = c["freq"].size
+    P = c["npol"]
+    bounds = np.linspace(0, R, c["chunks"] + 1).astype(int)
+    grid = np.zeros((c["ny"], c["nx"], P), np.complex64)
+    out = {}
+    p = lambda a: a.ctypes.data_as(ctypes.c_void_p)  # noqa: E731
+    for k, (a, b) in enumerate(zip(bounds[:-1], bounds[1:])):
+        n = int(b - a)
+        uvw = np.ascontiguousarray(c["uvw"][:, a:b])
+        sl = lambda x: np.ascontiguousarray(x[a:b])  # noqa: E731
+        pre = dict(gridding_data=np.zeros((n, 4), np.int32), conv_index=np.zeros(n, np.int32),
+                   to_grid=np.zeros(n, np.int32), to_compress=np.zeros(n, np.int32),
+                   support=np.zeros(n, np.int32), take_conjugate=np.zeros(n, np.float32),
+                   conv_sum=np.zeros((P, n), np.float32))
+        err = ctypes.create_string_buffer(512)
+        rc = lib.mtref_grid_chunk(c["nx"], c["ny"], P, c["sampling"], c["wplanes"], ctypes.c_float(c["du"]),
+                                  ctypes.c_float(c["dv"]), ctypes.c_float(c["w_inc"]), p(c["table"]),
+                                  c["table"].size, p(c["conv_info"]), p(c["conv_sums"]), p(uvw),
+                                  p(sl(c["freq"])), p(sl(c["vis"])), p(sl(c["weights"])), p(sl(c["flags"])), n,
+                                  int(k == 0), p(grid), p(pre["gridding_data"]), p(pre["conv_index"]),
+                                  p(pre["to_grid"]), p(pre["to_compress"]), p(pre["support"]),
+                                  p(pre["take_conjugate"]), p(pre["conv_sum"]), err, 512)
+        if rc:
+            raise RuntimeError("reference chunk %d failed: %s" % (k, err.value.decode()))
+        for key, v in pre.items():
+            out["ref_%s_%d" % (key, k)] = v
+    out["ref_grid"] = grid
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--out", default=HERE)
+    ap.add_argument("--lib", default=os.path.join(ROOT, "oracle", "_ref", "libmtref.so"))
+    a = ap.parse_args()
+    lib = ctypes.CDLL(a.lib)
+    lib.mtref_grid_chunk.restype = ctypes.c_int
+    O.build()
+    os.makedirs(a.out, exist_ok=True)
+    for name, spec in CASES.items():
+        c = make_case(name, spec)
+        ref = run_reference(lib, c)
+        path = os.path.join(a.out, "grid_%s.npz" % name)
+        np.savez_compressed(path, **c, **ref)
+        print("%s: %d records, %d chunks, grid peak %.4g, %d bytes" % (
+            name, c["freq"].size, c["chunks"], np.abs(ref["ref_grid"]).max(), os.path.getsize(path)))
+
+
+if __name__ == "__main__":
+    main()
