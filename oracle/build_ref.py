@@ -31,8 +31,18 @@ SOURCES = [
     ("mt-imager/lib/operators", "CreateCompressionPlan.cu"),
     ("mt-imager/lib/operators", "CompressVisibilties.cu"),
     ("mt-imager/lib/operators", "ConvolutionGridder.cu"),
+    ("mt-imager/lib/operators", "CasaGridSF.cu"),
+    ("mt-imager/lib/operators", "WProjPreFFTconvFunc.cu"),
+    ("mt-imager/lib/operators", "ConvFunctionSupportFind.cu"),
+    ("mt-imager/lib/operators", "ConvFunctionReOrganize.cu"),
+    ("mt-imager/lib/operators", "SumConvolutionFunctions.cu"),
+    ("mt-imager/lib/operators", "PreIFFTUVCorrection.cu"),
+    ("mt-imager/lib/operators", "PostIFFTStokesConverter.cu"),
+    ("mt-imager/lib/operators", "SincCorrector.cu"),
     ("gafw/Implimentation/StandardOperators", "AccumulatedSum.cu"),
     ("gafw/Implimentation/StandardOperators", "ValueChangeDetect.cu"),
+    ("gafw/Implimentation/StandardOperators", "ZeroToCentre2DShift.cu"),
+    ("gafw/Implimentation/StandardOperators", "SingleMultiply.cu"),
 ]
 INCLUDE_DIRS = ["mt-imager/lib/operators", "gafw/Implimentation/StandardOperators"]
 ARCH = "-gencode=arch=compute_100a,code=sm_100a"
@@ -50,7 +60,9 @@ def build(reference: str = DEFAULT_REF, verbose: bool = False) -> str | None:
     os.makedirs(OUT, exist_ok=True)
     # stand-in headers first, so "GPUafw.h" and friends resolve to them
     inc = ["-I" + os.path.join(HERE, "ref_stubs")] + ["-I" + os.path.join(code, d) for d in INCLUDE_DIRS]
-    flags = [ARCH, "-O2", "-std=c++17", "-Xcompiler", "-fPIC", "-w", "-x", "cu"]
+    # -maxrregcount=64: the reference was written for sm_20/sm_30, whose
+    # 63-register limit every 1024-thread launch of its operators relies on
+    flags = [ARCH, "-O2", "-std=c++17", "-maxrregcount=64", "-Xcompiler", "-fPIC", "-w", "-x", "cu"]
     jobs = [(os.path.join(code, d, f), os.path.join(OUT, f + ".o")) for d, f in SOURCES]
     jobs.append((os.path.join(HERE, "ref_harness.cu"), os.path.join(OUT, "ref_harness.o")))
 

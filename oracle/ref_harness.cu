@@ -24,8 +24,13 @@
 #include "GPUafw.h"
 #include "ImagerOperators.h"
 #include "AccumulatedSum.h"
+#include "SingleMultiply.h"
 #include "ValueChangeDetect.h"
+#include "ZeroToCentre2DShift.h"
 
+#include <cufft.h>
+
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <memory>
@@ -53,6 +58,19 @@ MTREF_OP(mtimager, CompressVisibilities)
 MTREF_OP(mtimager, ConvolutionGridder)
 MTREF_OP(GAFW::GPU::StandardOperators, AccumulatedSum)
 MTREF_OP(GAFW::GPU::StandardOperators, ValueChangeDetect)
+MTREF_OP(mtimager, CasaGridSF)
+MTREF_OP(mtimager, WProjPreFFTConvFunc)
+MTREF_OP(mtimager, ConvFunctionSupportFind)
+MTREF_OP(mtimager, ConvFunctionReOrganize)
+MTREF_OP(mtimager, SumConvolutionFunctions)
+MTREF_OP(mtimager, PreIFFTUVCorrection)
+MTREF_OP(mtimager, SincCorrector)
+MTREF_OP(GAFW::GPU::StandardOperators, ZeroToCentre2DShift)
+MTREF_OP(GAFW::GPU::StandardOperators, SingleMultiply)
+mtimager::PostIFFTStokesConverter::PostIFFTStokesConverter(GAFW::GPU::GPUFactory *f, std::string n)
+    : GAFW::GPU::GPUArrayOperator(f, n) {}
+mtimager::PostIFFTStokesConverter::~PostIFFTStokesConverter() {}
+void mtimager::PostIFFTStokesConverter::validate(GAFW::GPU::ValidationData &) {}
 
 // ConvolutionGridder creates a texture object per submission and hands it to
 // the engine for release after the run (ConvolutionGridder.cpp:56-59).
@@ -136,6 +154,30 @@ struct Runner {
         if (post) op.postRunExecute(post);
     }
 };
+
+// The multiFFT2D / IFFT2D operators: one 2-D single-precision complex FFT per
+// plane of a [planes][rows][cols] array with a cufftPlan2d(rows, cols, C2C)
+// plan (std/MultiFFT2D.cpp:77-116 forward, std/IFFT2D.cpp:73-111 inverse,
+// unnormalised).  Their sources also carry GAFW validation code, so the
+// harness issues the same cuFFT calls itself.
+void fft_planes(const DevArray &in, const DevArray &out, int direction, cudaStream_t stream) {
+    const ArrayDimensions d(in.dims);
+    const int rows = (int)d.getNoOfRows(), cols = (int)d.getNoOfColumns();
+    const int planes = (int)(d.getTotalNoOfElements() / (unsigned)(rows * cols));
+    cufftHandle plan;
+    if (cufftPlan2d(&plan, rows, cols, CUFFT_C2C) != CUFFT_SUCCESS) throw GAFW::GeneralException("cufftPlan2d");
+    cufftSetStream(plan, stream);
+    for (int i = 0; i < planes; i++) {
+        cufftComplex *a = (cufftComplex *)in.d + (size_t)i * rows * cols;
+        cufftComplex *b = (cufftComplex *)out.d + (size_t)i * rows * cols;
+        if (cufftExecC2C(plan, a, b, direction) != CUFFT_SUCCESS) {
+            cufftDestroy(plan);
+            throw GAFW::GeneralException("cufftExecC2C");
+        }
+    }
+    checkCudaError(cudaStreamSynchronize(stream), "fft");
+    cufftDestroy(plan);
+}
 
 int fail(char *err, int errlen, const char *msg) {
     if (err && errlen > 0) {
@@ -266,6 +308,149 @@ int mtref_grid_chunk(int nx, int ny, int npol, int sampling, int wplanes, float 
         run.submit(gridder, {bdi2.get(), d_index.get(), g_data.get(), cvis.get(), a_table.get(), d_cidx.get()},
                    {g.get()}, gp);
         g->download(grid);
+    } catch (const std::exception &e) {
+        return fail(err, errlen, e.what());
+    }
+    return 0;
+}
+
+/* WProjectionConvFunction::calculate (WProjectionConvFunction.cpp:186-291)
+ * with the per-plane chain of WPlaneConvFunctionCalculator
+ * (WPlaneConvFunctionCalculator.cpp:36-66): casagridsf (generate) ->
+ * WProjPreFFTConvFunc -> multiFFT2D -> ZeroToCentre2DShift -> SingleMultiply ->
+ * ConvFunctionSupportFind; then ConvFunctionReOrganize per plane,
+ * concatenation and SumConvolutionFunctions.  The scalars follow the module:
+ * w_max = 0.25 / l_increment and the plane spacing in float
+ * (WProjectionConvFunction.cpp:105-112), w_k = k^2 * increment in float
+ * (:238), the divisor read from the unshifted w = 0 FFT at [0][0]
+ * (WPlaneConvFunctionCalculator.cpp:128-142), supports capped at S_t - 2.
+ *   table       out complex64 [table_capacity]
+ *   conv_info   out int [wplanes][2], conv_sums out float [wplanes][T*T]
+ *   table_elems out: elements written; divisor out: {re, im} */
+int mtref_wkernels(int nx, int ny, double l_increment, double m_increment, int wplanes, int sampling, void *table,
+                   int table_capacity, int *conv_info, float *conv_sums, int *table_elems, float *divisor,
+                   char *err, int errlen) {
+    try {
+        Runner run;
+        int st = std::min(nx, ny) / sampling;
+        if (st % 2 == 0) st++;
+        const unsigned S_t = (unsigned)st, PS = S_t * (unsigned)sampling;
+        const int T = sampling % 2 ? sampling : sampling + 1;
+        const float maxW = 0.25 / l_increment;
+        const float wIncrement = wplanes == 1 ? 1.0f : maxW / (float)((wplanes - 1) * (wplanes - 1));
+        GAFW::Tools::CppProperties::Properties taper_p, screen_p, find_p, none;
+        typedef GAFW::Tools::CppProperties::Properties PR;
+        taper_p.set("lmPlanePostCorrection", 1, PR::Bool);
+        taper_p.set("generate", 1, PR::Bool);
+        screen_p.set("sampling", sampling, PR::Int);
+        screen_p.set("support", st, PR::Int);
+        screen_p.set("total_l", l_increment * nx, PR::Double);
+        screen_p.set("total_m", m_increment * ny, PR::Double);
+        screen_p.set("lwimager-removeedge", 0, PR::Bool);
+        find_p.set("ConvolutionFunction.sampling", sampling, PR::Int);
+        find_p.set("ConvolutionFunction.takeaszero", 1e-3f, PR::Float);
+        Arr taper = make({S_t, S_t}, real_float, 4);
+        Arr screen = make({PS, PS}, complex_float, 8), fftd = make({PS, PS}, complex_float, 8);
+        Arr shifted = make({PS, PS}, complex_float, 8), normed = make({PS, PS}, complex_float, 8);
+        Arr sup = make({1}, real_float, 4);
+        mtimager::CasaGridSF taper_op(nullptr, "taper");
+        run.submit(taper_op, {}, {taper.get()}, taper_p);
+        mtimager::WProjPreFFTConvFunc screen_op(nullptr, "preFFTConvFunction");
+        screen_op.params = screen_p;    // read through getBoolParameter (WProjPreFFTconvFunc.cu:141)
+        // divisor: the w = 0 plane's FFT at the origin, before the shift
+        screen_p.set("w", 0.0f, PR::Float);
+        run.submit(screen_op, {taper.get()}, {screen.get()}, screen_p);
+        fft_planes(*screen, *fftd, CUFFT_FORWARD, run.stream);
+        float dv[2];
+        checkCudaError(cudaMemcpy(dv, fftd->d, 8, cudaMemcpyDeviceToHost), "read divisor");
+        divisor[0] = dv[0];
+        divisor[1] = dv[1];
+        if (dv[1] > 1e-3) return fail(err, errlen, "w=0 origin has a non-zero imaginary part");
+        const float multiplier = 1 / dv[0];
+        GAFW::Tools::CppProperties::Properties mult_p;
+        mult_p.set("multiplier.value", multiplier, PR::Float);
+        GAFW::GPU::StandardOperators::ZeroToCentre2DShift shift_op(nullptr, "convFuncZeroShift");
+        GAFW::GPU::StandardOperators::SingleMultiply mult_op(nullptr, "convNormalizer");
+        mtimager::ConvFunctionSupportFind find_op(nullptr, "supportfind");
+        mtimager::ConvFunctionReOrganize org_op(nullptr, "convFuncOrganise");
+        int offset = 0;
+        for (int k = 0; k < wplanes; k++) {
+            const float w = k * k * wIncrement;
+            screen_p.set("w", w, PR::Float);
+            run.submit(screen_op, {taper.get()}, {screen.get()}, screen_p);
+            fft_planes(*screen, *fftd, CUFFT_FORWARD, run.stream);
+            run.submit(shift_op, {fftd.get()}, {shifted.get()}, none);
+            run.submit(mult_op, {shifted.get()}, {normed.get()}, mult_p);
+            run.submit(find_op, {normed.get()}, {sup.get()}, find_p);
+            float fs = 0;
+            checkCudaError(cudaMemcpy(&fs, sup->d, 4, cudaMemcpyDeviceToHost), "read support");
+            int S = (int)fs;
+            if (S > st - 2) S = st - 2;
+            if (S < 1) return fail(err, errlen, "plane without support");
+            const unsigned n = (unsigned)(T * T * S * S);
+            if (offset + (int)n > table_capacity) return fail(err, errlen, "table capacity too small");
+            Arr plane = make({n}, complex_float, 8);
+            GAFW::Tools::CppProperties::Properties org_p;
+            org_p.set("ConvolutionFunction.sampling", sampling, PR::Int);
+            org_p.set("ConvolutionFunction.support", S, PR::Int);
+            run.submit(org_op, {normed.get()}, {plane.get()}, org_p);
+            checkCudaError(cudaMemcpy((char *)table + (size_t)offset * 8, plane->d, (size_t)n * 8,
+                                      cudaMemcpyDeviceToHost), "read plane");
+            conv_info[2 * k] = S;
+            conv_info[2 * k + 1] = offset;
+            offset += (int)n;
+        }
+        *table_elems = offset;
+        Arr info = make({(unsigned)wplanes, 2}, real_int, 4), all = make({(unsigned)offset}, complex_float, 8);
+        Arr sums = make({(unsigned)wplanes, (unsigned)(T * T)}, real_float, 4);
+        info->upload(conv_info);
+        all->upload(table);
+        GAFW::Tools::CppProperties::Properties sum_p;
+        sum_p.set("sampling", sampling, PR::Int);
+        mtimager::SumConvolutionFunctions sum_op(nullptr, "SumConvolutionFunctions");
+        run.submit(sum_op, {info.get(), all.get()}, {sums.get()}, sum_p);
+        sums->download(conv_sums);
+    } catch (const std::exception &e) {
+        return fail(err, errlen, e.what());
+    }
+    return 0;
+}
+
+/* ImageFinalizer (ImageFinalizer.cpp:31-44): PreIFFTUVCorrection -> IFFT2D ->
+ * ZeroToCentre2DShift -> StokesConverter -> casagridsf (lmPlanePostCorrection)
+ * -> SincCorrector.
+ *   grid        complex64 [ny][nx][P]; normalizer float [P]
+ *   image       out float [P][ny][nx] */
+int mtref_finalize(int nx, int ny, int npol, int sampling, int pol_type, const void *grid, const float *normalizer,
+                   float *image, char *err, int errlen) {
+    try {
+        typedef GAFW::Tools::CppProperties::Properties PR;
+        Runner run;
+        const unsigned P = (unsigned)npol, X = (unsigned)nx, Y = (unsigned)ny;
+        Arr g = make({Y, X, P}, complex_float, 8), prep = make({P, Y, X}, complex_float, 8);
+        Arr ifft = make({P, Y, X}, complex_float, 8), shifted = make({P, Y, X}, complex_float, 8);
+        Arr norm = make({P}, real_float, 4), stokes = make({P, Y, X}, real_float, 4);
+        Arr tapered = make({P, Y, X}, real_float, 4), fin = make({P, Y, X}, real_float, 4);
+        g->upload(grid);
+        norm->upload(normalizer);
+        PR none, stokes_p, taper_p, sinc_p;
+        stokes_p.set("PolarizationType", pol_type, PR::Int);
+        taper_p.set("lmPlanePostCorrection", 1, PR::Bool);
+        taper_p.set("generate", 0, PR::Bool);
+        taper_p.set("sampling", 1, PR::Int);
+        sinc_p.set("sampling", sampling, PR::Int);
+        mtimager::PreIFFTUVCorrection pre_op(nullptr, "FFTPrepare");
+        run.submit(pre_op, {g.get()}, {prep.get()}, none);
+        fft_planes(*prep, *ifft, CUFFT_INVERSE, run.stream);
+        GAFW::GPU::StandardOperators::ZeroToCentre2DShift shift_op(nullptr, "Shift");
+        run.submit(shift_op, {ifft.get()}, {shifted.get()}, none);
+        mtimager::PostIFFTStokesConverter stokes_op(nullptr, "StokesConversion");
+        run.submit(stokes_op, {shifted.get(), norm.get()}, {stokes.get()}, stokes_p);
+        mtimager::CasaGridSF taper_op(nullptr, "TaperCorrection");
+        run.submit(taper_op, {stokes.get()}, {tapered.get()}, taper_p);
+        mtimager::SincCorrector sinc_op(nullptr, "SincCorrection");
+        run.submit(sinc_op, {tapered.get()}, {fin.get()}, sinc_p);
+        fin->download(image);
     } catch (const std::exception &e) {
         return fail(err, errlen, e.what());
     }

@@ -19,6 +19,7 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <complex>
 #include <map>
 #include <stdexcept>
 #include <string>
@@ -56,6 +57,7 @@ public:
     unsigned getNoOfRows() const { return dims.size() < 2 ? 1 : dims[dims.size() - 2]; }
     unsigned getX() const { return getNoOfColumns(); }
     unsigned getY() const { return getNoOfRows(); }
+    unsigned getZ() const { return dims.size() < 3 ? 1 : dims[dims.size() - 3]; }
     unsigned getTotalNoOfElements() const {
         unsigned n = dims.empty() ? 0 : 1;
         for (unsigned d : dims) n *= d;
@@ -72,19 +74,28 @@ enum StoreType { real_int, real_uint, real_float, real_double, complex_float, co
 namespace Tools { namespace CppProperties {
 class Properties {
 public:
-    int getIntProperty(const std::string &k) const { return (int)get(k); }
-    float getFloatProperty(const std::string &k) const { return (float)get(k); }
-    double getDoubleProperty(const std::string &k) const { return get(k); }
-    bool getBoolProperty(const std::string &k) const { return get(k) != 0.0; }
-    void set(const std::string &k, double v) { values[k] = v; }
+    enum PropertyType { Int, Float, Double, Bool, Complex };
+    int getIntProperty(const std::string &k) const { return (int)get(k).value; }
+    float getFloatProperty(const std::string &k) const { return (float)get(k).value; }
+    double getDoubleProperty(const std::string &k) const { return get(k).value; }
+    bool getBoolProperty(const std::string &k) const { return get(k).value != 0.0; }
+    std::complex<float> getComplexProperty(const std::string &k) const {
+        return std::complex<float>((float)get(k).value, 0.0f);
+    }
+    PropertyType getPropertyType(const std::string &k) const { return get(k).type; }
+    void set(const std::string &k, double v, PropertyType t = Double) { values[k] = Entry{v, t}; }
 
 private:
-    double get(const std::string &k) const {
+    struct Entry {
+        double value;
+        PropertyType type;
+    };
+    const Entry &get(const std::string &k) const {
         auto it = values.find(k);
         if (it == values.end()) throw GeneralException("property not set: " + k);
         return it->second;
     }
-    std::map<std::string, double> values;
+    std::map<std::string, Entry> values;
 };
 }}  // namespace Tools::CppProperties
 
@@ -101,12 +112,13 @@ typedef struct {
     GAFW::GeneralImplimentation::StoreType type;
 } GPUArrayDescriptor;
 
-// Launch shape covering a rows x columns array with 32 x 32 thread blocks.
+// Launch shape covering a rows x columns array with 16 x 16 thread blocks
+// (small enough for every operator kernel's register use on sm_100a).
 class GPUDeviceDescriptor {
 public:
     int getBestThreadsAndBlocksDim(const int rows, const int columns, dim3 &blocks, dim3 &threads) {
-        threads = dim3(32, 32, 1);
-        blocks = dim3((unsigned)(columns + 31) / 32, (unsigned)(rows + 31) / 32, 1);
+        threads = dim3(16, 16, 1);
+        blocks = dim3((unsigned)(columns + 15) / 16, (unsigned)(rows + 15) / 16, 1);
         if (blocks.x == 0) blocks.x = 1;
         if (blocks.y == 0) blocks.y = 1;
         return 0;
@@ -138,7 +150,7 @@ public:
 
 class GPUArrayOperator {
 public:
-    enum LogCategory { other, execution_submission };
+    enum LogCategory { other, execution, execution_submission };
     GPUArrayOperator(GPUFactory *, std::string nickname, std::string name = "GPUMatrixOperator")
         : nickname(nickname), name(name) {}
     virtual ~GPUArrayOperator() {}
@@ -146,6 +158,7 @@ public:
     virtual void validate(ValidationData &) {}
     virtual void submitToGPU(GPUSubmissionData &data) = 0;
     virtual void postRunExecute(void *) {}
+    bool getBoolParameter(const std::string &k) const { return params.getBoolProperty(k); }
     void logDebug(int, const std::string &) {}
     void logWarn(int, const std::string &) {}
     void logInfo(int, const std::string &) {}

@@ -11,6 +11,11 @@ compressed .npz files:
                     complex64, with its convInfo and ConvSums), the seven
                     PreProcessUVW outputs of every chunk and the accumulated
                     grid from ConvolutionGridder.
+  image_<case>.npz  ImageFinalizer (ImageFinalizer.cpp:31-44) applied to that
+                    grid with the normaliser sum of the chunks' ConvSums.
+  wkernels_<g>.npz  WProjectionConvFunction (WProjectionConvFunction.cpp:
+                    186-291): kernel table, convInfo, ConvSums and the w=0
+                    divisor for a geometry.
 
     python tests/golden/make_golden.py [--out DIR]
 """
@@ -45,6 +50,15 @@ CASES = {
                              radius_m=150.0, flag_frac=0.1, dec_deg=-88.0, nsrc=3), chunks=1, npol=1,
                     w_max_from_data=True),
 }
+
+
+# name: (nx, cell arcsec, w-planes, oversampling); w_max by the reference's rule
+KERNEL_GEOMETRIES = {
+    "cap_s4": (128, 2000.0, 6, 4),     # supports 7-31, the last planes at the S_t - 2 cap
+    "odd_s3": (96, 1500.0, 6, 3),      # odd oversampling, supports 7-23
+}
+# polarisation type of each grid case's image (0 linear, 1 circular)
+IMAGE_POL_TYPE = {"even_s4": 0, "odd_s3_p2": 1, "wide_s4": 0}
 
 
 def partial_flags(flags, rng, frac=0.05):
@@ -111,13 +125,50 @@ def run_reference(lib, c):
     return out
 
 
+def run_wkernels(lib, nx, cell, nw, s):
+    dl = cell * synth.ARCSEC
+    cap = 4_000_000
+    table = np.zeros(cap, np.complex64)
+    info = np.zeros((nw, 2), np.int32)
+    T = s if s % 2 else s + 1
+    sums = np.zeros((nw, T * T), np.float32)
+    n = ctypes.c_int(0)
+    div = np.zeros(2, np.float32)
+    err = ctypes.create_string_buffer(512)
+    p = lambda a: a.ctypes.data_as(ctypes.c_void_p)  # noqa: E731
+    rc = lib.mtref_wkernels(nx, nx, ctypes.c_double(dl), ctypes.c_double(dl), nw, s, p(table), cap, p(info),
+                            p(sums), ctypes.byref(n), p(div), err, 512)
+    if rc:
+        raise RuntimeError("reference w-kernels failed: " + err.value.decode())
+    return dict(nx=nx, dl=dl, wplanes=nw, sampling=s, ref_table=table[: n.value].copy(), ref_conv_info=info,
+                ref_conv_sums=sums, ref_divisor=div)
+
+
+def run_finalize(lib, c, ref, pol_type):
+    P = int(c["npol"])
+    norm = np.zeros(P, np.float64)
+    for k in range(int(c["chunks"])):
+        norm += ref["ref_conv_sum_%d" % k].astype(np.float64).sum(axis=1)
+    norm = norm.astype(np.float32)
+    img = np.zeros((P, int(c["ny"]), int(c["nx"])), np.float32)
+    err = ctypes.create_string_buffer(512)
+    p = lambda a: a.ctypes.data_as(ctypes.c_void_p)  # noqa: E731
+    grid = np.ascontiguousarray(ref["ref_grid"])
+    rc = lib.mtref_finalize(int(c["nx"]), int(c["ny"]), P, int(c["sampling"]), pol_type, p(grid), p(norm), p(img),
+                            err, 512)
+    if rc:
+        raise RuntimeError("reference finalize failed: " + err.value.decode())
+    return dict(pol_type=pol_type, normalizer=norm, ref_image=img)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=HERE)
     ap.add_argument("--lib", default=os.path.join(ROOT, "oracle", "_ref", "libmtref.so"))
     a = ap.parse_args()
     lib = ctypes.CDLL(a.lib)
-    lib.mtref_grid_chunk.restype = ctypes.c_int
+    for f in (lib.mtref_grid_chunk, lib.mtref_wkernels, lib.mtref_finalize):
+        f.restype = ctypes.c_int
     O.build()
     os.makedirs(a.out, exist_ok=True)
     for name, spec in CASES.items():
@@ -127,6 +178,17 @@ def main():
         np.savez_compressed(path, **c, **ref)
         print("%s: %d records, %d chunks, grid peak %.4g, %d bytes" % (
             name, c["freq"].size, c["chunks"], np.abs(ref["ref_grid"]).max(), os.path.getsize(path)))
+        img = run_finalize(lib, c, ref, IMAGE_POL_TYPE[name])
+        path = os.path.join(a.out, "image_%s.npz" % name)
+        np.savez_compressed(path, **img)
+        print("  image peak %.4g, %d bytes" % (np.abs(img["ref_image"]).max(), os.path.getsize(path)))
+    for name, g in KERNEL_GEOMETRIES.items():
+        k = run_wkernels(lib, *g)
+        path = os.path.join(a.out, "wkernels_%s.npz" % name)
+        np.savez_compressed(path, **k)
+        print("%s: supports %s, %d elements, divisor %s, %d bytes" % (
+            name, k["ref_conv_info"][:, 0].tolist(), k["ref_table"].size, k["ref_divisor"].tolist(),
+            os.path.getsize(path)))
 
 
 if __name__ == "__main__":
