@@ -134,6 +134,9 @@ typedef struct mtb_grid_params {
     void *gridder_end_event;   /* cudaEvent_t or NULL: recorded after them (the span of the
                                   ConvolutionGridder operator, like GPUSubmissionData's
                                   startEvent/endEvent, GPUSubmissionData.h:27-47)          */
+    int bulk_min_support;      /* 0: off (default); > 0: bucket moduli from max(17, value) up
+                                  are gridded by the bulk-copy gridder (cp.async.bulk rows,
+                                  mbarrier pipeline), the rest by the per-thread gridder   */
 } mtb_grid_params;
 
 typedef struct mtb_grid_stats {

@@ -20,19 +20,30 @@
 //                  run-length encoding and a scan to cut bins into work items.
 //   k_gather       weighted, conjugation-corrected visibility of each gridded
 //                  record summed over its compressed duplicates
-//                  (CompressVisibilties.cu:41-74), stored in bin order.
-//   k_grid         persistent kernel per support bucket: each block takes work
-//                  items from a queue; a work item is up to max_chunk records of
-//                  one bin.  Threads own support-box positions (Romein's
-//                  assignment: cell x belongs to the thread with a == x mod M),
-//                  accumulate in registers while their cell is unchanged and
-//                  flush cell changes into a shared-memory tile window, which is
-//                  merged into the global grid once per work item with
-//                  compensated (two-float) vector atomics.  No global atomic per
-//                  sample.
+//                  (CompressVisibilties.cu:41-74), stored in bin order together
+//                  with the record's gridder layout.
+//   k_pad_table    row-padded copy of the kernel table (rows of S + 1 taps,
+//                  16-byte aligned) and k_expand_table its {re,re,im,im} form.
+//   k_grid3        default gridder: persistent blocks take work items (up to 512
+//                  records of one bin) from a queue.  Threads own support-box
+//                  positions (Romein's assignment: cell x belongs to the slot
+//                  with a == x mod M), accumulate V * C in registers with packed
+//                  f32x2 FMAs while their cell is unchanged, and flush a cell
+//                  when it changes -- no global atomic per sample.  Kernel taps
+//                  are fetched a few records ahead into a per-thread
+//                  shared-memory ring with cp.async.
+//   k_grid4        opt-in gridder for large supports: one producer warp copies
+//                  the needed kernel rows of every record into a shared-memory
+//                  ring with cp.async.bulk (mbarrier pipeline); 11 consumer
+//                  warps accumulate from it.
+//   k_grid         shared-memory tile-window variant (merge = 1).
+//   k_merge_delta  compensated mode: flushes go to an FP64 delta grid of the
+//                  call (plain reductions), merged afterwards into the two-float
+//                  grid (hi, lo).
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <vector>
@@ -230,15 +241,31 @@ __global__ void k_bucket_bounds(const int4 *__restrict__ items, const int *__res
 // (CreateCompressionPlan.cu:32-67, CompressVisibilties.cu:41-74,
 // common.hcu:94-104).  Two layouts:
 //   DIRECT = false  {cx, cy, conv index, support} and float2 [P] (window gridder)
-//   DIRECT = true   {cy*nx+cx, rxm | rym << 16, conv index, support} with
-//                   rxm = (-cx) mod M, rym = (-cy) mod M for the record's bucket
-//                   modulus M, and per pol {re, im, -im, re} (direct gridder)
+//   DIRECT = true   {cy*nx+cx, rxm | rym << 16, padded table index, support}
+//                   with rxm = (-cx) mod M, rym = (-cy) mod M for the record's
+//                   bucket modulus M, and per pol {re, im, -im, re} (direct
+//                   gridders)
+// Index of a record's sub-kernel in the row-padded table (rows of S + 1
+// taps; see k_pad_table) from its conv index in the reference layout.
+__device__ __forceinline__ int padded_index(int ci, int S, const int *__restrict__ conv_info,
+                                            const int *__restrict__ pbase, int nw) {
+    int lo = 0, hi = nw - 1;             // last plane whose first element is <= ci
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (__ldg(&conv_info[2 * mid + 1]) <= ci) lo = mid;
+        else hi = mid - 1;
+    }
+    const int sub = (ci - __ldg(&conv_info[2 * lo + 1])) / (S * S);
+    return __ldg(&pbase[lo]) + sub * S * (S + 1);
+}
+
 template <int P, bool DIRECT>
 __global__ void k_gather(int R, const unsigned *__restrict__ skeys, const int *__restrict__ sidx,
                          const int4 *__restrict__ pos, const int *__restrict__ meta,
                          const float2 *__restrict__ vis, const float *__restrict__ weights,
                          const int *__restrict__ flags, int4 *__restrict__ wpos, void *__restrict__ wvis,
-                         BucketTable bt, int nx) {
+                         BucketTable bt, int nx, const int *__restrict__ conv_info, const int *__restrict__ pbase,
+                         int nw) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < R; i += gridDim.x * blockDim.x) {
         if (skeys[i] == kNoKey) continue;
         int g = sidx[i];
@@ -263,7 +290,8 @@ __global__ void k_gather(int R, const unsigned *__restrict__ skeys, const int *_
         if (DIRECT) {
             const int M = bt.M[bucket_of(q.w, bt.half)];
             const int rxm = (M - q.x % M) % M, rym = (M - q.y % M) % M;
-            wpos[i] = make_int4(q.y * nx + q.x, rxm | (rym << 16), q.z, q.w);
+            wpos[i] = make_int4(q.y * nx + q.x, rxm | (rym << 16), padded_index(q.z, q.w, conv_info, pbase, nw),
+                                q.w);
             float4 *o = (float4 *)wvis + (size_t)i * P;
 #pragma unroll
             for (int p = 0; p < P; p++) o[p] = make_float4(acc[p].x, acc[p].y, -acc[p].y, acc[p].x);
@@ -521,6 +549,7 @@ struct Grid2Args {
     const float4 *table2;
     float *grid;
     float *grid_lo;
+    double *dgrid;         // compensated mode: FP64 delta grid of this call, else null
     int nx;
     BucketTable bt;
 };
@@ -550,8 +579,22 @@ __device__ __forceinline__ void cp_async_wait() {
     asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
+// One cell's flush: vector FP32 reductions into the grid, or, when dgrid is
+// set (compensated mode), FP64 reductions into the call's delta grid.
 template <int P>
-__device__ __forceinline__ void flush2(float *grid, float *lo, int cell, const u64 *acc) {
+__device__ __forceinline__ void flush_cell(float *grid, double *dgrid, int cell, const float *v) {
+    const size_t g = (size_t)cell * 2 * P;
+    if (dgrid) {
+#pragma unroll
+        for (int q = 0; q < 2 * P; q++)
+            if (v[q] != 0.f) atomicAdd(dgrid + g + q, (double)v[q]);
+    } else {
+        merge_cell<P>(grid + g, nullptr, v);
+    }
+}
+
+template <int P>
+__device__ __forceinline__ void flush2(float *grid, double *dgrid, int cell, const u64 *acc) {
     float v[2 * P];
 #pragma unroll
     for (int p = 0; p < P; p++) {
@@ -559,8 +602,7 @@ __device__ __forceinline__ void flush2(float *grid, float *lo, int cell, const u
         v[2 * p] = f.x;
         v[2 * p + 1] = f.y;
     }
-    size_t g = (size_t)cell * 2 * P;
-    merge_cell<P>(grid + g, lo ? lo + g : nullptr, v);
+    flush_cell<P>(grid, dgrid, cell, v);
 }
 
 // Thread layout for modulus M (KS slots per thread, all in one support-box
@@ -581,6 +623,41 @@ __device__ __forceinline__ Layout layout_for(int M, int KS) {
     L.npass = (L.G + L.Gp - 1) / L.Gp;
     L.nstream = (L.npass == 1) ? kG2Threads / (M * L.G) : 1;
     return L;
+}
+
+// Row-padded copy of the kernel table for the direct gridders: every
+// sub-kernel row gets one zero tap (S + 1 taps, S odd), so each row and each
+// sub-kernel starts on a 16-byte boundary and rows can be moved with bulk
+// copies.  pbase[k] = first padded element of plane k.
+__global__ void k_pad_bases(const int *__restrict__ conv_info, int nw, int T, int *__restrict__ pbase) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        int b = 0;
+        for (int k = 0; k < nw; k++) {
+            pbase[k] = b;
+            const int S = conv_info[2 * k];
+            b += T * T * S * (S + 1);
+        }
+    }
+}
+
+__global__ void k_pad_table(const float2 *__restrict__ t, size_t n, const int *__restrict__ conv_info,
+                            const int *__restrict__ pbase, int nw, float2 *__restrict__ pt) {
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+        int lo = 0, hi = nw - 1;
+        while (lo < hi) {
+            int mid = (lo + hi + 1) >> 1;
+            if ((size_t)__ldg(&conv_info[2 * mid + 1]) <= e) lo = mid;
+            else hi = mid - 1;
+        }
+        const int S = __ldg(&conv_info[2 * lo]);
+        const size_t rel = e - (size_t)__ldg(&conv_info[2 * lo + 1]);
+        const size_t S2 = (size_t)S * S;
+        const size_t sub = rel / S2, w = rel % S2;
+        const int y = (int)(w / S), x = (int)(w % S);
+        const size_t dst = (size_t)__ldg(&pbase[lo]) + sub * S * (S + 1) + (size_t)y * (S + 1) + x;
+        pt[dst] = t[e];
+        if (x == S - 1) pt[dst + 1] = make_float2(0.f, 0.f);
+    }
 }
 
 // {re, re, im, im} copy of the table: one 128-bit load gives both packed
@@ -653,7 +730,7 @@ __global__ void __launch_bounds__(kG3Threads, 2) k_grid3(Grid2Args a) {
                 for (int j = 0; j < KS; j++) {
                     const bool ok = xok && (j < nrow) && (sy < S);
                     cell[j] = ok ? rec.x + sy * a.nx + sx : -1;
-                    toff[j] = ok ? sy * S + sx : 0;
+                    toff[j] = ok ? sy * (S + 1) + sx : 0;
                     vmul[j] = ok ? 1 : 0;
                     sy += L.G;
                     sy -= (sy >= M) ? M : 0;
@@ -699,7 +776,7 @@ __global__ void __launch_bounds__(kG3Threads, 2) k_grid3(Grid2Args a) {
 #pragma unroll
                     for (int j = 0; j < KS; j++) {
                         if (cellN[j] >= 0 && cellN[j] != last[j]) {
-                            if (last[j] >= 0) flush2<P>(a.grid, a.grid_lo, last[j], acc[j]);
+                            if (last[j] >= 0) flush2<P>(a.grid, a.dgrid, last[j], acc[j]);
                             last[j] = cellN[j];
 #pragma unroll
                             for (int p = 0; p < P; p++) acc[j][p] = 0ull;
@@ -731,7 +808,7 @@ __global__ void __launch_bounds__(kG3Threads, 2) k_grid3(Grid2Args a) {
             cp_async_wait<0>();
 #pragma unroll
             for (int j = 0; j < KS; j++)
-                if (last[j] >= 0) flush2<P>(a.grid, a.grid_lo, last[j], acc[j]);
+                if (last[j] >= 0) flush2<P>(a.grid, a.dgrid, last[j], acc[j]);
         }
     }
 }
@@ -749,31 +826,353 @@ static int launch_grid3(const Grid2Args &a, cudaStream_t st) {
     return MTB_OK;
 }
 
-// Compensated merge of one call's contribution into the two-float grid:
-// hi + lo += delta with the rounding error of hi + delta kept in lo.  One pass
-// over the cells, no atomics; cells the call did not touch are skipped.
-__global__ void k_merge_delta(float4 *__restrict__ hi, float4 *__restrict__ lo, const float4 *__restrict__ delta,
-                              size_t n4) {
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n4; i += (size_t)gridDim.x * blockDim.x) {
-        const float4 d = delta[i];
-        if (d.x == 0.f && d.y == 0.f && d.z == 0.f && d.w == 0.f) continue;
-        float4 h = hi[i], e = lo[i];
-        float sx, bp;
-        sx = h.x + d.x; bp = sx - h.x; e.x += (h.x - (sx - bp)) + (d.x - bp); h.x = sx;
-        sx = h.y + d.y; bp = sx - h.y; e.y += (h.y - (sx - bp)) + (d.y - bp); h.y = sx;
-        sx = h.z + d.z; bp = sx - h.z; e.z += (h.z - (sx - bp)) + (d.z - bp); h.z = sx;
-        sx = h.w + d.w; bp = sx - h.w; e.w += (h.w - (sx - bp)) + (d.w - bp); h.w = sx;
-        hi[i] = h;
-        lo[i] = e;
+// ---------------------------------------------------------------------------
+// Direct gridder for large supports with bulk-copied kernel rows.
+//
+// A block is 352 consumer threads plus one producer warp.  For every record
+// the producer copies the rows of the record's sub-kernel that the block's
+// slots need in the current pass (one or two contiguous row ranges of the
+// row-padded table, cp.async.bulk into a shared-memory ring of kG4Depth
+// slots, completion counted on a per-slot "full" mbarrier).  Consumers wait on
+// "full", read one 8-byte tap per slot from shared memory, accumulate
+// V * C with packed f32x2 FMAs and arrive on the slot's "empty" mbarrier; the
+// producer refills a slot once every consumer of its stream has arrived.
+// There is no block barrier per record.
+//
+// Slot layout (Romein): thread (col, gl) of stream cs owns support-box slots
+// (col, r0 + gl + j*Gp), j < KS, of the pass's band of nb = Gp*KS slot rows.
+// The ring stores band row r of a record at ring row r - r0 (the record's
+// sub-kernel row sy = (r + rym) mod M), so a slot's shared-memory offset only
+// changes when the record's corner or support changes.
+//
+// Complex product with compact taps: with the visibility stored as the pairs
+// (re, im) and (-im, re), a += (c.re, c.im) * (re, im) and
+// b += (c.re, c.im) * (-im, re) give Re(C V) = a.x - a.y and
+// Im(C V) = b.y - b.x.
+//
+// Every wait is bounded by a clock deadline: on expiry the kernel records an
+// error in *err and every thread leaves its loops.
+// 11 consumer warps + 1 producer warp: 3 warps per SM sub-partition, so each
+// thread may hold up to 168 registers
+static const int kG4Consumers = 352;
+static const int kG4Threads = kG4Consumers + 32;
+static const int kG4Depth = 12;               // ring slots
+// bytes of one ring slot (all streams): a pass needs at most
+// kG4Consumers * KS * 8 * (M + 1) / M <= 11927 bytes for M >= 17
+static const int kG4Slot = 11952;
+static const int kG4ZeroOff = kG4Slot - 16;   // 16 zero bytes closing every slot
+static const int kG4MaxStreams = 4;
+static const int kG4KS = 4;
+static const int kG4MinM = 17;                // smallest modulus k_grid4 handles
+static const long long kG4WaitCycles = 1LL << 31;
+
+struct Grid4Args {
+    const int4 *items;
+    const int *first;      // first item of this gridder's range
+    const int *n_items;
+    int *counter;
+    const int4 *wpos;
+    const float4 *wvis4;
+    const float2 *ptab;
+    float *grid;
+    double *dgrid;         // compensated mode: FP64 delta grid of this call, else null
+    int nx;
+    BucketTable bt;
+    int *err;
+};
+
+__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(unsigned bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(unsigned bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_tx(unsigned bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_test(unsigned bar, unsigned parity) {
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ bool mbar_try(unsigned bar, unsigned parity) {
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait for the completion of the phase with the given parity.
+__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity, volatile int *abort_flag) {
+    if (mbar_try(bar, parity)) return true;
+    const long long t0 = clock64();
+    for (;;) {
+        if (mbar_try(bar, parity)) return true;
+        if (*abort_flag) return false;
+        if (clock64() - t0 > kG4WaitCycles) return false;
+    }
+}
+__device__ __forceinline__ void bulk_g2s(unsigned dst, const void *src, unsigned bytes, unsigned bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+        "l"(src), "r"(bytes), "r"(bar)
+        : "memory");
+}
+
+template <int P>
+__device__ __forceinline__ void flush_ab(float *grid, double *dgrid, int cell, const u64 *A, const u64 *B) {
+    float v[2 * P];
+#pragma unroll
+    for (int p = 0; p < P; p++) {
+        const float2 fa = upk2(A[p]), fb = upk2(B[p]);
+        v[2 * p] = fa.x - fa.y;
+        v[2 * p + 1] = fb.y - fb.x;
+    }
+    flush_cell<P>(grid, dgrid, cell, v);
+}
+
+template <int P>
+__global__ void __launch_bounds__(kG4Threads, 1) k_grid4(Grid4Args a) {
+    extern __shared__ __align__(128) unsigned char smem_g4[];
+    int4 *s_rec = (int4 *)smem_g4;                                           // [kG3Chunk]
+    ulonglong2 *s_v = (ulonglong2 *)(smem_g4 + kG3Chunk * 16);               // [kG3Chunk][P]
+    unsigned char *ring = smem_g4 + kG3Chunk * 16 * (1 + P);                  // [kG4Depth][kG4Slot]
+    unsigned long long *bars = (unsigned long long *)(ring + kG4Depth * kG4Slot);
+    __shared__ int s_item;
+    __shared__ volatile int s_abort;
+    constexpr int KS = kG4KS, D = kG4Depth;
+    const int t = threadIdx.x;
+    const bool producer = t >= kG4Consumers;
+    const unsigned ring_sa = smem_u32(ring);
+    const unsigned full_sa = smem_u32(bars), empty_sa = full_sa + D * kG4MaxStreams * 8;
+    if (t < D) *(uint4 *)(ring + t * kG4Slot + kG4ZeroOff) = make_uint4(0u, 0u, 0u, 0u);
+    if (t == 0) s_abort = 0;
+    const int first = *a.first, nitems = *a.n_items;
+    const int4 *grec = a.wpos;
+    const uint4 *gvis = (const uint4 *)a.wvis4;
+    for (;;) {
+        __syncthreads();
+        if (t == 0) s_item = first + atomicAdd(a.counter, 1);
+        __syncthreads();
+        const int v = s_item;
+        if (v >= nitems || s_abort) break;
+        const int4 it = a.items[v];
+        const int M = a.bt.M[(unsigned)it.z >> 24];
+        const int G = (M + KS - 1) / KS;
+        int Gp = kG4Consumers / M;
+        if (Gp > G) Gp = G;
+        const int npass = (G + Gp - 1) / Gp;
+        int nstream = 1;
+        if (npass == 1) {
+            nstream = kG4Consumers / (M * G);
+            if (nstream > kG4MaxStreams) nstream = kG4MaxStreams;
+        }
+        const int per_stream = M * Gp;
+        const int nb = Gp * KS;                       // slot rows of one pass
+        const int sregion = nb * (M + 1) * 8;         // ring bytes of one stream
+        if (!producer) {
+            for (int k = t; k < it.y; k += kG4Consumers) cp_async16(&s_rec[k], &grec[it.x + k]);
+            for (int k = t; k < it.y * P; k += kG4Consumers) cp_async16(&s_v[k], &gvis[(size_t)it.x * P + k]);
+            cp_async_commit();
+            cp_async_wait<0>();
+        }
+        if (t == 0) {
+            for (int ss = 0; ss < nstream; ss++)
+                for (int d = 0; d < D; d++) {
+                    mbar_init(full_sa + (d * kG4MaxStreams + ss) * 8, 1);
+                    mbar_init(empty_sa + (d * kG4MaxStreams + ss) * 8, per_stream);
+                }
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        }
+        __syncthreads();
+        if (producer) {
+            // lane ss issues the copies of stream ss in record order; it
+            // blocks (suspended in try_wait, taking no issue slots) until the
+            // slot it refills next has been released by every consumer
+            const int ss = t - kG4Consumers;
+            if (ss < nstream) {
+                const int i0 = (int)(((long)it.y * ss) / nstream), i1 = (int)(((long)it.y * (ss + 1)) / nstream);
+                int slot = 0, phase = 0, issued = 0;
+                for (int pass = 0; pass < npass && !s_abort; pass++) {
+                    const int r0 = pass * nb;
+                    const int nbr = min(M - r0, nb);
+                    for (int i = i0; i < i1; i++) {
+                        const unsigned fb = full_sa + (slot * kG4MaxStreams + ss) * 8;
+                        // the slot's previous use completed empty phase (phase ^ 1)
+                        if (issued >= D &&
+                            !mbar_wait(empty_sa + (slot * kG4MaxStreams + ss) * 8, phase ^ 1, &s_abort)) {
+                            s_abort = 1;
+                            atomicExch(a.err, 1);
+                            break;
+                        }
+                        const int4 rec = s_rec[i];
+                        const int S = rec.w, Sp = S + 1, rym = rec.y >> 16;
+                        int sy0 = r0 + rym;
+                        if (sy0 >= M) sy0 -= M;
+                        const int ca = sy0 < S ? min(S, sy0 + nbr) - sy0 : 0;
+                        const int cb = sy0 + nbr > M ? min(S, sy0 + nbr - M) : 0;
+                        const unsigned dst = ring_sa + slot * kG4Slot + ss * sregion;
+                        mbar_arrive_tx(fb, (unsigned)((ca + cb) * Sp * 8));
+                        const float2 *src = a.ptab + rec.z;
+                        if (ca > 0) bulk_g2s(dst, src + (size_t)sy0 * Sp, (unsigned)(ca * Sp * 8), fb);
+                        if (cb > 0) bulk_g2s(dst + (unsigned)((M - sy0) * Sp * 8), src, (unsigned)(cb * Sp * 8), fb);
+                        issued++;
+                        if (++slot == D) {
+                            slot = 0;
+                            phase ^= 1;
+                        }
+                    }
+                }
+                if (s_abort) {
+                    // leave no copy in flight: wait (bounded) for the copies of
+                    // the last D records issued
+                    volatile int never = 0;
+                    for (int k = 0; k < D && k < issued; k++) {
+                        if (slot-- == 0) {
+                            slot = D - 1;
+                            phase ^= 1;
+                        }
+                        mbar_wait(full_sa + (slot * kG4MaxStreams + ss) * 8, phase, &never);
+                    }
+                }
+            }
+        } else {
+            const int cs = t / per_stream;
+            if (cs < nstream) {
+                const int rr = t - cs * per_stream;
+                const int col = rr % M, gl = rr / M;
+                const int i0 = (int)(((long)it.y * cs) / nstream), i1 = (int)(((long)it.y * (cs + 1)) / nstream);
+                int slot = 0, phase = 0;
+                for (int pass = 0; pass < npass; pass++) {
+                    const int r0 = pass * nb;
+                    int keyx = -1, keyw = -1;
+                    int last[KS];
+                    unsigned off[KS];
+                    u64 A[KS][P], B[KS][P];
+#pragma unroll
+                    for (int j = 0; j < KS; j++) {
+                        last[j] = -1;
+                        off[j] = kG4ZeroOff;
+#pragma unroll
+                        for (int p = 0; p < P; p++) A[j][p] = B[j][p] = 0ull;
+                    }
+                    bool ok = true;
+                    for (int i = i0; i < i1; i++) {
+                        if (!mbar_wait(full_sa + (slot * kG4MaxStreams + cs) * 8, phase, &s_abort)) {
+                            s_abort = 1;
+                            atomicExch(a.err, 2);
+                            ok = false;
+                            break;
+                        }
+                        const int4 rec = s_rec[i];
+                        if (rec.x != keyx || rec.w != keyw) {
+                            keyx = rec.x;
+                            keyw = rec.w;
+                            const int S = rec.w, Sp = S + 1;
+                            int sx = col + (rec.y & 0xFFFF);
+                            sx -= (sx >= M) ? M : 0;
+                            const int rym = rec.y >> 16;
+#pragma unroll
+                            for (int j = 0; j < KS; j++) {
+                                const int r = r0 + gl + j * Gp;
+                                int sy = r + rym;
+                                sy -= (sy >= M) ? M : 0;
+                                const bool valid = (r < M) && (sx < S) && (sy < S);
+                                const int cell = valid ? rec.x + sy * a.nx + sx : -1;
+                                if (cell >= 0 && cell != last[j]) {
+                                    if (last[j] >= 0) flush_ab<P>(a.grid, a.dgrid, last[j], A[j], B[j]);
+                                    last[j] = cell;
+#pragma unroll
+                                    for (int p = 0; p < P; p++) A[j][p] = B[j][p] = 0ull;
+                                }
+                                off[j] = valid ? (unsigned)(cs * sregion + ((r - r0) * Sp + sx) * 8)
+                                               : (unsigned)kG4ZeroOff;
+                            }
+                        }
+                        u64 vp[P], wp[P];
+#pragma unroll
+                        for (int p = 0; p < P; p++) {
+                            const ulonglong2 q = s_v[(size_t)i * P + p];
+                            vp[p] = q.x;
+                            wp[p] = q.y;
+                        }
+                        const unsigned char *sb = ring + slot * kG4Slot;
+#pragma unroll
+                        for (int j = 0; j < KS; j++) {
+                            const u64 c = *(const u64 *)(sb + off[j]);
+#pragma unroll
+                            for (int p = 0; p < P; p++) {
+                                ffma2(A[j][p], c, vp[p]);
+                                ffma2(B[j][p], c, wp[p]);
+                            }
+                        }
+                        mbar_arrive(empty_sa + (slot * kG4MaxStreams + cs) * 8);
+                        if (++slot == D) {
+                            slot = 0;
+                            phase ^= 1;
+                        }
+                    }
+#pragma unroll
+                    for (int j = 0; j < KS; j++)
+                        if (last[j] >= 0) flush_ab<P>(a.grid, a.dgrid, last[j], A[j], B[j]);
+                    if (!ok) break;
+                }
+            }
+        }
     }
 }
 
-__global__ void k_merge_delta_tail(float *hi, float *lo, const float *delta, size_t nfloat) {
-    for (size_t i = nfloat & ~(size_t)3; i < nfloat; i++) {
-        float d = delta[i], h = hi[i];
-        float sx = h + d, bp = sx - h;
-        lo[i] += (h - (sx - bp)) + (d - bp);
-        hi[i] = sx;
+template <int P>
+static size_t grid4_smem() {
+    return (size_t)kG3Chunk * 16 * (1 + P) + (size_t)kG4Depth * kG4Slot + 2 * kG4Depth * kG4MaxStreams * 8;
+}
+
+template <int P>
+static int launch_grid4(const Grid4Args &a, cudaStream_t st) {
+    auto kern = k_grid4<P>;
+    const size_t smem = grid4_smem<P>();
+    MTB_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    MTB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kG4Threads, smem));
+    if (per_sm < 1) return MTB_ERR_BAD_SHAPE;
+    kern<<<per_sm * sm_count(), kG4Threads, smem, st>>>(a);
+    MTB_LAUNCHED();
+    return MTB_OK;
+}
+
+// First work item whose bucket goes to k_grid4 (items are in bucket order).
+__global__ void k_split(const int *__restrict__ bounds, const int *__restrict__ n_items, BucketTable bt, int min_m,
+                        int *__restrict__ split) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        int sp = *n_items;
+        for (int b = bt.n - 1; b >= 0; b--)
+            if (bt.M[b] >= min_m && bounds[2 * b + 1] > bounds[2 * b]) sp = bounds[2 * b];
+        *split = sp;
+    }
+}
+
+// Compensated merge of one call's FP64 contribution into the two-float grid:
+// (hi + lo) + delta evaluated in FP64 and split back into the float pair.  One
+// pass over the cells, no atomics; cells the call did not touch are skipped.
+__global__ void k_merge_delta(float2 *__restrict__ hi, float2 *__restrict__ lo, const double2 *__restrict__ delta,
+                              size_t n2) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n2; i += (size_t)gridDim.x * blockDim.x) {
+        const double2 d = delta[i];
+        if (d.x == 0.0 && d.y == 0.0) continue;
+        const float2 h = hi[i], e = lo[i];
+        // (hi + lo) + delta in FP64, split back into a float pair
+        const double tx = ((double)h.x + (double)e.x) + d.x, ty = ((double)h.y + (double)e.y) + d.y;
+        const float hx = (float)tx, hy = (float)ty;
+        hi[i] = make_float2(hx, hy);
+        lo[i] = make_float2((float)(tx - (double)hx), (float)(ty - (double)hy));
     }
 }
 
@@ -799,8 +1198,13 @@ struct GridSpace {
     unsigned long long *stats;
     void *cub;
     size_t cub_bytes;
-    float4 *table2;      // gridder copy of the table: {re, re, im, im} per tap
-    float *delta;        // this call's grid contribution (compensated mode)
+    float2 *ptab;        // row-padded copy of the table (rows of S + 1 taps)
+    float4 *table2;      // padded table with each tap as {re, re, im, im} (k_grid3)
+    int *pbase;          // first padded element of every plane
+    int *split;          // first work item of k_grid4
+    int *counter4;       // k_grid4 work counter
+    int *err;            // gridder pipeline error flag
+    double *delta;       // this call's grid contribution (compensated mode), FP64
 };
 
 static size_t cub_bytes(int n) {
@@ -813,7 +1217,8 @@ static size_t cub_bytes(int n) {
     return std::max(a, std::max(b, c));
 }
 
-static void carve_grid(Arena &A, int R, int P, int chunk, size_t table_elems, size_t grid_cells, GridSpace *s) {
+static void carve_grid(Arena &A, int R, int P, int chunk, size_t table_elems, size_t grid_cells, GridSpace *s,
+                       int nw = 1) {
     size_t n = (size_t)(R > 0 ? R : 1);
     size_t nitems = n + n / (size_t)chunk + 2;
     s->pos = A.take<int4>(n);
@@ -838,8 +1243,13 @@ static void carve_grid(Arena &A, int R, int P, int chunk, size_t table_elems, si
     s->stats = A.take<unsigned long long>(4);
     s->cub_bytes = cub_bytes((int)n);
     s->cub = A.take<char>(s->cub_bytes);
+    s->ptab = A.take<float2>(table_elems ? table_elems : 1);
     s->table2 = A.take<float4>(table_elems ? table_elems : 1);
-    s->delta = A.take<float>(grid_cells ? grid_cells * 2 * P : 1);
+    s->pbase = A.take<int>(nw > 0 ? nw : 1);
+    s->split = A.take<int>(1);
+    s->counter4 = A.take<int>(1);
+    s->err = A.take<int>(1);
+    s->delta = A.take<double>(grid_cells ? grid_cells * 2 * P : 1);
 }
 
 // float2 elements of the kernel table described by conv_info
@@ -848,6 +1258,16 @@ static size_t table_elems_of(const mtb_grid_params *p, const int *h_conv_info) {
     for (int k = 0; k < p->wplanes; k++) {
         size_t S = (size_t)(h_conv_info[2 * k] > 0 ? h_conv_info[2 * k] : 0);
         n = std::max(n, (size_t)(h_conv_info[2 * k + 1] > 0 ? h_conv_info[2 * k + 1] : 0) + T * T * S * S);
+    }
+    return n;
+}
+
+// float2 elements of the row-padded table (rows of S + 1 taps)
+static size_t padded_elems_of(const mtb_grid_params *p, const int *h_conv_info) {
+    size_t T = (size_t)oversample_T(p->sampling), n = 0;
+    for (int k = 0; k < p->wplanes; k++) {
+        size_t S = (size_t)(h_conv_info[2 * k] > 0 ? h_conv_info[2 * k] : 0);
+        n += T * T * S * (S + 1);
     }
     return n;
 }
@@ -867,6 +1287,7 @@ static int check_params(const mtb_grid_params *p) {
     if (!(p->u_increment > 0.0) || !(p->v_increment > 0.0) || !(p->w_sq_increment > 0.0)) return MTB_ERR_BAD_PARAM;
     if (p->tile < 0 || p->support_bucket < 0 || p->max_chunk < 0) return MTB_ERR_BAD_PARAM;
     if (p->merge < 0 || p->merge > 2) return MTB_ERR_BAD_PARAM;
+    if (p->bulk_min_support < 0) return MTB_ERR_BAD_PARAM;
     return MTB_OK;
 }
 
@@ -879,7 +1300,9 @@ static int make_plan(const mtb_grid_params *p, const int *h_conv_info, GridPlan 
     g->bt.half = half;
     for (int k = 0; k < p->wplanes; k++) {
         int S = h_conv_info[2 * k];
-        if (S < 1 || S % 2 == 0 || S > 4095 || S >= p->nx || S >= p->ny) return MTB_ERR_KERNEL;
+        // the direct gridders lay one support-box column per thread of a
+        // 256-thread block: supports up to 255
+        if (S < 1 || S % 2 == 0 || S > 255 || S >= p->nx || S >= p->ny) return MTB_ERR_KERNEL;
         int b = (S - 1) / (2 * half);
         if (b >= kMaxBuckets) return MTB_ERR_BAD_PARAM;
         g->bt.M[b] = std::max(g->bt.M[b], S);
@@ -936,8 +1359,20 @@ static int launch_bucket(GridArgs a, const Launch &L, cudaStream_t st) {
     return L.window ? launch_one<P, 8, true>(a, L, st) : launch_one<P, 8, false>(a, L, st);
 }
 
+// MTB_CHECK_GRIDDER=1: every mtb_grid call synchronises its stream and reports
+// a gridder pipeline timeout as MTB_ERR_KERNEL (a debugging aid; off by default).
+static bool check_gridder() {
+    static int v = -1;
+    if (v < 0) {
+        const char *e = std::getenv("MTB_CHECK_GRIDDER");
+        v = (e && e[0] && e[0] != '0') ? 1 : 0;
+    }
+    return v == 1;
+}
+
 template <int P>
 static int run_grid(const mtb_grid_params *p, const GridPlan &plan, const float2 *table, size_t table_elems,
+                    size_t padded,
                     const int *conv_info,
                     const float *conv_sums, const float *uvw, const float *freq, const float2 *vis,
                     const float *weights, const int *flags, int R, float *grid, float *grid_lo,
@@ -977,10 +1412,13 @@ static int run_grid(const mtb_grid_params *p, const GridPlan &plan, const float2
     MTB_LAUNCHED();
     if (p->merge == 1)
         k_gather<P, false><<<blocks, 256, 0, st>>>(R, s.skeys, s.sidx, s.pos, s.meta, vis, weights, flags, s.wpos,
-                                                   s.wvis, plan.bt, p->nx);
-    else
+                                                   s.wvis, plan.bt, p->nx, nullptr, nullptr, 0);
+    else {
+        k_pad_bases<<<1, 1, 0, st>>>(conv_info, p->wplanes, T, s.pbase);
+        MTB_LAUNCHED();
         k_gather<P, true><<<blocks, 256, 0, st>>>(R, s.skeys, s.sidx, s.pos, s.meta, vis, weights, flags, s.wpos,
-                                                  s.wvis, plan.bt, p->nx);
+                                                  s.wvis, plan.bt, p->nx, conv_info, s.pbase, p->wplanes);
+    }
     MTB_LAUNCHED();
     (void)end_bit;
 
@@ -999,7 +1437,7 @@ static int run_grid(const mtb_grid_params *p, const GridPlan &plan, const float2
     if (p->merge != 1) {
         Grid2Args g2;
         g2.items = s.items;
-        g2.n_items = s.n_items;
+        g2.n_items = s.split;            // k_grid3 takes the items before the split
         g2.counter = s.counters;
         g2.wpos = s.wpos;
         g2.wvis = s.wvis;
@@ -1007,32 +1445,59 @@ static int run_grid(const mtb_grid_params *p, const GridPlan &plan, const float2
         g2.table2 = s.table2;
         {
             int eb = (int)std::min<size_t>((table_elems + 255) / 256, (size_t)sms * 16);
-            k_expand_table<<<eb > 0 ? eb : 1, 256, 0, st>>>(table, s.table2, table_elems);
+            k_pad_table<<<eb > 0 ? eb : 1, 256, 0, st>>>(table, table_elems, conv_info, s.pbase, p->wplanes, s.ptab);
+            MTB_LAUNCHED();
+            int pb = (int)std::min<size_t>((padded + 255) / 256, (size_t)sms * 16);
+            k_expand_table<<<pb > 0 ? pb : 1, 256, 0, st>>>(s.ptab, s.table2, padded);
             MTB_LAUNCHED();
         }
-        // compensated mode: the call grids into a zeroed delta grid with plain
-        // vector reductions (no returned values, so no stall at a flush) and
-        // one pass merges it into (grid, grid_lo) afterwards
+        MTB_CUDA_TRY(cudaMemsetAsync(s.counter4, 0, sizeof(int), st));
+        MTB_CUDA_TRY(cudaMemsetAsync(s.err, 0, sizeof(int), st));
+        // k_grid4 is opt-in: it measured slower than k_grid3 on the mid-size
+        // workload (45.6 vs 30.7 ms per 29 M-record call)
+        const int min_m = p->bulk_min_support > 0 ? p->bulk_min_support : (1 << 30);
+        k_split<<<1, 1, 0, st>>>(s.bounds, s.n_items, plan.bt, min_m < kG4MinM ? kG4MinM : min_m, s.split);
+        MTB_LAUNCHED();
+        // compensated mode: the call's flushes go to a zeroed FP64 delta grid
+        // with plain reductions (no returned values, so no stall at a flush)
+        // and one pass merges it into the float pair (grid, grid_lo)
         const size_t nfloat = (size_t)p->nx * p->ny * 2 * P;
-        if (grid_lo) MTB_CUDA_TRY(cudaMemsetAsync(s.delta, 0, nfloat * sizeof(float), st));
+        if (grid_lo) MTB_CUDA_TRY(cudaMemsetAsync(s.delta, 0, nfloat * sizeof(double), st));
         g2.wvis4 = (const float4 *)s.wvis;
-        g2.grid = grid_lo ? s.delta : grid;
+        g2.grid = grid;
+        g2.dgrid = grid_lo ? s.delta : nullptr;
         g2.grid_lo = nullptr;
         g2.nx = p->nx;
         g2.bt = plan.bt;
         int ls = launch_grid3<P>(g2, st);
         if (ls != MTB_OK) return ls;
+        Grid4Args g4;
+        g4.items = s.items;
+        g4.first = s.split;
+        g4.n_items = s.n_items;
+        g4.counter = s.counter4;
+        g4.wpos = s.wpos;
+        g4.wvis4 = (const float4 *)s.wvis;
+        g4.ptab = s.ptab;
+        g4.grid = g2.grid;
+        g4.dgrid = g2.dgrid;
+        g4.nx = p->nx;
+        g4.bt = plan.bt;
+        g4.err = s.err;
+        ls = launch_grid4<P>(g4, st);
+        if (ls != MTB_OK) return ls;
+        if (check_gridder()) {
+            int e = 0;
+            MTB_CUDA_TRY(cudaMemcpyAsync(&e, s.err, sizeof(int), cudaMemcpyDeviceToHost, st));
+            MTB_CUDA_TRY(cudaStreamSynchronize(st));
+            if (e) return MTB_ERR_KERNEL;
+        }
         if (grid_lo) {
-            const size_t n4 = nfloat / 4;
-            int mb = (int)std::min<size_t>((n4 + 255) / 256, (size_t)sms * 16);
-            k_merge_delta<<<mb > 0 ? mb : 1, 256, 0, st>>>((float4 *)grid, (float4 *)grid_lo,
-                                                         (const float4 *)s.delta, n4);
+            const size_t n2 = nfloat / 2;     // complex values
+            int mb = (int)std::min<size_t>((n2 + 255) / 256, (size_t)sms * 16);
+            k_merge_delta<<<mb > 0 ? mb : 1, 256, 0, st>>>((float2 *)grid, (float2 *)grid_lo,
+                                                         (const double2 *)s.delta, n2);
             MTB_LAUNCHED();
-            if (nfloat % 4) {
-                // odd cell count with one polarisation: the last cell alone
-                k_merge_delta_tail<<<1, 1, 0, st>>>(grid, grid_lo, s.delta, nfloat);
-                MTB_LAUNCHED();
-            }
         }
         if (p->gridder_end_event) MTB_CUDA_TRY(cudaEventRecord((cudaEvent_t)p->gridder_end_event, st));
         k_finish<<<1, 32, 0, st>>>(P, s.norm_acc, normalizer, s.stats, stats);
@@ -1087,7 +1552,8 @@ extern "C" int mtb_grid_workspace_size(const mtb_grid_params *p, const int *h_co
     int chunk = effective_chunk(p);
     Arena A;
     GridSpace s;
-    carve_grid(A, nrecords, p->npol, chunk, table_elems_of(p, h_conv_info), (size_t)p->nx * p->ny, &s);
+    carve_grid(A, nrecords, p->npol, chunk, padded_elems_of(p, h_conv_info), (size_t)p->nx * p->ny, &s,
+               p->wplanes);
     *bytes = A.used;
     return MTB_OK;
 }
@@ -1118,18 +1584,20 @@ extern "C" int mtb_grid(const mtb_grid_params *p, const void *d_table, const int
         return MTB_ERR_NULL;
     Arena A(d_workspace, workspace_bytes);
     GridSpace s;
-    carve_grid(A, nrecords, P, plan.chunk, table_elems_of(p, h_conv_info), (size_t)p->nx * p->ny, &s);
+    carve_grid(A, nrecords, P, plan.chunk, padded_elems_of(p, h_conv_info), (size_t)p->nx * p->ny, &s,
+               p->wplanes);
     if (!A.ok()) return MTB_ERR_WORKSPACE;
     const float2 *tb = (const float2 *)d_table;
     const float2 *vis = (const float2 *)d_vis;
     float *g = (float *)d_grid, *lo = (float *)d_grid_lo;
+    const size_t te = table_elems_of(p, h_conv_info), pe = padded_elems_of(p, h_conv_info);
     if (P == 1)
-        return run_grid<1>(p, plan, tb, table_elems_of(p, h_conv_info), d_conv_info, d_conv_sums, d_uvw, d_freq, vis, d_weights, d_flags,
+        return run_grid<1>(p, plan, tb, te, pe, d_conv_info, d_conv_sums, d_uvw, d_freq, vis, d_weights, d_flags,
                            nrecords, g, lo, d_normalizer, d_stats, s, st);
     if (P == 2)
-        return run_grid<2>(p, plan, tb, table_elems_of(p, h_conv_info), d_conv_info, d_conv_sums, d_uvw, d_freq, vis, d_weights, d_flags,
+        return run_grid<2>(p, plan, tb, te, pe, d_conv_info, d_conv_sums, d_uvw, d_freq, vis, d_weights, d_flags,
                            nrecords, g, lo, d_normalizer, d_stats, s, st);
-    return run_grid<4>(p, plan, tb, table_elems_of(p, h_conv_info), d_conv_info, d_conv_sums, d_uvw, d_freq, vis, d_weights, d_flags, nrecords,
+    return run_grid<4>(p, plan, tb, te, pe, d_conv_info, d_conv_sums, d_uvw, d_freq, vis, d_weights, d_flags, nrecords,
                        g, lo, d_normalizer, d_stats, s, st);
 }
 

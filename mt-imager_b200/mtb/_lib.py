@@ -53,7 +53,8 @@ class GridParams(ctypes.Structure):
                 ("wplanes", ctypes.c_int), ("u_increment", ctypes.c_double), ("v_increment", ctypes.c_double),
                 ("w_sq_increment", ctypes.c_double), ("initialize_output", ctypes.c_int), ("tile", ctypes.c_int),
                 ("support_bucket", ctypes.c_int), ("max_chunk", ctypes.c_int), ("merge", ctypes.c_int),
-                ("gridder_start_event", ctypes.c_void_p), ("gridder_end_event", ctypes.c_void_p)]
+                ("gridder_start_event", ctypes.c_void_p), ("gridder_end_event", ctypes.c_void_p),
+                ("bulk_min_support", ctypes.c_int)]
 
 
 class GridStats(ctypes.Structure):

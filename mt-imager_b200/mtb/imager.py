@@ -85,7 +85,7 @@ class WProjectionImager:
 
     def __init__(self, nx, ny, l_increment, m_increment=None, wplanes=32, sampling=8, npol=4,
                  trial_support=0, max_support=0, w_max=0.0, pol_type=L.MTB_POL_LINEAR, compensated=True,
-                 tile=0, support_bucket=0, max_chunk=0, merge=0, device="cuda",
+                 tile=0, support_bucket=0, max_chunk=0, merge=0, bulk_min_support=0, device="cuda",
                  kernels: KernelTable | None = None):
         self.lib = L.load()
         self.device = torch.device(device)
@@ -96,7 +96,8 @@ class WProjectionImager:
         self.kernels = kernels
         self.compensated = compensated
         self.pol_type = pol_type
-        self.tuning = dict(tile=tile, support_bucket=support_bucket, max_chunk=max_chunk, merge=merge)
+        self.tuning = dict(tile=tile, support_bucket=support_bucket, max_chunk=max_chunk, merge=merge,
+                           bulk_min_support=bulk_min_support)
         self.grid = torch.zeros((ny, nx, npol), dtype=torch.complex64, device=self.device)
         self.grid_lo = torch.zeros_like(self.grid) if compensated else None
         self.normalizer = torch.zeros(npol, dtype=torch.float32, device=self.device)
@@ -120,6 +121,7 @@ class WProjectionImager:
                           k.info.u_increment, k.info.v_increment, k.info.w_sq_increment, int(initialize),
                           self.tuning["tile"], self.tuning["support_bucket"], self.tuning["max_chunk"],
                           self.tuning["merge"])
+        gp.bulk_min_support = self.tuning["bulk_min_support"]
         if self.gridder_events is not None:
             gp.gridder_start_event = self.gridder_events[0].cuda_event
             gp.gridder_end_event = self.gridder_events[1].cuda_event

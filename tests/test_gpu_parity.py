@@ -159,7 +159,8 @@ def test_chunked_equals_single(cfg1):
 
 
 @pytest.mark.parametrize("tuning", [dict(tile=16), dict(tile=64), dict(support_bucket=3), dict(max_chunk=37),
-                                    dict(merge=1), dict(merge=2), dict(merge=1, tile=16)])
+                                    dict(merge=1), dict(merge=2), dict(merge=1, tile=16),
+                                    dict(bulk_min_support=17), dict(bulk_min_support=25)])
 def test_tuning_does_not_change_result(cfg1, tuning):
     obs, setup, geo, kern, img_o, grid_o, norm_o = cfg1
     im, img = run_gpu(obs, setup, **tuning)
@@ -168,18 +169,21 @@ def test_tuning_does_not_change_result(cfg1, tuning):
     assert rel_rms(img[0], img_o[0]) <= IMAGE_RMS_TOL
 
 
-@pytest.mark.parametrize("kw", [dict(), dict(tile=64), dict(nx=320, s=3), dict(merge=1)])
+@pytest.mark.parametrize("kw", [dict(), dict(tile=64), dict(nx=320, s=3), dict(merge=1),
+                                dict(bulk_min_support=17), dict(nx=320, s=3, bulk_min_support=17)])
 def test_large_supports(oracle, kw):
-    """Supports up to 55 (and 105 with odd sampling): register-tile widths 1,
-    2 and 8, the shared-memory window and the direct-merge variants, and
-    support bands split across blocks."""
+    """Supports up to 55 (and 105 with odd sampling): the per-thread and the
+    bulk-copy direct gridders (one and several passes, one and several record
+    streams), the shared-memory window variant, and support bands split across
+    blocks."""
     tile = kw.pop("tile", 0)
     merge = kw.pop("merge", 0)
+    bulk = kw.pop("bulk_min_support", 0)
     obs, setup = wide_case(**kw)
     geo = oracle.geometry_for(setup)
     kern = oracle.wkernels(geo)
     img_o, grid_o, norm_o = oracle.image_channel(obs, 0, setup, kern, geo)
-    im, img = run_gpu(obs, setup, tile=tile, merge=merge)
+    im, img = run_gpu(obs, setup, tile=tile, merge=merge, bulk_min_support=bulk)
     assert np.array_equal(im.kernels.conv_info, kern["conv_info"])
     assert np.abs(im.kernels.table.cpu().numpy() - kern["table"]).max() <= KERNEL_TOL
     g = im.grid_sum().cpu().numpy()
@@ -232,14 +236,17 @@ def test_empty_and_fully_rejected_chunks(oracle):
 
 
 def test_compensated_merge_tracks_fp64(cfg1):
-    """The two-float grid is at least as close to the FP64 grid as the plain
-    FP32 one."""
+    """Accumulated over many chunks, the two-float grid stays at least as close
+    to the FP64 grid as plain FP32 accumulation (within one chunk both
+    accumulate identically, so only the cross-chunk merge can differ; the
+    slack covers the unspecified order of the FP32 reductions)."""
     obs, setup, geo, kern, img_o, grid_o, norm_o = cfg1
-    a, _ = run_gpu(obs, setup, compensated=True)
-    b, _ = run_gpu(obs, setup, compensated=False)
-    ea = np.abs(a.grid_sum().cpu().numpy() - grid_o).max()
-    eb = np.abs(b.grid.cpu().numpy() - grid_o).max()
-    assert ea <= eb * 1.0001
+    a, _ = run_gpu(obs, setup, chunks=16, compensated=True)
+    b, _ = run_gpu(obs, setup, chunks=16, compensated=False)
+    ea = np.sqrt(np.mean(np.abs(a.grid_sum().cpu().numpy() - grid_o) ** 2))
+    eb = np.sqrt(np.mean(np.abs(b.grid.cpu().numpy() - grid_o) ** 2))
+    assert ea <= eb * 1.02
+    assert np.abs(a.grid_sum().cpu().numpy() - grid_o).max() <= GRID_TOL * np.abs(grid_o).max()
 
 
 def test_status_codes(oracle):
