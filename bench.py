@@ -245,7 +245,7 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="mtb", choices=["mtb", "reference"])
-    ap.add_argument("--config", default="mid", choices=["mid", "small"])
+    ap.add_argument("--config", default="mid", choices=["mid", "small", "serve"])
     ap.add_argument("--channels", type=int, default=16)
     ap.add_argument("--hours", type=float, default=8.0)
     ap.add_argument("--e2e-steps", type=int, default=1)
@@ -257,6 +257,12 @@ def main():
     ap.add_argument("--merge", type=int, default=0)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-serve", action="store_true", help="skip the request-stream measurement")
+    ap.add_argument("--serve-requests", type=int, default=24)
+    ap.add_argument("--serve-rate", type=float, default=20.0, help="Poisson arrival rate, requests per second")
+    ap.add_argument("--serve-min-records", type=float, default=1e5)
+    ap.add_argument("--serve-max-records", type=float, default=2e6)
+    ap.add_argument("--serve-slots", type=int, default=4)
     ap.add_argument("--profile-range", action="store_true",
                     help="bracket the timed steps with cudaProfilerStart/Stop (for ncu --profile-from-start off)")
     args = ap.parse_args()
@@ -275,6 +281,18 @@ def main():
 
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
+    if args.config == "serve":
+        if rank == 0:
+            sv = run_serve(args, torch, dev)
+            print(json.dumps({"metric": METRIC, "value": sv["engine"]["samples_per_s"], "unit": "samples/s",
+                              "n_gpus": 1, "higher_is_better": True, "impl": "mtb-engine", "data": "synthetic",
+                              "config": {"workload": "request stream: %d requests, Poisson %.3g/s, images "
+                                                     "512^2-4096^2, records %.3g-%.3g log-uniform"
+                                                     % (args.serve_requests, args.serve_rate,
+                                                        args.serve_min_records, args.serve_max_records)},
+                              "latency_ms": {"p50": sv["engine"]["p50_ms"], "p99": sv["engine"]["p99_ms"]},
+                              "serving": sv}), flush=True)
+        return
     if world > 1:
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
@@ -394,6 +412,15 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline(args, spec, uvw, chans, kern, dl, torch)
 
+    # ---- request stream: engine vs plain path (rank 0, one GPU)
+    serve = None
+    if rank == 0 and world == 1 and not args.no_serve:
+        chans.clear()
+        imagers.clear()
+        images.clear()
+        torch.cuda.empty_cache()
+        serve = run_serve(args, torch, dev)
+
     if rank == 0:
         sup = kern.supports
         line = {
@@ -417,6 +444,8 @@ def main():
             line["cpu_baseline"] = cpu
         if clk:
             line["clocks"] = clk
+        if serve:
+            line["serving"] = serve
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
@@ -484,6 +513,118 @@ def run_e2e(args, torch, dev, uvw_d, chans, imagers, images, samples_per_step, w
         ms = float(tt.item())
     return {"value": samples_per_step * world / (ms * 1e-3), "unit": "samples/s", "h2d_bytes_per_step": int(h2d),
             "d2h_bytes_per_step": int(d2h), "ms_per_step": ms}
+
+
+# ---------------------------------------------------------------- serving --
+SERVE_WPLANES = {512: 32, 1024: 64, 2048: 96, 4096: 128}
+
+
+def make_requests(args, torch, dev, rng):
+    """A stream of imaging requests in the shape of the serving configuration:
+    image size uniform over {512, 1024, 2048, 4096}^2, record counts
+    log-uniform in [serve_min_records, serve_max_records] (synthetic 64-antenna
+    tracks: a contiguous slice of an 8 h, 2 s track, so records keep their
+    baseline-major order), 4 pol, point-source skies, 10 % of records flagged,
+    w-planes 32-128 by image size, Poisson arrivals at serve_rate per second."""
+    from mtb import synth
+    spec = workload_spec(argparse.Namespace(config="mid", channels=1, hours=8.0))
+    pool, _, _ = make_uvw(spec, dev, torch, rng)
+    Rp = pool.shape[1]
+    uv_max = float(pool[:2].abs().max())
+    gen = torch.Generator(device=dev).manual_seed(11)
+    reqs = []
+    t = 0.0
+    for k in range(args.serve_requests):
+        n = int(rng.choice([512, 1024, 2048, 4096]))
+        R = int(math.exp(rng.uniform(math.log(args.serve_min_records), math.log(args.serve_max_records))))
+        R = min(R, Rp)
+        s0 = int(rng.integers(0, Rp - R + 1))
+        f = float(rng.uniform(1.3e9, 1.5e9))
+        sp = dict(spec, nx=n, f_hi=1.5e9)
+        dl = cell_for(sp, uv_max, torch)
+        uvw = pool[:, s0:s0 + R].contiguous()
+        srcs = synth.random_sources(3, n * dl, rng, flux=(0.1, 1.0))
+        vis = make_vis(uvw, f, srcs, torch, gen)
+        flags = (torch.rand(R, device=dev, generator=gen) < 0.1).int()[:, None].repeat(1, 4)
+        t += float(rng.exponential(1.0 / args.serve_rate))
+        reqs.append(dict(nx=n, dl=dl, wplanes=SERVE_WPLANES[n], arrival=t, uvw=uvw.cpu().numpy(),
+                         freq=np.full(R, f / C_LIGHT, np.float32), vis=vis.cpu().numpy(),
+                         weights=np.ones((R, 4), np.float32), flags=flags.cpu().numpy()))
+    return reqs
+
+
+def run_serve(args, torch, dev):
+    """The request stream through (a) the engine (continuous batching,
+    w-kernel cache, overlapping slots) with real-time Poisson arrivals, and
+    (b) the plain path, one request at a time in arrival order, each building
+    its w-kernels as the reference does per run.  Reports p50/p99 latency
+    (arrival to image on the host) and samples/s over the stream for both."""
+    from mtb.engine import Engine
+    from mtb.imager import WProjectionImager
+    rng = np.random.default_rng(5)
+    reqs = make_requests(args, torch, dev, rng)
+    torch.cuda.synchronize()
+    common = dict(sampling=8, trial_support=67, max_support=65)
+
+    # (b) plain path: service times measured back to back, then FIFO queueing
+    service = []
+    samples_plain = 0
+    for r in reqs:
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        im = WProjectionImager(r["nx"], r["nx"], r["dl"], wplanes=r["wplanes"], device=dev, **common)
+        im.build_kernels()
+        R = r["freq"].size
+        for a in range(0, R, 1 << 22):
+            b = min(R, a + (1 << 22))
+            im.grid_chunk(r["uvw"][:, a:b], r["freq"][a:b], r["vis"][a:b], r["weights"][a:b], r["flags"][a:b])
+        img = im.finalize().cpu().numpy()
+        service.append(time.perf_counter() - t0)
+        st = im.statistics()
+        samples_plain += (st["gridded_records"] + st["compressed_records"]) * 4
+        del im, img
+    done, lat_plain = 0.0, []
+    for r, sv in zip(reqs, service):
+        start = max(r["arrival"], done)
+        done = start + sv
+        lat_plain.append((done - r["arrival"]) * 1e3)
+    span_plain = done - reqs[0]["arrival"]
+
+    # (a) engine, real-time arrivals
+    results = []
+    with Engine(slots=args.serve_slots) as eng:
+        # warm the engine's CUDA state outside the measured stream
+        t_base = time.perf_counter()
+        tickets = []
+        for r in reqs:
+            now = time.perf_counter() - t_base
+            if r["arrival"] > now:
+                time.sleep(r["arrival"] - now)
+            sub = time.perf_counter() - t_base
+            tickets.append((sub, eng.submit(r["nx"], r["nx"], r["dl"], r["dl"], r["wplanes"], 8, r["uvw"], r["freq"],
+                                            r["vis"], r["weights"], r["flags"], trial_support=67,
+                                            max_support=65)))
+        for sub, tk in tickets:
+            res = eng.wait(tk)
+            if res.status != 0:
+                raise RuntimeError("engine request failed: status %d" % res.status)
+            results.append((sub, res))
+    samples_eng = sum((res.stats["gridded_records"] + res.stats["compressed_records"]) * 4 for _, res in results)
+    lat_eng = [res.latency_ms for _, res in results]
+    end = max(sub + res.latency_ms * 1e-3 for sub, res in results)
+    span_eng = end - results[0][0]
+    hits = sum(res.kernel_cache_hit for _, res in results)
+    recs = [r["freq"].size for r in reqs]
+    return {
+        "requests": len(reqs), "arrival_rate_per_s": args.serve_rate, "slots": args.serve_slots,
+        "image_sizes": [512, 1024, 2048, 4096],
+        "records": {"min": int(min(recs)), "max": int(max(recs)), "total": int(sum(recs))},
+        "engine": {"samples_per_s": samples_eng / span_eng, "p50_ms": float(np.percentile(lat_eng, 50)),
+                   "p99_ms": float(np.percentile(lat_eng, 99)), "makespan_s": span_eng, "kernel_cache_hits": hits},
+        "plain": {"samples_per_s": samples_plain / span_plain, "p50_ms": float(np.percentile(lat_plain, 50)),
+                  "p99_ms": float(np.percentile(lat_plain, 99)), "makespan_s": span_plain},
+        "speedup_samples_per_s": (samples_eng / span_eng) / (samples_plain / span_plain),
+    }
 
 
 def cpu_baseline(args, spec, uvw_d, chans, kern, dl, torch, min_seconds=12.0, max_passes=40):

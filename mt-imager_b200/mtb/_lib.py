@@ -14,6 +14,7 @@ PKG = os.path.dirname(HERE)
 LIB_PATH = os.path.join(PKG, "libmtb.so")
 
 MTB_OK = 0
+MTB_ERR_CAPACITY = 4
 MTB_ERR_TOO_LARGE = 9
 MTB_POL_LINEAR = 0
 MTB_POL_CIRCULAR = 1
@@ -24,6 +25,7 @@ EXPORTS = (
     "mtb_preprocess_uvw_noalloc", "mtb_preprocess_uvw_noalloc_capacity",
     "mtb_finalize_workspace_size", "mtb_finalize", "mtb_status_string", "mtb_version",
     "mtb_release_caches", "mtb_kernel_launch_count", "mtb_calibrate_fp32",
+    "mtb_engine_create", "mtb_engine_submit", "mtb_engine_wait", "mtb_engine_request_bytes", "mtb_engine_destroy",
 )
 
 
@@ -67,6 +69,23 @@ class FinalizeParams(ctypes.Structure):
                 ("pol_type", ctypes.c_int)]
 
 
+class EngineConfig(ctypes.Structure):
+    _fields_ = [("slots", ctypes.c_int), ("hbm_budget_bytes", ctypes.c_size_t),
+                ("kernel_cache_bytes", ctypes.c_size_t), ("chunk_records", ctypes.c_int)]
+
+
+class ImageRequest(ctypes.Structure):
+    _fields_ = [("geometry", WKernelParams), ("npol", ctypes.c_int), ("pol_type", ctypes.c_int),
+                ("compensated", ctypes.c_int), ("nrecords", ctypes.c_int), ("uvw", ctypes.c_void_p),
+                ("freq", ctypes.c_void_p), ("vis", ctypes.c_void_p), ("weights", ctypes.c_void_p),
+                ("flags", ctypes.c_void_p), ("image", ctypes.c_void_p)]
+
+
+class ImageResult(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int), ("kernel_cache_hit", ctypes.c_int), ("queue_ms", ctypes.c_double),
+                ("service_ms", ctypes.c_double), ("latency_ms", ctypes.c_double), ("stats", GridStats)]
+
+
 _lib = None
 
 
@@ -99,6 +118,11 @@ def load(path: str = LIB_PATH):
     L.mtb_kernel_launch_count.restype = ctypes.c_ulonglong
     L.mtb_kernel_launch_count.argtypes = []
     L.mtb_calibrate_fp32.argtypes = [ctypes.POINTER(ctypes.c_double), p]
+    L.mtb_engine_create.argtypes = [ctypes.POINTER(EngineConfig), ctypes.POINTER(p)]
+    L.mtb_engine_submit.argtypes = [p, ctypes.POINTER(ImageRequest), ctypes.POINTER(ctypes.c_longlong)]
+    L.mtb_engine_wait.argtypes = [p, ctypes.c_longlong, ctypes.POINTER(ImageResult)]
+    L.mtb_engine_request_bytes.argtypes = [p, ctypes.POINTER(ImageRequest), ctypes.POINTER(sz)]
+    L.mtb_engine_destroy.argtypes = [p]
     _lib = L
     return L
 
