@@ -114,6 +114,15 @@ int mtb_wkernel_build(const mtb_wkernel_params *p, void *d_workspace, size_t wor
                       void *d_table, size_t table_capacity, int *d_conv_info, int *h_conv_info,
                       float *d_conv_sums, size_t *table_elems, mtb_stream_t stream);
 
+/* The taper-only gridding kernel of mode=normal (OnlyTaperConvFunction.cpp:29-99):
+ * the uv-plane prolate-spheroidal function of CasaGridSF.cu:107-149, per axis
+ * (1 - nu^2) grdsf(nu) with nu = d / (3 sampling), evaluated in FP64, in the
+ * table / convInfo / ConvSums format of mtb_wkernel_build with one plane
+ * (grid with wplanes = 1 and w_sq_increment = 1).  Synchronises `stream`.
+ *   d_table  out float2 [T*T*support*support]  (table_capacity at least that) */
+int mtb_taper_kernel_build(int support, int sampling, void *d_table, size_t table_capacity, int *d_conv_info,
+                           int *h_conv_info, float *d_conv_sums, size_t *table_elems, mtb_stream_t stream);
+
 /* ------------------------------------------------------------- gridding -- */
 typedef struct mtb_grid_params {
     int nx, ny;              /* uvImage.columns, uvImage.rows                          */
@@ -137,6 +146,9 @@ typedef struct mtb_grid_params {
     int bulk_min_support;      /* 0: off (default); > 0: bucket moduli from max(17, value) up
                                   are gridded by the bulk-copy gridder (cp.async.bulk rows,
                                   mbarrier pipeline), the rest by the per-thread gridder   */
+    int psf;                   /* 1: grid every visibility as 1 + 0i (the PSF; mt-imager's
+                                  psf=true, VisibilityForPSFStorageManager.cpp:65-77);
+                                  d_vis may then be NULL                                   */
 } mtb_grid_params;
 
 typedef struct mtb_grid_stats {

@@ -131,15 +131,38 @@ private:
     KernelTable() = default;
 };
 
+// Device buffers an Imager works in.  Grow-only: a Buffers object kept across
+// images (one per stream in a server) is reused without new allocations once
+// it has seen the largest image.
+struct ImagerBuffers {
+    DeviceArray<float2> grid, lo;
+    DeviceArray<float> norm;
+    DeviceArray<mtb_grid_stats> stats;
+    DeviceArray<unsigned char> ws, fin;
+
+    template <class T>
+    static void ensure(DeviceArray<T> &a, size_t n, cudaStream_t s) {
+        if (a.size() < n) a = DeviceArray<T>(n, s);
+    }
+};
+
 class Imager {
 public:
-    Imager(std::shared_ptr<const KernelTable> k, int npol, int pol_type, bool compensated, cudaStream_t stream)
-        : k_(std::move(k)), npol_(npol), pol_type_(pol_type), s_(stream) {
+    // buffers: kept by the caller and reused across images, or nullptr to let
+    // the imager own its own
+    Imager(std::shared_ptr<const KernelTable> k, int npol, int pol_type, bool compensated, cudaStream_t stream,
+           ImagerBuffers *buffers = nullptr)
+        : k_(std::move(k)), npol_(npol), pol_type_(pol_type), compensated_(compensated), s_(stream) {
+        if (!buffers) {
+            own_.reset(new ImagerBuffers());
+            buffers = own_.get();
+        }
+        b_ = buffers;
         const size_t cells = (size_t)k_->params.nx * k_->params.ny * npol;
-        grid_ = DeviceArray<float2>(cells, s_);
-        if (compensated) lo_ = DeviceArray<float2>(cells, s_);
-        norm_ = DeviceArray<float>(npol, s_);
-        stats_ = DeviceArray<mtb_grid_stats>(1, s_);
+        ImagerBuffers::ensure(b_->grid, cells, s_);
+        if (compensated) ImagerBuffers::ensure(b_->lo, cells, s_);
+        ImagerBuffers::ensure(b_->norm, (size_t)npol, s_);
+        ImagerBuffers::ensure(b_->stats, 1, s_);
         reset();
     }
     const KernelTable &kernels() const { return *k_; }
@@ -176,11 +199,11 @@ public:
     void grid(const float *uvw, const float *freq, const void *vis, const float *weights, const int *flags,
               int records) {
         mtb_grid_params gp = grid_params();
-        const size_t need = workspace_bytes(records);
-        if (ws_.bytes() < need) ws_ = DeviceArray<unsigned char>(need, s_);
+        ImagerBuffers::ensure(b_->ws, workspace_bytes(records), s_);
         check(mtb_grid(&gp, k_->table.data(), k_->conv_info.data(), k_->h_conv_info.data(), k_->conv_sums.data(),
-                       uvw, freq, vis, weights, flags, records, grid_.data(), lo_.data(), norm_.data(),
-                       stats_.data(), ws_.data(), ws_.bytes(), (mtb_stream_t)s_),
+                       uvw, freq, vis, weights, flags, records, b_->grid.data(),
+                       compensated_ ? b_->lo.data() : nullptr, b_->norm.data(), b_->stats.data(), b_->ws.data(),
+                       b_->ws.bytes(), (mtb_stream_t)s_),
               "mtb_grid");
         fresh_ = false;
     }
@@ -195,16 +218,16 @@ public:
         fp.pol_type = pol_type_;
         size_t need = 0;
         check(mtb_finalize_workspace_size(&fp, &need), "mtb_finalize_workspace_size");
-        if (fin_.bytes() < need) fin_ = DeviceArray<unsigned char>(need, s_);
-        check(mtb_finalize(&fp, grid_.data(), lo_.data(), norm_.data(), image, fin_.data(), fin_.bytes(),
-                           (mtb_stream_t)s_),
+        ImagerBuffers::ensure(b_->fin, need, s_);
+        check(mtb_finalize(&fp, b_->grid.data(), compensated_ ? b_->lo.data() : nullptr, b_->norm.data(), image,
+                           b_->fin.data(), b_->fin.bytes(), (mtb_stream_t)s_),
               "mtb_finalize");
     }
 
     // Statistics of the image so far (synchronises the stream).
     mtb_grid_stats stats() const {
         mtb_grid_stats h;
-        cuda_check(cudaMemcpyAsync(&h, stats_.data(), sizeof(h), cudaMemcpyDeviceToHost, s_), "stats");
+        cuda_check(cudaMemcpyAsync(&h, b_->stats.data(), sizeof(h), cudaMemcpyDeviceToHost, s_), "stats");
         cuda_check(cudaStreamSynchronize(s_), "stats sync");
         return h;
     }
@@ -212,12 +235,11 @@ public:
 private:
     std::shared_ptr<const KernelTable> k_;
     int npol_, pol_type_;
+    bool compensated_;
     cudaStream_t s_;
     bool fresh_ = true;
-    DeviceArray<float2> grid_, lo_;
-    DeviceArray<float> norm_;
-    DeviceArray<mtb_grid_stats> stats_;
-    DeviceArray<unsigned char> ws_, fin_;
+    std::unique_ptr<ImagerBuffers> own_;
+    ImagerBuffers *b_ = nullptr;
 };
 
 }  // namespace mtb

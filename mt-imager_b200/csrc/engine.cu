@@ -13,6 +13,7 @@
 
 #include <algorithm>
 #include <chrono>
+#include <cstdint>
 #include <condition_variable>
 #include <cstring>
 #include <deque>
@@ -129,7 +130,7 @@ struct mtb_engine {
 
     void worker(int slot);
     void run(mtb::Job *j, cudaStream_t st, unsigned char *const pinned[2], unsigned char *const dstage[2],
-             cudaEvent_t const ev[2]);
+             cudaEvent_t const ev[2], mtb::ImagerBuffers &bufs, mtb::DeviceArray<float> &img);
 };
 
 namespace {
@@ -194,6 +195,10 @@ void mtb_engine::worker(int slot) {
              cudaMalloc((void **)&dstage[b], sbytes) == cudaSuccess &&
              cudaEventCreateWithFlags(&ev[b], cudaEventDisableTiming) == cudaSuccess;
     }
+    {
+    // device buffers of this slot, reused (grow-only) by every request it runs
+    mtb::ImagerBuffers bufs;
+    mtb::DeviceArray<float> img;
     for (;;) {
         mtb::Job *j = nullptr;
         {
@@ -206,7 +211,7 @@ void mtb_engine::worker(int slot) {
             j->t_admit = mtb::Clock::now();
         }
         if (ok) {
-            run(j, st, pinned, dstage, ev);
+            run(j, st, pinned, dstage, ev, bufs, img);
         } else {
             j->res.status = MTB_ERR_CUDA;
         }
@@ -221,6 +226,8 @@ void mtb_engine::worker(int slot) {
         }
         cv.notify_all();
     }
+    if (st) cudaStreamSynchronize(st);
+    }   // slot buffers released on the slot's stream
     for (int b = 0; b < 2; b++) {
         if (pinned[b]) cudaFreeHost(pinned[b]);
         if (dstage[b]) cudaFree(dstage[b]);
@@ -230,14 +237,14 @@ void mtb_engine::worker(int slot) {
 }
 
 void mtb_engine::run(mtb::Job *j, cudaStream_t st, unsigned char *const pinned[2], unsigned char *const dstage[2],
-                     cudaEvent_t const ev[2]) {
+                     cudaEvent_t const ev[2], mtb::ImagerBuffers &bufs, mtb::DeviceArray<float> &img) {
     const mtb_image_request &r = j->req;
     const int P = r.npol, R = r.nrecords;
     try {
         bool hit = false;
         std::shared_ptr<mtb::KernelTable> k = cache->get(r.geometry, st, &hit);
         j->res.kernel_cache_hit = hit ? 1 : 0;
-        mtb::Imager im(k, P, r.pol_type, r.compensated != 0, st);
+        mtb::Imager im(k, P, r.pol_type, r.compensated != 0, st, &bufs);
         const int chunk = cfg.chunk_records;
         int b = 0;
         for (int c0 = 0; c0 < R; c0 += chunk, b ^= 1) {
@@ -266,9 +273,11 @@ void mtb_engine::run(mtb::Job *j, cudaStream_t st, unsigned char *const pinned[2
                     (const int *)(d + off_fl), n);
         }
         if (R == 0) im.grid(nullptr, nullptr, nullptr, nullptr, nullptr, 0);
-        mtb::DeviceArray<float> img((size_t)P * r.geometry.nx * r.geometry.ny, st);
+        const size_t npix = (size_t)P * r.geometry.nx * r.geometry.ny;
+        mtb::ImagerBuffers::ensure(img, npix, st);
         im.finalize(img.data());
-        mtb::cuda_check(cudaMemcpyAsync(r.image, img.data(), img.bytes(), cudaMemcpyDeviceToHost, st), "D2H");
+        mtb::cuda_check(cudaMemcpyAsync(r.image, img.data(), npix * sizeof(float), cudaMemcpyDeviceToHost, st),
+                        "D2H");
         j->res.stats = im.stats();   // synchronises the stream
         j->res.status = MTB_OK;
     } catch (const mtb::Error &e) {
@@ -296,6 +305,14 @@ extern "C" int mtb_engine_create(const mtb_engine_config *cfg, mtb_engine **engi
     size_t budget = e->cfg.hbm_budget_bytes ? e->cfg.hbm_budget_bytes : free_b / 10 * 7;
     if (budget <= staging + e->cfg.kernel_cache_bytes) return MTB_ERR_CAPACITY;
     e->budget = budget - staging - e->cfg.kernel_cache_bytes;
+    // keep memory freed by finished requests in the device's stream-ordered
+    // pool instead of returning it to the driver at every synchronisation, so
+    // the next request's cudaMallocAsync is served from the pool
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, e->device) == cudaSuccess) {
+        uint64_t keep = (uint64_t)budget;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
     e->cache.reset(new mtb::KernelCache(e->cfg.kernel_cache_bytes));
     for (int s = 0; s < e->cfg.slots; s++) e->workers.emplace_back(&mtb_engine::worker, e.get(), s);
     *engine = e.release();

@@ -265,7 +265,7 @@ __global__ void k_gather(int R, const unsigned *__restrict__ skeys, const int *_
                          const float2 *__restrict__ vis, const float *__restrict__ weights,
                          const int *__restrict__ flags, int4 *__restrict__ wpos, void *__restrict__ wvis,
                          BucketTable bt, int nx, const int *__restrict__ conv_info, const int *__restrict__ pbase,
-                         int nw) {
+                         int nw, int psf) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < R; i += gridDim.x * blockDim.x) {
         if (skeys[i] == kNoKey) continue;
         int g = sidx[i];
@@ -278,7 +278,7 @@ __global__ void k_gather(int R, const unsigned *__restrict__ skeys, const int *_
             float im = (m & 2) ? -1.0f : 1.0f;
 #pragma unroll
             for (int p = 0; p < P; p++) {
-                float2 v = vis[(size_t)r * P + p];
+                const float2 v = psf ? make_float2(1.0f, 0.0f) : vis[(size_t)r * P + p];
                 float wgt = weights[(size_t)r * P + p];
                 float keep = 1.0f - (float)flags[(size_t)r * P + p];
                 acc[p].x += v.x * wgt * keep;
@@ -1412,12 +1412,12 @@ static int run_grid(const mtb_grid_params *p, const GridPlan &plan, const float2
     MTB_LAUNCHED();
     if (p->merge == 1)
         k_gather<P, false><<<blocks, 256, 0, st>>>(R, s.skeys, s.sidx, s.pos, s.meta, vis, weights, flags, s.wpos,
-                                                   s.wvis, plan.bt, p->nx, nullptr, nullptr, 0);
+                                                   s.wvis, plan.bt, p->nx, nullptr, nullptr, 0, p->psf);
     else {
         k_pad_bases<<<1, 1, 0, st>>>(conv_info, p->wplanes, T, s.pbase);
         MTB_LAUNCHED();
         k_gather<P, true><<<blocks, 256, 0, st>>>(R, s.skeys, s.sidx, s.pos, s.meta, vis, weights, flags, s.wpos,
-                                                  s.wvis, plan.bt, p->nx, conv_info, s.pbase, p->wplanes);
+                                                  s.wvis, plan.bt, p->nx, conv_info, s.pbase, p->wplanes, p->psf);
     }
     MTB_LAUNCHED();
     (void)end_bit;
@@ -1579,8 +1579,8 @@ extern "C" int mtb_grid(const mtb_grid_params *p, const void *d_table, const int
         if (d_stats) MTB_CUDA_TRY(cudaMemsetAsync(d_stats, 0, sizeof(mtb_grid_stats), st));
     }
     if (nrecords == 0) return MTB_OK;
-    if (!d_table || !d_conv_info || !d_conv_sums || !d_uvw || !d_freq || !d_vis || !d_weights || !d_flags ||
-        !d_workspace)
+    if (!d_table || !d_conv_info || !d_conv_sums || !d_uvw || !d_freq || (!d_vis && !p->psf) || !d_weights ||
+        !d_flags || !d_workspace)
         return MTB_ERR_NULL;
     Arena A(d_workspace, workspace_bytes);
     GridSpace s;

@@ -306,3 +306,55 @@ extern "C" int mtb_wkernel_build(const mtb_wkernel_params *p, void *d_workspace,
     MTB_CUDA_TRY(cudaStreamSynchronize(st));
     return MTB_OK;
 }
+
+// ----------------------------------------------------- taper-only kernel --
+// mode=normal (OnlyTaperConvFunction.cpp:29-99): the uv-plane gridding
+// function of CasaGridSF.cu:107-149 -- per axis (1 - nu^2) grdsf(nu) with
+// nu = d / (3 s) for offsets d < 3 s from the centre of a (S s [+1 for even s])^2
+// array, zero beyond -- cut into the [oy][ox][sy][sx] table of one plane by the
+// same rule as ConvFunctionReOrganize.cu:30-71, with its ConvSums.  Small
+// enough to evaluate on the host in FP64.
+extern "C" int mtb_taper_kernel_build(int support, int sampling, void *d_table, size_t table_capacity,
+                                      int *d_conv_info, int *h_conv_info, float *d_conv_sums, size_t *table_elems,
+                                      mtb_stream_t stream) {
+    using namespace mtb;
+    if (!d_table || !h_conv_info || !d_conv_sums || !table_elems) return MTB_ERR_NULL;
+    if (support < 1 || support % 2 == 0 || support > 255 || sampling < 1 || sampling > 64) return MTB_ERR_BAD_PARAM;
+    const int S = support, s = sampling, T = oversample_T(s);
+    const int dim = S * s + ((s & 1) ? 0 : 1);
+    const size_t n = (size_t)T * T * S * S;
+    if (table_capacity < n) return MTB_ERR_CAPACITY;
+    const int zero_at = 3 * s;
+    auto g = [&](int d) {
+        d = d < 0 ? -d : d;
+        if (d >= zero_at) return 0.0;
+        const double nu = (double)d / (double)zero_at;
+        return (1.0 - nu * nu) * grdsf(nu);
+    };
+    const int cb = dim / 2 - ((S / 2) * s + s / 2);
+    std::vector<float2> tab(n);
+    std::vector<float> sums((size_t)T * T);
+    for (int oy = 0; oy < T; oy++)
+        for (int ox = 0; ox < T; ox++) {
+            double sum = 0.0;
+            for (int py = 0; py < S; py++)
+                for (int px = 0; px < S; px++) {
+                    const int yc = py * s + oy + cb, xc = px * s + ox + cb;
+                    const double v = g(yc - dim / 2) * g(xc - dim / 2);
+                    const size_t i = (((size_t)oy * T + ox) * S + py) * S + px;
+                    tab[i] = make_float2((float)v, 0.0f);
+                    sum += (double)(float)v;
+                }
+            sums[(size_t)oy * T + ox] = (float)sum;
+        }
+    cudaStream_t st = (cudaStream_t)stream;
+    h_conv_info[0] = S;
+    h_conv_info[1] = 0;
+    MTB_CUDA_TRY(cudaMemcpyAsync(d_table, tab.data(), n * sizeof(float2), cudaMemcpyHostToDevice, st));
+    MTB_CUDA_TRY(cudaMemcpyAsync(d_conv_sums, sums.data(), sums.size() * sizeof(float), cudaMemcpyHostToDevice, st));
+    if (d_conv_info) MTB_CUDA_TRY(cudaMemcpyAsync(d_conv_info, h_conv_info, 2 * sizeof(int), cudaMemcpyHostToDevice, st));
+    // the host staging vectors go out of scope on return
+    MTB_CUDA_TRY(cudaStreamSynchronize(st));
+    *table_elems = n;
+    return MTB_OK;
+}

@@ -25,6 +25,7 @@ EXPORTS = (
     "mtb_preprocess_uvw_noalloc", "mtb_preprocess_uvw_noalloc_capacity",
     "mtb_finalize_workspace_size", "mtb_finalize", "mtb_status_string", "mtb_version",
     "mtb_release_caches", "mtb_kernel_launch_count", "mtb_calibrate_fp32",
+    "mtb_taper_kernel_build", "mtb_fits_create", "mtb_fits_write_channel", "mtb_fits_close",
     "mtb_engine_create", "mtb_engine_submit", "mtb_engine_wait", "mtb_engine_request_bytes", "mtb_engine_destroy",
 )
 
@@ -56,7 +57,7 @@ class GridParams(ctypes.Structure):
                 ("w_sq_increment", ctypes.c_double), ("initialize_output", ctypes.c_int), ("tile", ctypes.c_int),
                 ("support_bucket", ctypes.c_int), ("max_chunk", ctypes.c_int), ("merge", ctypes.c_int),
                 ("gridder_start_event", ctypes.c_void_p), ("gridder_end_event", ctypes.c_void_p),
-                ("bulk_min_support", ctypes.c_int)]
+                ("bulk_min_support", ctypes.c_int), ("psf", ctypes.c_int)]
 
 
 class GridStats(ctypes.Structure):
@@ -67,6 +68,13 @@ class GridStats(ctypes.Structure):
 class FinalizeParams(ctypes.Structure):
     _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("npol", ctypes.c_int), ("sampling", ctypes.c_int),
                 ("pol_type", ctypes.c_int)]
+
+
+class FitsHeader(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nstokes", ctypes.c_int), ("nchan", ctypes.c_int),
+                ("l_increment", ctypes.c_double), ("m_increment", ctypes.c_double), ("ra_deg", ctypes.c_double),
+                ("dec_deg", ctypes.c_double), ("freqs_hz", ctypes.c_void_p), ("stokes", ctypes.c_void_p),
+                ("telescope", ctypes.c_char_p), ("observer", ctypes.c_char_p), ("obs_mjd", ctypes.c_double)]
 
 
 class EngineConfig(ctypes.Structure):
@@ -106,6 +114,7 @@ def load(path: str = LIB_PATH):
     L.mtb_preprocess_uvw.argtypes = [ctypes.POINTER(GridParams), p, p, p, p, p, p, p, i] + [p] * 8 + [sz, p]
     L.mtb_preprocess_uvw_noalloc.argtypes = [ctypes.POINTER(GridParams), p, p, p, p, p, p, p, i] + [p] * 7 + [p]
     L.mtb_preprocess_uvw_noalloc_capacity.argtypes = []
+    L.mtb_taper_kernel_build.argtypes = [i, i, p, sz, p, p, p, ctypes.POINTER(sz), p]
     L.mtb_finalize_workspace_size.argtypes = [ctypes.POINTER(FinalizeParams), ctypes.POINTER(sz)]
     L.mtb_finalize.argtypes = [ctypes.POINTER(FinalizeParams), p, p, p, p, p, sz, p]
     for name in EXPORTS:
@@ -118,6 +127,9 @@ def load(path: str = LIB_PATH):
     L.mtb_kernel_launch_count.restype = ctypes.c_ulonglong
     L.mtb_kernel_launch_count.argtypes = []
     L.mtb_calibrate_fp32.argtypes = [ctypes.POINTER(ctypes.c_double), p]
+    L.mtb_fits_create.argtypes = [ctypes.c_char_p, ctypes.POINTER(FitsHeader), ctypes.POINTER(p)]
+    L.mtb_fits_write_channel.argtypes = [p, i, p]
+    L.mtb_fits_close.argtypes = [p]
     L.mtb_engine_create.argtypes = [ctypes.POINTER(EngineConfig), ctypes.POINTER(p)]
     L.mtb_engine_submit.argtypes = [p, ctypes.POINTER(ImageRequest), ctypes.POINTER(ctypes.c_longlong)]
     L.mtb_engine_wait.argtypes = [p, ctypes.c_longlong, ctypes.POINTER(ImageResult)]

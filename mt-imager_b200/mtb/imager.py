@@ -54,6 +54,33 @@ def wkernel_params(nx, ny, l_increment, m_increment, wplanes, sampling, trial_su
                            max_support, float(w_max))
 
 
+def build_taper_kernels(nx, ny, l_increment, m_increment, support=7, sampling=8, device="cuda",
+                        stream=None) -> KernelTable:
+    """mode=normal: the taper-only kernel table (one plane, no w-term) of
+    OnlyTaperConvFunction.cpp:29-99 through mtb_taper_kernel_build."""
+    lib = L.load()
+    T = sampling if sampling % 2 else sampling + 1
+    n = T * T * support * support
+    table = torch.empty(n, dtype=torch.complex64, device=device)
+    d_ci = torch.empty((1, 2), dtype=torch.int32, device=device)
+    h_ci = np.zeros((1, 2), np.int32)
+    sums = torch.empty((1, T * T), dtype=torch.float32, device=device)
+    got = ctypes.c_size_t(0)
+    L.check(lib.mtb_taper_kernel_build(support, sampling, _ptr(table), n, _ptr(d_ci),
+                                       h_ci.ctypes.data_as(ctypes.c_void_p), _ptr(sums), ctypes.byref(got),
+                                       _stream(stream)), "mtb_taper_kernel_build")
+    params = wkernel_params(nx, ny, l_increment, m_increment, 1, sampling)
+    info = L.WKernelInfo()
+    info.trial_support = support
+    info.support_cap = support
+    info.T = T
+    info.w_sq_increment = 1.0        # one plane (WProjectionConvFunction.cpp:110)
+    info.total_l, info.total_m = l_increment * nx, m_increment * ny
+    info.u_increment, info.v_increment = 1.0 / (l_increment * nx), 1.0 / (m_increment * ny)
+    info.table_capacity = n
+    return KernelTable(table=table, conv_info=h_ci, d_conv_info=d_ci, conv_sums=sums, info=info, params=params)
+
+
 def query_wkernels(params: L.WKernelParams) -> L.WKernelInfo:
     lib = L.load()
     info = L.WKernelInfo()
@@ -86,11 +113,19 @@ class WProjectionImager:
     def __init__(self, nx, ny, l_increment, m_increment=None, wplanes=32, sampling=8, npol=4,
                  trial_support=0, max_support=0, w_max=0.0, pol_type=L.MTB_POL_LINEAR, compensated=True,
                  tile=0, support_bucket=0, max_chunk=0, merge=0, bulk_min_support=0, device="cuda",
-                 kernels: KernelTable | None = None):
+                 kernels: KernelTable | None = None, psf=False, mode="wproj", taper_support=7):
+        """mode "wproj" (W-projection kernels) or "normal" (taper-only kernel of
+        support taper_support at oversampling `sampling`, one plane); psf
+        grids every visibility as 1 + 0i (mt-imager's psf=true)."""
         self.lib = L.load()
         self.device = torch.device(device)
         self.nx, self.ny, self.npol = nx, ny, npol
         m_increment = l_increment if m_increment is None else m_increment
+        if mode not in ("wproj", "normal"):
+            raise ValueError("mode must be 'wproj' or 'normal'")
+        self.mode, self.psf, self.taper_support = mode, bool(psf), taper_support
+        if mode == "normal":
+            wplanes = 1
         self.params = wkernel_params(nx, ny, l_increment, m_increment, wplanes, sampling, trial_support,
                                      max_support, w_max)
         self.kernels = kernels
@@ -112,7 +147,12 @@ class WProjectionImager:
     # -- WProjectionConvFunction
     def build_kernels(self, stream=None) -> KernelTable:
         if self.kernels is None:
-            self.kernels = build_wkernels(self.params, self.device, stream)
+            if self.mode == "normal":
+                p = self.params
+                self.kernels = build_taper_kernels(p.nx, p.ny, p.l_increment, p.m_increment, self.taper_support,
+                                                   p.sampling, self.device, stream)
+            else:
+                self.kernels = build_wkernels(self.params, self.device, stream)
         return self.kernels
 
     def grid_params(self, initialize: bool) -> L.GridParams:
@@ -122,6 +162,7 @@ class WProjectionImager:
                           self.tuning["tile"], self.tuning["support_bucket"], self.tuning["max_chunk"],
                           self.tuning["merge"])
         gp.bulk_min_support = self.tuning["bulk_min_support"]
+        gp.psf = int(self.psf)
         if self.gridder_events is not None:
             gp.gridder_start_event = self.gridder_events[0].cuda_event
             gp.gridder_end_event = self.gridder_events[1].cuda_event

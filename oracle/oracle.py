@@ -194,6 +194,39 @@ def wkernels(geo):
                 divisor=divisor)
 
 
+def taper_kernels(support, sampling):
+    """mode=normal kernel table (OnlyTaperConvFunction.cpp:29-99): the uv
+    gridding function of CasaGridSF.cu:107-149 -- per axis (1 - nu^2) grdsf(nu),
+    nu = d / (3 s) for offsets d < 3 s from the centre of a (S s [+1 for even
+    s])^2 array -- cut by ConvFunctionReOrganize.cu:30-71 into one plane of
+    [oy][ox][sy][sx] sub-kernels, with SumConvolutionFunctions.cu:29-56 sums."""
+    S, s = int(support), int(sampling)
+    T = s if s % 2 else s + 1
+    dim = S * s + (0 if s % 2 else 1)
+    zero_at = 3 * s
+    g = lib().orc_grdsf
+
+    def f(d):
+        d = abs(d)
+        if d >= zero_at:
+            return 0.0
+        nu = d / zero_at
+        return (1.0 - nu * nu) * g(nu)
+
+    axis = np.array([f(i - dim // 2) for i in range(dim)])
+    full = np.outer(axis, axis)
+    cb = dim // 2 - ((S // 2) * s + s // 2)
+    table = np.zeros((T, T, S, S), np.complex128)
+    for oy in range(T):
+        for ox in range(T):
+            rows = np.arange(S) * s + oy + cb
+            cols = np.arange(S) * s + ox + cb
+            table[oy, ox] = full[np.ix_(rows, cols)]
+    table = table.reshape(-1)
+    sums = table.real.reshape(T * T, S * S).sum(axis=1)[None, :]
+    return dict(table=table, conv_info=np.array([[S, 0]], np.int32), conv_sums=sums, supports=np.array([S]))
+
+
 # ------------------------------------------------------------ preprocess --
 def preprocess(uvw, freq, weights, flags, geo, kern):
     """PreProcessUVW (WProjPreProcessUVW.cu:112-324) in FP64."""

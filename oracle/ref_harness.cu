@@ -416,6 +416,43 @@ int mtref_wkernels(int nx, int ny, double l_increment, double m_increment, int w
     return 0;
 }
 
+/* mode=normal kernels (OnlyTaperConvFunction.cpp:29-99): casagridsf (uv
+ * gridding function, complex output) -> ConvFunctionReOrganize ->
+ * SumConvolutionFunctions with convInfo = {support, 0}.
+ *   table out complex64 [T*T*support*support], conv_sums out float [T*T] */
+int mtref_taper_kernel(int support, int sampling, void *table, float *conv_sums, char *err, int errlen) {
+    try {
+        typedef GAFW::Tools::CppProperties::Properties PR;
+        Runner run;
+        const int T = sampling % 2 ? sampling : sampling + 1;
+        const unsigned size = (unsigned)(support * sampling + (sampling % 2 ? 0 : 1));
+        const unsigned n = (unsigned)(T * T * support * support);
+        Arr full = make({size, size}, complex_float, 8), org = make({n}, complex_float, 8);
+        Arr info = make({1, 2}, real_int, 4), sums = make({1, (unsigned)(T * T)}, real_float, 4);
+        PR taper_p, org_p, sum_p;
+        taper_p.set("lmPlanePostCorrection", 0, PR::Bool);
+        taper_p.set("generate", 1, PR::Bool);
+        taper_p.set("support", support, PR::Int);
+        taper_p.set("sampling", sampling, PR::Int);
+        mtimager::CasaGridSF taper_op(nullptr, "taper");
+        run.submit(taper_op, {}, {full.get()}, taper_p);
+        org_p.set("ConvolutionFunction.sampling", sampling, PR::Int);
+        org_p.set("ConvolutionFunction.support", support, PR::Int);
+        mtimager::ConvFunctionReOrganize org_op(nullptr, "convFuncOrganise");
+        run.submit(org_op, {full.get()}, {org.get()}, org_p);
+        const int ci[2] = {support, 0};
+        info->upload(ci);
+        sum_p.set("sampling", sampling, PR::Int);
+        mtimager::SumConvolutionFunctions sum_op(nullptr, "SumConvolutionFunctions");
+        run.submit(sum_op, {info.get(), org.get()}, {sums.get()}, sum_p);
+        org->download(table);
+        sums->download(conv_sums);
+    } catch (const std::exception &e) {
+        return fail(err, errlen, e.what());
+    }
+    return 0;
+}
+
 /* ImageFinalizer (ImageFinalizer.cpp:31-44): PreIFFTUVCorrection -> IFFT2D ->
  * ZeroToCentre2DShift -> StokesConverter -> casagridsf (lmPlanePostCorrection)
  * -> SincCorrector.

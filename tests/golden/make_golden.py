@@ -16,6 +16,8 @@ compressed .npz files:
   wkernels_<g>.npz  WProjectionConvFunction (WProjectionConvFunction.cpp:
                     186-291): kernel table, convInfo, ConvSums and the w=0
                     divisor for a geometry.
+  taper_<g>.npz     mode=normal kernel (OnlyTaperConvFunction.cpp:29-99):
+                    table and ConvSums for a support and oversampling.
 
     python tests/golden/make_golden.py [--out DIR]
 """
@@ -57,6 +59,8 @@ KERNEL_GEOMETRIES = {
     "cap_s4": (128, 2000.0, 6, 4),     # supports 7-31, the last planes at the S_t - 2 cap
     "odd_s3": (96, 1500.0, 6, 3),      # odd oversampling, supports 7-23
 }
+# name: (support, oversampling) of mode=normal kernels
+TAPER_KERNELS = {"s7_o8": (7, 8), "s7_o3": (7, 3), "s9_o4": (9, 4)}
 # polarisation type of each grid case's image (0 linear, 1 circular)
 IMAGE_POL_TYPE = {"even_s4": 0, "odd_s3_p2": 1, "wide_s4": 0}
 
@@ -161,17 +165,31 @@ def run_finalize(lib, c, ref, pol_type):
     return dict(pol_type=pol_type, normalizer=norm, ref_image=img)
 
 
+def run_taper(lib, support, sampling):
+    T = sampling if sampling % 2 else sampling + 1
+    table = np.zeros(T * T * support * support, np.complex64)
+    sums = np.zeros((1, T * T), np.float32)
+    err = ctypes.create_string_buffer(512)
+    p = lambda a: a.ctypes.data_as(ctypes.c_void_p)  # noqa: E731
+    rc = lib.mtref_taper_kernel(support, sampling, p(table), p(sums), err, 512)
+    if rc:
+        raise RuntimeError("reference taper kernel failed: " + err.value.decode())
+    return dict(support=support, sampling=sampling, ref_table=table, ref_conv_sums=sums)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=HERE)
     ap.add_argument("--lib", default=os.path.join(ROOT, "oracle", "_ref", "libmtref.so"))
+    ap.add_argument("--only", default="", help="comma-separated fixture kinds to make (grid,wkernels,taper)")
     a = ap.parse_args()
+    only = set(a.only.split(",")) if a.only else {"grid", "wkernels", "taper"}
     lib = ctypes.CDLL(a.lib)
-    for f in (lib.mtref_grid_chunk, lib.mtref_wkernels, lib.mtref_finalize):
+    for f in (lib.mtref_grid_chunk, lib.mtref_wkernels, lib.mtref_finalize, lib.mtref_taper_kernel):
         f.restype = ctypes.c_int
     O.build()
     os.makedirs(a.out, exist_ok=True)
-    for name, spec in CASES.items():
+    for name, spec in (CASES.items() if "grid" in only else []):
         c = make_case(name, spec)
         ref = run_reference(lib, c)
         path = os.path.join(a.out, "grid_%s.npz" % name)
@@ -182,7 +200,12 @@ def main():
         path = os.path.join(a.out, "image_%s.npz" % name)
         np.savez_compressed(path, **img)
         print("  image peak %.4g, %d bytes" % (np.abs(img["ref_image"]).max(), os.path.getsize(path)))
-    for name, g in KERNEL_GEOMETRIES.items():
+    for name, (sup, smp) in (TAPER_KERNELS.items() if "taper" in only else []):
+        k = run_taper(lib, sup, smp)
+        path = os.path.join(a.out, "taper_%s.npz" % name)
+        np.savez_compressed(path, **k)
+        print("%s: %d elements, %d bytes" % (name, k["ref_table"].size, os.path.getsize(path)))
+    for name, g in (KERNEL_GEOMETRIES.items() if "wkernels" in only else []):
         k = run_wkernels(lib, *g)
         path = os.path.join(a.out, "wkernels_%s.npz" % name)
         np.savez_compressed(path, **k)
