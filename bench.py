@@ -245,7 +245,7 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="mtb", choices=["mtb", "reference"])
-    ap.add_argument("--config", default="mid", choices=["mid", "small", "serve"])
+    ap.add_argument("--config", default="mid", choices=["mid", "small", "serve", "cube"])
     ap.add_argument("--channels", type=int, default=16)
     ap.add_argument("--hours", type=float, default=8.0)
     ap.add_argument("--e2e-steps", type=int, default=1)
@@ -258,6 +258,9 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-serve", action="store_true", help="skip the request-stream measurement")
+    ap.add_argument("--cube-images", type=int, default=16)
+    ap.add_argument("--cube-min-hours", type=float, default=0.25)
+    ap.add_argument("--cube-max-hours", type=float, default=2.0)
     ap.add_argument("--serve-requests", type=int, default=24)
     ap.add_argument("--serve-rate", type=float, default=20.0, help="Poisson arrival rate, requests per second")
     ap.add_argument("--serve-min-records", type=float, default=1e5)
@@ -281,6 +284,18 @@ def main():
 
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
+    if args.config == "cube":
+        if rank == 0:
+            cb = run_cube(args, torch, dev)
+            print(json.dumps({"metric": METRIC, "value": cb["batched_cuda_graph"]["samples_per_s"],
+                              "unit": "samples/s", "n_gpus": 1, "higher_is_better": True, "impl": "mtb-batch",
+                              "data": "synthetic", "config": {"workload": "batched cubes: %d channel images, "
+                                                                          "%.3g-%.3g h tracks, 1024^2/2048^2, 64 "
+                                                                          "w-planes" % (args.cube_images,
+                                                                                       args.cube_min_hours,
+                                                                                       args.cube_max_hours)},
+                              "cube": cb}), flush=True)
+        return
     if args.config == "serve":
         if rank == 0:
             sv = run_serve(args, torch, dev)
@@ -551,6 +566,83 @@ def make_requests(args, torch, dev, rng):
                          freq=np.full(R, f / C_LIGHT, np.float32), vis=vis.cpu().numpy(),
                          weights=np.ones((R, 4), np.float32), flags=flags.cpu().numpy()))
     return reqs
+
+
+def run_cube(args, torch, dev):
+    """Batched cubes: independent channel images with uneven record counts
+    (64-antenna tracks of U(cube_min_hours, cube_max_hours) at 2 s, flagging
+    U(0, 60 %)), image size 1024^2 or 2048^2 per image, 64 w-planes, supports
+    up to 49.  Gridded (a) image by image with mtb_grid, (b) all images with
+    one mtb_grid_batch launch, (c) that batch replayed from a captured CUDA
+    graph.  Inputs resident in HBM; samples/s of the gridding of every image."""
+    from mtb.imager import WProjectionImager, build_wkernels, grid_batch, wkernel_params
+    rng = np.random.default_rng(4)
+    spec = workload_spec(argparse.Namespace(config="mid", channels=1, hours=8.0))
+    pool, nbl, nt = make_uvw(spec, dev, torch, rng)
+    uv_max = float(pool[:2].abs().max())
+    gen = torch.Generator(device=dev).manual_seed(13)
+    kern = {}
+    entries = []
+    for k in range(args.cube_images):
+        n = int(rng.choice([1024, 2048]))
+        hours = float(rng.uniform(args.cube_min_hours, args.cube_max_hours))
+        ntk = max(1, int(hours * 1800))
+        # the first ntk integrations of every baseline (records stay baseline-major)
+        sel = pool.reshape(3, nbl, nt)[:, :, :ntk].reshape(3, -1).contiguous()
+        R = sel.shape[1]
+        dl = cell_for(dict(spec, nx=n, max_support=49), uv_max, torch)
+        if n not in kern:
+            kern[n] = build_wkernels(wkernel_params(n, n, dl, dl, 64, 8, 51, 49), dev)
+        f = float(rng.uniform(1.3e9, 1.5e9))
+        srcs = sources_for(dict(spec, nsrc=20), n * dl, rng)
+        vis = make_vis(sel, f, srcs, torch, gen)
+        frac = float(rng.uniform(0.0, 0.6))
+        flags = (torch.rand(R, device=dev, generator=gen) < frac).int()[:, None].repeat(1, 4).contiguous()
+        im = WProjectionImager(n, n, dl, wplanes=64, sampling=8, trial_support=51, max_support=49, kernels=kern[n],
+                               device=dev)
+        entries.append((im, sel, torch.full((R,), f / C_LIGHT, dtype=torch.float32, device=dev), vis,
+                        torch.ones((R, 4), dtype=torch.float32, device=dev), flags))
+    torch.cuda.synchronize()
+
+    def single():
+        for im, *arrs in entries:
+            im.reset()
+            im.grid_device(*arrs)
+
+    ws = [None]
+
+    def batched():
+        for im, *_ in entries:
+            im.reset()
+        ws[0] = grid_batch(entries, workspace=ws[0])
+
+    def timed(fn, reps=3):
+        for _ in range(2):
+            fn()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(reps):
+            fn()
+        b.record()
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / reps
+
+    ms_single = timed(single)
+    stats = [im.statistics() for im, *_ in entries]
+    samples = sum((s["gridded_records"] + s["compressed_records"]) * 4 for s in stats)
+    ms_batch = timed(batched)
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph):
+        batched()
+    ms_graph = timed(graph.replay)
+    del graph
+    recs = [arrs[1].numel() for _, *arrs in entries]
+    return {"images": len(entries), "records": {"min": int(min(recs)), "max": int(max(recs)), "total": int(sum(recs))},
+            "image_sizes": sorted({im.nx for im, *_ in entries}), "samples_per_image_set": int(samples),
+            "per_image_launches": {"ms": ms_single, "samples_per_s": samples / (ms_single * 1e-3)},
+            "one_batched_launch": {"ms": ms_batch, "samples_per_s": samples / (ms_batch * 1e-3)},
+            "batched_cuda_graph": {"ms": ms_graph, "samples_per_s": samples / (ms_graph * 1e-3)}}
 
 
 def run_serve(args, torch, dev):

@@ -176,6 +176,39 @@ int mtb_grid(const mtb_grid_params *p, const void *d_table, const int *d_conv_in
              void *d_grid, void *d_grid_lo, float *d_normalizer, mtb_grid_stats *d_stats,
              void *d_workspace, size_t workspace_bytes, mtb_stream_t stream);
 
+/* One image of a batched gridding launch. */
+typedef struct mtb_grid_job {
+    mtb_grid_params params;      /* per image; npol must be the same for every job of a batch;
+                                    merge and bulk_min_support are ignored (the batch runs the
+                                    per-thread direct gridder)                               */
+    const void *d_table;         /* the image's kernel table, as for mtb_grid               */
+    const int *d_conv_info;
+    const int *h_conv_info;
+    const float *d_conv_sums;
+    const float *d_uvw, *d_freq; /* the image's chunk of records, as for mtb_grid           */
+    const void *d_vis;
+    const float *d_weights;
+    const int *d_flags;
+    int nrecords;
+    void *d_grid;                /* accumulated outputs, as for mtb_grid                    */
+    void *d_grid_lo;
+    float *d_normalizer;
+    mtb_grid_stats *d_stats;
+} mtb_grid_job;
+
+/* Workspace for mtb_grid_batch over these jobs. */
+int mtb_grid_batch_workspace_size(const mtb_grid_job *jobs, int njobs, size_t *bytes);
+
+/* Grids one chunk of records into each of up to 64 images -- channels of a cube
+ * or unrelated images of any geometry -- with ONE persistent gridder launch fed
+ * by a work queue over (image, support bucket, tile) bins.  Every image is
+ * preprocessed and binned as by mtb_grid, its work items are concatenated into
+ * one queue, and the gridder takes each item's image from it.  The result for
+ * every image equals mtb_grid's.  All work is enqueued on `stream`; the call
+ * can be captured into a CUDA graph. */
+int mtb_grid_batch(const mtb_grid_job *jobs, int njobs, void *d_workspace, size_t workspace_bytes,
+                   mtb_stream_t stream);
+
 /* The PreProcessUVW operator alone, with its seven outputs in the reference's
  * layout (code/mt-imager/lib/operators/WProjPreProcessUVW.cpp:66-85,
  * WProjPreProcessUVW.cu:112-324), FP64 coordinates.  Workspace: as for

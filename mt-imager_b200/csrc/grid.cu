@@ -538,20 +538,27 @@ static const int kG3Chunk = 512;            // records of one work item, staged 
 static const int kG3Depth = 4;              // records of kernel values fetched ahead
 static const int kG3KS = 4;                 // support-box slots per thread
 
-struct Grid2Args {
-    const int4 *items;
-    const int *n_items;
-    int *counter;
+// One image of a k_grid3 launch: its records and visibilities in gridder
+// layout, its expanded padded kernel table, its grid (or FP64 delta grid in
+// compensated mode) and the modulus of each of its support buckets.
+struct GridJobDesc {
     const int4 *wpos;
-    const float2 *wvis;
     const float4 *wvis4;
-    const float2 *table;
     const float4 *table2;
     float *grid;
-    float *grid_lo;
     double *dgrid;         // compensated mode: FP64 delta grid of this call, else null
+    const int *M;          // [kMaxBuckets] bucket moduli (device)
     int nx;
-    BucketTable bt;
+    int pad_;
+};
+static const int kMaxBatch = 64;   // images one batched launch grids
+
+struct Grid2Args {
+    const int4 *items;     // work items; item.w selects the image
+    const int *n_items;
+    int *counter;
+    int njobs;
+    GridJobDesc jobs[kMaxBatch];
 };
 
 typedef unsigned long long u64;
@@ -685,9 +692,6 @@ __global__ void __launch_bounds__(kG3Threads, 2) k_grid3(Grid2Args a) {
     __shared__ int s_item;
     const int t = threadIdx.x;
     const int nitems = a.n_items[0];
-    const ulonglong2 *tab = (const ulonglong2 *)a.table2;
-    const int4 *grec = a.wpos;
-    const uint4 *gvis = (const uint4 *)a.wvis4;
     constexpr int KS = kG3KS, D = kG3Depth;
     for (;;) {
         __syncthreads();
@@ -696,13 +700,20 @@ __global__ void __launch_bounds__(kG3Threads, 2) k_grid3(Grid2Args a) {
         const int v = s_item;
         if (v >= nitems) break;
         const int4 it = a.items[v];
+        const GridJobDesc &J = a.jobs[it.w];
+        const ulonglong2 *tab = (const ulonglong2 *)J.table2;
+        const int4 *grec = J.wpos;
+        const uint4 *gvis = (const uint4 *)J.wvis4;
+        float *const ggrid = J.grid;
+        double *const gdelta = J.dgrid;
+        const int gnx = J.nx;
         // stage the item's records (gridder layout, 16-byte pieces)
         for (int k = t; k < it.y; k += kG3Threads) cp_async16(&s_rec[k], &grec[it.x + k]);
         for (int k = t; k < it.y * P; k += kG3Threads) cp_async16(&s_v[k], &gvis[(size_t)it.x * P + k]);
         cp_async_commit();
         cp_async_wait<0>();
         __syncthreads();
-        const int M = a.bt.M[(unsigned)it.z >> 24];
+        const int M = J.M[(unsigned)it.z >> 24];
         const Layout L = layout_for(M, KS);
         const int per_stream = M * L.Gp;
         const int stream = t / per_stream;
@@ -729,7 +740,7 @@ __global__ void __launch_bounds__(kG3Threads, 2) k_grid3(Grid2Args a) {
 #pragma unroll
                 for (int j = 0; j < KS; j++) {
                     const bool ok = xok && (j < nrow) && (sy < S);
-                    cell[j] = ok ? rec.x + sy * a.nx + sx : -1;
+                    cell[j] = ok ? rec.x + sy * gnx + sx : -1;
                     toff[j] = ok ? sy * (S + 1) + sx : 0;
                     vmul[j] = ok ? 1 : 0;
                     sy += L.G;
@@ -776,7 +787,7 @@ __global__ void __launch_bounds__(kG3Threads, 2) k_grid3(Grid2Args a) {
 #pragma unroll
                     for (int j = 0; j < KS; j++) {
                         if (cellN[j] >= 0 && cellN[j] != last[j]) {
-                            if (last[j] >= 0) flush2<P>(a.grid, a.dgrid, last[j], acc[j]);
+                            if (last[j] >= 0) flush2<P>(ggrid, gdelta, last[j], acc[j]);
                             last[j] = cellN[j];
 #pragma unroll
                             for (int p = 0; p < P; p++) acc[j][p] = 0ull;
@@ -808,7 +819,7 @@ __global__ void __launch_bounds__(kG3Threads, 2) k_grid3(Grid2Args a) {
             cp_async_wait<0>();
 #pragma unroll
             for (int j = 0; j < KS; j++)
-                if (last[j] >= 0) flush2<P>(a.grid, a.dgrid, last[j], acc[j]);
+                if (last[j] >= 0) flush2<P>(ggrid, gdelta, last[j], acc[j]);
         }
     }
 }
@@ -1148,6 +1159,10 @@ static int launch_grid4(const Grid4Args &a, cudaStream_t st) {
     return MTB_OK;
 }
 
+__global__ void k_set_moduli(BucketTable bt, int *__restrict__ M) {
+    for (int b = threadIdx.x; b < kMaxBuckets; b += blockDim.x) M[b] = bt.M[b];
+}
+
 // First work item whose bucket goes to k_grid4 (items are in bucket order).
 __global__ void k_split(const int *__restrict__ bounds, const int *__restrict__ n_items, BucketTable bt, int min_m,
                         int *__restrict__ split) {
@@ -1201,6 +1216,7 @@ struct GridSpace {
     float2 *ptab;        // row-padded copy of the table (rows of S + 1 taps)
     float4 *table2;      // padded table with each tap as {re, re, im, im} (k_grid3)
     int *pbase;          // first padded element of every plane
+    int *moduli;         // bucket moduli of the plan (device copy)
     int *split;          // first work item of k_grid4
     int *counter4;       // k_grid4 work counter
     int *err;            // gridder pipeline error flag
@@ -1246,6 +1262,7 @@ static void carve_grid(Arena &A, int R, int P, int chunk, size_t table_elems, si
     s->ptab = A.take<float2>(table_elems ? table_elems : 1);
     s->table2 = A.take<float4>(table_elems ? table_elems : 1);
     s->pbase = A.take<int>(nw > 0 ? nw : 1);
+    s->moduli = A.take<int>(kMaxBuckets);
     s->split = A.take<int>(1);
     s->counter4 = A.take<int>(1);
     s->err = A.take<int>(1);
@@ -1370,13 +1387,15 @@ static bool check_gridder() {
     return v == 1;
 }
 
+// Everything of one mtb_grid call before the gridder kernels: preprocessing,
+// compression, binning into work items, the gathered records and
+// visibilities, and (direct gridders) the padded and expanded kernel tables,
+// the bucket moduli on the device and the zeroed delta grid.
 template <int P>
-static int run_grid(const mtb_grid_params *p, const GridPlan &plan, const float2 *table, size_t table_elems,
-                    size_t padded,
-                    const int *conv_info,
-                    const float *conv_sums, const float *uvw, const float *freq, const float2 *vis,
-                    const float *weights, const int *flags, int R, float *grid, float *grid_lo,
-                    float *normalizer, mtb_grid_stats *stats, GridSpace &s, cudaStream_t st) {
+static int prepare_grid(const mtb_grid_params *p, const GridPlan &plan, const float2 *table, size_t table_elems,
+                        size_t padded, const int *conv_info, const float *conv_sums, const float *uvw,
+                        const float *freq, const float2 *vis, const float *weights, const int *flags, int R,
+                        bool compensated, GridSpace &s, cudaStream_t st) {
     const int T = oversample_T(p->sampling);
     const int sms = sm_count();
     MTB_CUDA_TRY(cudaMemsetAsync(s.norm_acc, 0, 4 * sizeof(double), st));
@@ -1410,114 +1429,142 @@ static int run_grid(const mtb_grid_params *p, const GridPlan &plan, const float2
     k_bucket_bounds<<<blocks, 256, 0, st>>>(s.items, s.item_start, s.nchunks, s.num_runs, s.bounds, plan.bt.n,
                                             s.n_items);
     MTB_LAUNCHED();
-    if (p->merge == 1)
+    if (p->merge == 1) {
         k_gather<P, false><<<blocks, 256, 0, st>>>(R, s.skeys, s.sidx, s.pos, s.meta, vis, weights, flags, s.wpos,
                                                    s.wvis, plan.bt, p->nx, nullptr, nullptr, 0, p->psf);
-    else {
-        k_pad_bases<<<1, 1, 0, st>>>(conv_info, p->wplanes, T, s.pbase);
         MTB_LAUNCHED();
-        k_gather<P, true><<<blocks, 256, 0, st>>>(R, s.skeys, s.sidx, s.pos, s.meta, vis, weights, flags, s.wpos,
-                                                  s.wvis, plan.bt, p->nx, conv_info, s.pbase, p->wplanes, p->psf);
+        (void)end_bit;
+        return MTB_OK;
     }
+    k_pad_bases<<<1, 1, 0, st>>>(conv_info, p->wplanes, T, s.pbase);
+    MTB_LAUNCHED();
+    k_gather<P, true><<<blocks, 256, 0, st>>>(R, s.skeys, s.sidx, s.pos, s.meta, vis, weights, flags, s.wpos,
+                                              s.wvis, plan.bt, p->nx, conv_info, s.pbase, p->wplanes, p->psf);
     MTB_LAUNCHED();
     (void)end_bit;
-
-    GridArgs a;
-    a.items = s.items;
-    a.bounds = s.bounds;
-    a.counters = s.counters;
-    a.wpos = s.wpos;
-    a.wvis = s.wvis;
-    a.table = table;
-    a.grid = grid;
-    a.grid_lo = grid_lo;
-    a.nx = p->nx;
-    a.ny = p->ny;
-    if (p->gridder_start_event) MTB_CUDA_TRY(cudaEventRecord((cudaEvent_t)p->gridder_start_event, st));
-    if (p->merge != 1) {
-        Grid2Args g2;
-        g2.items = s.items;
-        g2.n_items = s.split;            // k_grid3 takes the items before the split
-        g2.counter = s.counters;
-        g2.wpos = s.wpos;
-        g2.wvis = s.wvis;
-        g2.table = table;
-        g2.table2 = s.table2;
-        {
-            int eb = (int)std::min<size_t>((table_elems + 255) / 256, (size_t)sms * 16);
-            k_pad_table<<<eb > 0 ? eb : 1, 256, 0, st>>>(table, table_elems, conv_info, s.pbase, p->wplanes, s.ptab);
-            MTB_LAUNCHED();
-            int pb = (int)std::min<size_t>((padded + 255) / 256, (size_t)sms * 16);
-            k_expand_table<<<pb > 0 ? pb : 1, 256, 0, st>>>(s.ptab, s.table2, padded);
-            MTB_LAUNCHED();
-        }
-        MTB_CUDA_TRY(cudaMemsetAsync(s.counter4, 0, sizeof(int), st));
-        MTB_CUDA_TRY(cudaMemsetAsync(s.err, 0, sizeof(int), st));
-        // k_grid4 is opt-in: it measured slower than k_grid3 on the mid-size
-        // workload (45.6 vs 30.7 ms per 29 M-record call)
-        const int min_m = p->bulk_min_support > 0 ? p->bulk_min_support : (1 << 30);
-        k_split<<<1, 1, 0, st>>>(s.bounds, s.n_items, plan.bt, min_m < kG4MinM ? kG4MinM : min_m, s.split);
+    {
+        int eb = (int)std::min<size_t>((table_elems + 255) / 256, (size_t)sms * 16);
+        k_pad_table<<<eb > 0 ? eb : 1, 256, 0, st>>>(table, table_elems, conv_info, s.pbase, p->wplanes, s.ptab);
         MTB_LAUNCHED();
-        // compensated mode: the call's flushes go to a zeroed FP64 delta grid
-        // with plain reductions (no returned values, so no stall at a flush)
-        // and one pass merges it into the float pair (grid, grid_lo)
-        const size_t nfloat = (size_t)p->nx * p->ny * 2 * P;
-        if (grid_lo) MTB_CUDA_TRY(cudaMemsetAsync(s.delta, 0, nfloat * sizeof(double), st));
-        g2.wvis4 = (const float4 *)s.wvis;
-        g2.grid = grid;
-        g2.dgrid = grid_lo ? s.delta : nullptr;
-        g2.grid_lo = nullptr;
-        g2.nx = p->nx;
-        g2.bt = plan.bt;
-        int ls = launch_grid3<P>(g2, st);
-        if (ls != MTB_OK) return ls;
-        Grid4Args g4;
-        g4.items = s.items;
-        g4.first = s.split;
-        g4.n_items = s.n_items;
-        g4.counter = s.counter4;
-        g4.wpos = s.wpos;
-        g4.wvis4 = (const float4 *)s.wvis;
-        g4.ptab = s.ptab;
-        g4.grid = g2.grid;
-        g4.dgrid = g2.dgrid;
-        g4.nx = p->nx;
-        g4.bt = plan.bt;
-        g4.err = s.err;
-        ls = launch_grid4<P>(g4, st);
-        if (ls != MTB_OK) return ls;
-        if (check_gridder()) {
-            int e = 0;
-            MTB_CUDA_TRY(cudaMemcpyAsync(&e, s.err, sizeof(int), cudaMemcpyDeviceToHost, st));
-            MTB_CUDA_TRY(cudaStreamSynchronize(st));
-            if (e) return MTB_ERR_KERNEL;
-        }
-        if (grid_lo) {
-            const size_t n2 = nfloat / 2;     // complex values
-            int mb = (int)std::min<size_t>((n2 + 255) / 256, (size_t)sms * 16);
-            k_merge_delta<<<mb > 0 ? mb : 1, 256, 0, st>>>((float2 *)grid, (float2 *)grid_lo,
-                                                         (const double2 *)s.delta, n2);
-            MTB_LAUNCHED();
+        int pb = (int)std::min<size_t>((padded + 255) / 256, (size_t)sms * 16);
+        k_expand_table<<<pb > 0 ? pb : 1, 256, 0, st>>>(s.ptab, s.table2, padded);
+        MTB_LAUNCHED();
+    }
+    k_set_moduli<<<1, 32, 0, st>>>(plan.bt, s.moduli);
+    MTB_LAUNCHED();
+    MTB_CUDA_TRY(cudaMemsetAsync(s.counter4, 0, sizeof(int), st));
+    MTB_CUDA_TRY(cudaMemsetAsync(s.err, 0, sizeof(int), st));
+    // compensated mode: the call's flushes go to a zeroed FP64 delta grid
+    // with plain reductions (no returned values, so no stall at a flush)
+    // and one pass merges it into the float pair (grid, grid_lo)
+    if (compensated)
+        MTB_CUDA_TRY(cudaMemsetAsync(s.delta, 0, (size_t)p->nx * p->ny * 2 * P * sizeof(double), st));
+    return MTB_OK;
+}
+
+template <int P>
+static GridJobDesc job_desc(const mtb_grid_params *p, float *grid, bool compensated, const GridSpace &s) {
+    GridJobDesc d;
+    d.wpos = s.wpos;
+    d.wvis4 = (const float4 *)s.wvis;
+    d.table2 = s.table2;
+    d.grid = grid;
+    d.dgrid = compensated ? s.delta : nullptr;
+    d.M = s.moduli;
+    d.nx = p->nx;
+    d.pad_ = 0;
+    return d;
+}
+
+// After the gridder kernels: fold the delta grid into (grid, grid_lo) and
+// add the call's normaliser sums and statistics.
+template <int P>
+static int finish_grid(const mtb_grid_params *p, float *grid, float *grid_lo, float *normalizer,
+                       mtb_grid_stats *stats, GridSpace &s, cudaStream_t st) {
+    const int sms = sm_count();
+    if (grid_lo) {
+        const size_t n2 = (size_t)p->nx * p->ny * P;     // complex values
+        int mb = (int)std::min<size_t>((n2 + 255) / 256, (size_t)sms * 16);
+        k_merge_delta<<<mb > 0 ? mb : 1, 256, 0, st>>>((float2 *)grid, (float2 *)grid_lo,
+                                                     (const double2 *)s.delta, n2);
+        MTB_LAUNCHED();
+    }
+    k_finish<<<1, 32, 0, st>>>(P, s.norm_acc, normalizer, s.stats, stats);
+    MTB_LAUNCHED();
+    return MTB_OK;
+}
+
+template <int P>
+static int run_grid(const mtb_grid_params *p, const GridPlan &plan, const float2 *table, size_t table_elems,
+                    size_t padded, const int *conv_info, const float *conv_sums, const float *uvw,
+                    const float *freq, const float2 *vis, const float *weights, const int *flags, int R,
+                    float *grid, float *grid_lo, float *normalizer, mtb_grid_stats *stats, GridSpace &s,
+                    cudaStream_t st) {
+    const bool direct = p->merge != 1;
+    MTB_TRY(prepare_grid<P>(p, plan, table, table_elems, padded, conv_info, conv_sums, uvw, freq, vis, weights,
+                            flags, R, direct && grid_lo != nullptr, s, st));
+    if (p->gridder_start_event) MTB_CUDA_TRY(cudaEventRecord((cudaEvent_t)p->gridder_start_event, st));
+    if (!direct) {
+        GridArgs a;
+        a.items = s.items;
+        a.bounds = s.bounds;
+        a.counters = s.counters;
+        a.wpos = s.wpos;
+        a.wvis = s.wvis;
+        a.table = table;
+        a.grid = grid;
+        a.grid_lo = grid_lo;
+        a.nx = p->nx;
+        a.ny = p->ny;
+        for (int b = 0; b < plan.bt.n; b++) {
+            int M = plan.bt.M[b];
+            if (M <= 0) continue;
+            a.bucket = b;
+            a.M = M;
+            a.tile = plan.bt.tile[b];
+            a.W = a.tile + M - 1;
+            Launch L = launch_shape(M, P, a.tile, p->merge);
+            MTB_TRY(launch_bucket<P>(a, L, st));
         }
         if (p->gridder_end_event) MTB_CUDA_TRY(cudaEventRecord((cudaEvent_t)p->gridder_end_event, st));
         k_finish<<<1, 32, 0, st>>>(P, s.norm_acc, normalizer, s.stats, stats);
         MTB_LAUNCHED();
         return MTB_OK;
     }
-    for (int b = 0; b < plan.bt.n; b++) {
-        int M = plan.bt.M[b];
-        if (M <= 0) continue;
-        a.bucket = b;
-        a.M = M;
-        a.tile = plan.bt.tile[b];
-        a.W = a.tile + M - 1;
-        Launch L = launch_shape(M, P, a.tile, p->merge);
-        MTB_TRY(launch_bucket<P>(a, L, st));
+    // k_grid4 is opt-in: it measured slower than k_grid3 on the mid-size
+    // workload (45.6 vs 30.7 ms per 29 M-record call)
+    const int min_m = p->bulk_min_support > 0 ? p->bulk_min_support : (1 << 30);
+    k_split<<<1, 1, 0, st>>>(s.bounds, s.n_items, plan.bt, min_m < kG4MinM ? kG4MinM : min_m, s.split);
+    MTB_LAUNCHED();
+    Grid2Args g2;
+    g2.items = s.items;
+    g2.n_items = s.split;            // k_grid3 takes the items before the split
+    g2.counter = s.counters;
+    g2.njobs = 1;
+    g2.jobs[0] = job_desc<P>(p, grid, grid_lo != nullptr, s);
+    MTB_TRY(launch_grid3<P>(g2, st));
+    Grid4Args g4;
+    g4.items = s.items;
+    g4.first = s.split;
+    g4.n_items = s.n_items;
+    g4.counter = s.counter4;
+    g4.wpos = s.wpos;
+    g4.wvis4 = (const float4 *)s.wvis;
+    g4.ptab = s.ptab;
+    g4.grid = grid;
+    g4.dgrid = g2.jobs[0].dgrid;
+    g4.nx = p->nx;
+    g4.bt = plan.bt;
+    g4.err = s.err;
+    MTB_TRY(launch_grid4<P>(g4, st));
+    if (check_gridder()) {
+        int e = 0;
+        MTB_CUDA_TRY(cudaMemcpyAsync(&e, s.err, sizeof(int), cudaMemcpyDeviceToHost, st));
+        MTB_CUDA_TRY(cudaStreamSynchronize(st));
+        if (e) return MTB_ERR_KERNEL;
     }
     if (p->gridder_end_event) MTB_CUDA_TRY(cudaEventRecord((cudaEvent_t)p->gridder_end_event, st));
-    k_finish<<<1, 32, 0, st>>>(P, s.norm_acc, normalizer, s.stats, stats);
-    MTB_LAUNCHED();
-    return MTB_OK;
+    return finish_grid<P>(p, grid, grid_lo, normalizer, stats, s, st);
 }
 
 // PreProcessUVW's seven outputs in the reference's layout
@@ -1599,6 +1646,157 @@ extern "C" int mtb_grid(const mtb_grid_params *p, const void *d_table, const int
                            nrecords, g, lo, d_normalizer, d_stats, s, st);
     return run_grid<4>(p, plan, tb, te, pe, d_conv_info, d_conv_sums, d_uvw, d_freq, vis, d_weights, d_flags, nrecords,
                        g, lo, d_normalizer, d_stats, s, st);
+}
+
+// ---------------------------------------------------------- batched grid --
+struct BatchQueues {
+    const int4 *items[kMaxBatch];
+    const int *n_items[kMaxBatch];   // null: the image has no records
+};
+
+// One queue of every image's work items, image index in item.w.
+__global__ void k_concat_items(BatchQueues q, int njobs, int4 *__restrict__ out, int *__restrict__ n_total) {
+    const int j = blockIdx.x;
+    __shared__ int base, n;
+    if (threadIdx.x == 0) {
+        int b = 0;
+        for (int i = 0; i < j; i++) b += q.n_items[i] ? *q.n_items[i] : 0;
+        base = b;
+        n = q.n_items[j] ? *q.n_items[j] : 0;
+        if (j == njobs - 1) *n_total = b + n;
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < n; k += blockDim.x) {
+        int4 it = q.items[j][k];
+        it.w = j;
+        out[base + k] = it;
+    }
+}
+
+static int check_batch(const mtb_grid_job *jobs, int njobs) {
+    if (!jobs) return MTB_ERR_NULL;
+    if (njobs < 1 || njobs > kMaxBatch) return MTB_ERR_BAD_SHAPE;
+    for (int j = 0; j < njobs; j++) {
+        MTB_TRY(check_params(&jobs[j].params));
+        if (jobs[j].params.npol != jobs[0].params.npol) return MTB_ERR_BAD_SHAPE;
+        if (jobs[j].nrecords < 0) return MTB_ERR_BAD_SHAPE;
+        if (!jobs[j].h_conv_info) return MTB_ERR_NULL;
+    }
+    return MTB_OK;
+}
+
+static int batch_plans(const mtb_grid_job *jobs, int njobs, GridPlan *plans) {
+    for (int j = 0; j < njobs; j++) {
+        mtb_grid_params p = jobs[j].params;
+        p.merge = 0;
+        MTB_TRY(make_plan(&p, jobs[j].h_conv_info, &plans[j]));
+    }
+    return MTB_OK;
+}
+
+// every job's space, then the batch queue, its length and its counter
+static void carve_batch(Arena &A, const mtb_grid_job *jobs, int njobs, const GridPlan *plans, GridSpace *spaces,
+                        int4 **items, int **n_total, int **counter) {
+    size_t cap = 0;
+    for (int j = 0; j < njobs; j++) {
+        const mtb_grid_params *p = &jobs[j].params;
+        carve_grid(A, jobs[j].nrecords, p->npol, plans[j].chunk, padded_elems_of(p, jobs[j].h_conv_info),
+                   (size_t)p->nx * p->ny, &spaces[j], p->wplanes);
+        const size_t r = (size_t)(jobs[j].nrecords > 0 ? jobs[j].nrecords : 1);
+        cap += r + r / (size_t)plans[j].chunk + 2;
+    }
+    *items = A.take<int4>(cap);
+    *n_total = A.take<int>(1);
+    *counter = A.take<int>(1);
+}
+
+extern "C" int mtb_grid_batch_workspace_size(const mtb_grid_job *jobs, int njobs, size_t *bytes) {
+    if (!bytes) return MTB_ERR_NULL;
+    MTB_TRY(check_batch(jobs, njobs));
+    GridPlan plans[kMaxBatch];
+    MTB_TRY(batch_plans(jobs, njobs, plans));
+    Arena A;
+    GridSpace spaces[kMaxBatch];
+    int4 *items;
+    int *n_total, *counter;
+    carve_batch(A, jobs, njobs, plans, spaces, &items, &n_total, &counter);
+    *bytes = A.used;
+    return MTB_OK;
+}
+
+template <int P>
+static int run_batch(const mtb_grid_job *jobs, int njobs, const GridPlan *plans, GridSpace *spaces, int4 *items,
+                     int *n_total, int *counter, cudaStream_t st) {
+    BatchQueues q;
+    Grid2Args g2;
+    g2.njobs = njobs;
+    for (int j = 0; j < njobs; j++) {
+        const mtb_grid_job &J = jobs[j];
+        mtb_grid_params p = J.params;
+        p.merge = 0;
+        q.items[j] = spaces[j].items;
+        q.n_items[j] = nullptr;
+        g2.jobs[j] = job_desc<P>(&p, (float *)J.d_grid, J.d_grid_lo != nullptr, spaces[j]);
+        if (J.nrecords == 0) continue;
+        const size_t te = table_elems_of(&p, J.h_conv_info), pe = padded_elems_of(&p, J.h_conv_info);
+        MTB_TRY(prepare_grid<P>(&p, plans[j], (const float2 *)J.d_table, te, pe, J.d_conv_info, J.d_conv_sums,
+                                J.d_uvw, J.d_freq, (const float2 *)J.d_vis, J.d_weights, J.d_flags, J.nrecords,
+                                J.d_grid_lo != nullptr, spaces[j], st));
+        q.n_items[j] = spaces[j].n_items;
+    }
+    const mtb_grid_params &p0 = jobs[0].params;
+    if (p0.gridder_start_event) MTB_CUDA_TRY(cudaEventRecord((cudaEvent_t)p0.gridder_start_event, st));
+    k_concat_items<<<njobs, 256, 0, st>>>(q, njobs, items, n_total);
+    MTB_LAUNCHED();
+    MTB_CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(int), st));
+    g2.items = items;
+    g2.n_items = n_total;
+    g2.counter = counter;
+    MTB_TRY(launch_grid3<P>(g2, st));
+    if (p0.gridder_end_event) MTB_CUDA_TRY(cudaEventRecord((cudaEvent_t)p0.gridder_end_event, st));
+    for (int j = 0; j < njobs; j++) {
+        const mtb_grid_job &J = jobs[j];
+        if (J.nrecords == 0) continue;
+        MTB_TRY(finish_grid<P>(&J.params, (float *)J.d_grid, (float *)J.d_grid_lo, J.d_normalizer, J.d_stats,
+                               spaces[j], st));
+    }
+    return MTB_OK;
+}
+
+extern "C" int mtb_grid_batch(const mtb_grid_job *jobs, int njobs, void *d_workspace, size_t workspace_bytes,
+                              mtb_stream_t stream) {
+    MTB_TRY(check_batch(jobs, njobs));
+    cudaStream_t st = (cudaStream_t)stream;
+    for (int j = 0; j < njobs; j++) {
+        const mtb_grid_job &J = jobs[j];
+        if (!J.d_grid || !J.d_normalizer) return MTB_ERR_NULL;
+        if (J.nrecords > 0 && (!J.d_table || !J.d_conv_info || !J.d_conv_sums || !J.d_uvw || !J.d_freq ||
+                               (!J.d_vis && !J.params.psf) || !J.d_weights || !J.d_flags))
+            return MTB_ERR_NULL;
+    }
+    if (!d_workspace) return MTB_ERR_NULL;
+    GridPlan plans[kMaxBatch];
+    MTB_TRY(batch_plans(jobs, njobs, plans));
+    Arena A(d_workspace, workspace_bytes);
+    GridSpace spaces[kMaxBatch];
+    int4 *items;
+    int *n_total, *counter;
+    carve_batch(A, jobs, njobs, plans, spaces, &items, &n_total, &counter);
+    if (!A.ok()) return MTB_ERR_WORKSPACE;
+    for (int j = 0; j < njobs; j++) {
+        const mtb_grid_job &J = jobs[j];
+        const mtb_grid_params &p = J.params;
+        if (!p.initialize_output) continue;
+        const size_t gbytes = (size_t)p.nx * p.ny * p.npol * sizeof(float2);
+        MTB_CUDA_TRY(cudaMemsetAsync(J.d_grid, 0, gbytes, st));
+        if (J.d_grid_lo) MTB_CUDA_TRY(cudaMemsetAsync(J.d_grid_lo, 0, gbytes, st));
+        MTB_CUDA_TRY(cudaMemsetAsync(J.d_normalizer, 0, p.npol * sizeof(float), st));
+        if (J.d_stats) MTB_CUDA_TRY(cudaMemsetAsync(J.d_stats, 0, sizeof(mtb_grid_stats), st));
+    }
+    const int P = jobs[0].params.npol;
+    if (P == 1) return run_batch<1>(jobs, njobs, plans, spaces, items, n_total, counter, st);
+    if (P == 2) return run_batch<2>(jobs, njobs, plans, spaces, items, n_total, counter, st);
+    return run_batch<4>(jobs, njobs, plans, spaces, items, n_total, counter, st);
 }
 
 extern "C" int mtb_preprocess_uvw(const mtb_grid_params *p, const int *d_conv_info, const int *h_conv_info,

@@ -25,7 +25,7 @@ EXPORTS = (
     "mtb_preprocess_uvw_noalloc", "mtb_preprocess_uvw_noalloc_capacity",
     "mtb_finalize_workspace_size", "mtb_finalize", "mtb_status_string", "mtb_version",
     "mtb_release_caches", "mtb_kernel_launch_count", "mtb_calibrate_fp32",
-    "mtb_taper_kernel_build", "mtb_fits_create", "mtb_fits_write_channel", "mtb_fits_close",
+    "mtb_taper_kernel_build", "mtb_grid_batch_workspace_size", "mtb_grid_batch", "mtb_fits_create", "mtb_fits_write_channel", "mtb_fits_close",
     "mtb_engine_create", "mtb_engine_submit", "mtb_engine_wait", "mtb_engine_request_bytes", "mtb_engine_destroy",
 )
 
@@ -68,6 +68,14 @@ class GridStats(ctypes.Structure):
 class FinalizeParams(ctypes.Structure):
     _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("npol", ctypes.c_int), ("sampling", ctypes.c_int),
                 ("pol_type", ctypes.c_int)]
+
+
+class GridJob(ctypes.Structure):
+    _fields_ = [("params", GridParams), ("d_table", ctypes.c_void_p), ("d_conv_info", ctypes.c_void_p),
+                ("h_conv_info", ctypes.c_void_p), ("d_conv_sums", ctypes.c_void_p), ("d_uvw", ctypes.c_void_p),
+                ("d_freq", ctypes.c_void_p), ("d_vis", ctypes.c_void_p), ("d_weights", ctypes.c_void_p),
+                ("d_flags", ctypes.c_void_p), ("nrecords", ctypes.c_int), ("d_grid", ctypes.c_void_p),
+                ("d_grid_lo", ctypes.c_void_p), ("d_normalizer", ctypes.c_void_p), ("d_stats", ctypes.c_void_p)]
 
 
 class FitsHeader(ctypes.Structure):
@@ -127,6 +135,8 @@ def load(path: str = LIB_PATH):
     L.mtb_kernel_launch_count.restype = ctypes.c_ulonglong
     L.mtb_kernel_launch_count.argtypes = []
     L.mtb_calibrate_fp32.argtypes = [ctypes.POINTER(ctypes.c_double), p]
+    L.mtb_grid_batch_workspace_size.argtypes = [ctypes.POINTER(GridJob), i, ctypes.POINTER(sz)]
+    L.mtb_grid_batch.argtypes = [ctypes.POINTER(GridJob), i, p, sz, p]
     L.mtb_fits_create.argtypes = [ctypes.c_char_p, ctypes.POINTER(FitsHeader), ctypes.POINTER(p)]
     L.mtb_fits_write_channel.argtypes = [p, i, p]
     L.mtb_fits_close.argtypes = [p]

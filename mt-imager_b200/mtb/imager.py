@@ -236,3 +236,40 @@ class WProjectionImager:
         s = self.stats.cpu().numpy()
         return dict(gridded_records=int(s[0]), compressed_records=int(s[1]), gridded_points=int(s[2]),
                     compressed_points=int(s[3]))
+
+
+def grid_batch(entries, workspace=None, stream=None):
+    """Grid one chunk into each of several images with one persistent gridder
+    launch (mtb_grid_batch).  entries: (WProjectionImager, uvw, freq, vis,
+    weights, flags) with device tensors in the layouts of grid_device; every
+    imager must have the same npol.  Returns the workspace tensor so a caller
+    can pass it back (or keep it alive across a CUDA graph replay)."""
+    if not entries:
+        return workspace
+    lib = L.load()
+    jobs = (L.GridJob * len(entries))()
+    keep = []
+    for j, (im, uvw, freq, vis, weights, flags) in enumerate(entries):
+        k = im.build_kernels()
+        gp = im.grid_params(im._fresh)
+        J = jobs[j]
+        J.params = gp
+        J.d_table, J.d_conv_info = _ptr(k.table), _ptr(k.d_conv_info)
+        J.h_conv_info = k.conv_info.ctypes.data_as(ctypes.c_void_p)
+        J.d_conv_sums = _ptr(k.conv_sums)
+        J.d_uvw, J.d_freq, J.d_vis = _ptr(uvw), _ptr(freq), _ptr(vis)
+        J.d_weights, J.d_flags = _ptr(weights), _ptr(flags)
+        J.nrecords = int(freq.numel())
+        J.d_grid, J.d_grid_lo = _ptr(im.grid), _ptr(im.grid_lo)
+        J.d_normalizer, J.d_stats = _ptr(im.normalizer), _ptr(im.stats)
+        keep.append(k)
+    need = ctypes.c_size_t(0)
+    L.check(lib.mtb_grid_batch_workspace_size(jobs, len(entries), ctypes.byref(need)),
+            "mtb_grid_batch_workspace_size")
+    if workspace is None or workspace.numel() < need.value:
+        workspace = torch.empty(max(1, need.value), dtype=torch.uint8, device=entries[0][0].device)
+    L.check(lib.mtb_grid_batch(jobs, len(entries), _ptr(workspace), need.value, _stream(stream)),
+            "mtb_grid_batch")
+    for im, *_ in entries:
+        im._fresh = False
+    return workspace
