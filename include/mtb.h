@@ -149,6 +149,10 @@ typedef struct mtb_grid_params {
     int psf;                   /* 1: grid every visibility as 1 + 0i (the PSF; mt-imager's
                                   psf=true, VisibilityForPSFStorageManager.cpp:65-77);
                                   d_vis may then be NULL                                   */
+    int exact_delta;           /* compensated mode (d_grid_lo set): 0 (default) the call's
+                                  flushes accumulate in an FP32 delta grid merged into
+                                  (grid, grid_lo) with TwoSum; 1 they accumulate in FP64
+                                  (order-independent, about half the grid error, slower)   */
 } mtb_grid_params;
 
 typedef struct mtb_grid_stats {

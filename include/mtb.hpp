@@ -151,8 +151,9 @@ public:
     // buffers: kept by the caller and reused across images, or nullptr to let
     // the imager own its own
     Imager(std::shared_ptr<const KernelTable> k, int npol, int pol_type, bool compensated, cudaStream_t stream,
-           ImagerBuffers *buffers = nullptr)
-        : k_(std::move(k)), npol_(npol), pol_type_(pol_type), compensated_(compensated), s_(stream) {
+           ImagerBuffers *buffers = nullptr, bool exact_delta = false)
+        : k_(std::move(k)), npol_(npol), pol_type_(pol_type), compensated_(compensated), exact_delta_(exact_delta),
+          s_(stream) {
         if (!buffers) {
             own_.reset(new ImagerBuffers());
             buffers = own_.get();
@@ -184,6 +185,7 @@ public:
         gp.v_increment = k_->info.v_increment;
         gp.w_sq_increment = k_->info.w_sq_increment;
         gp.initialize_output = fresh_ ? 1 : 0;
+        gp.exact_delta = exact_delta_ ? 1 : 0;
         return gp;
     }
 
@@ -235,7 +237,7 @@ public:
 private:
     std::shared_ptr<const KernelTable> k_;
     int npol_, pol_type_;
-    bool compensated_;
+    bool compensated_, exact_delta_;
     cudaStream_t s_;
     bool fresh_ = true;
     std::unique_ptr<ImagerBuffers> own_;

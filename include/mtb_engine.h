@@ -14,7 +14,8 @@
  *     shared by every request of that geometry;
  *   - a request's records are streamed in chunks from host memory through
  *     pinned, double-buffered staging, each chunk gridded by mtb_grid.
- * The image of a request is the same whether it runs alone or in a mix.
+ * The image of a request is the same whether it runs alone or in a mix (to
+ * the rounding of the FP32 reductions, or exactly with exact_delta).
  */
 #ifndef MTB_ENGINE_H
 #define MTB_ENGINE_H
@@ -47,6 +48,8 @@ typedef struct mtb_image_request {
     const float *weights;         /* [R][P]                                                */
     const int *flags;             /* [R][P]                                                */
     float *image;                 /* host output [P][ny][nx]                               */
+    int exact_delta;              /* compensated gridding with an FP64 per-call delta grid
+                                     (order-independent result); see mtb_grid_params       */
 } mtb_image_request;
 
 typedef struct mtb_image_result {

@@ -166,6 +166,7 @@ int request_bytes(const mtb_engine_config &cfg, const mtb_image_request *r, size
     size_t fin = 0;
     s = mtb_finalize_workspace_size(&fp, &fin);
     if (s != MTB_OK) return s;
+    gp.exact_delta = r->exact_delta;
     *out = cells * 8 * (r->compensated ? 2 : 1) + cells * 4 + ws + fin + (1 << 20);
     return MTB_OK;
 }
@@ -244,7 +245,7 @@ void mtb_engine::run(mtb::Job *j, cudaStream_t st, unsigned char *const pinned[2
         bool hit = false;
         std::shared_ptr<mtb::KernelTable> k = cache->get(r.geometry, st, &hit);
         j->res.kernel_cache_hit = hit ? 1 : 0;
-        mtb::Imager im(k, P, r.pol_type, r.compensated != 0, st, &bufs);
+        mtb::Imager im(k, P, r.pol_type, r.compensated != 0, st, &bufs, r.exact_delta != 0);
         const int chunk = cfg.chunk_records;
         int b = 0;
         for (int c0 = 0; c0 < R; c0 += chunk, b ^= 1) {

@@ -37,9 +37,9 @@
 //                  ring with cp.async.bulk (mbarrier pipeline); 11 consumer
 //                  warps accumulate from it.
 //   k_grid         shared-memory tile-window variant (merge = 1).
-//   k_merge_delta  compensated mode: flushes go to an FP64 delta grid of the
-//                  call (plain reductions), merged afterwards into the two-float
-//                  grid (hi, lo).
+//   k_merge_delta  compensated mode: flushes go to a delta grid of the call
+//                  (plain reductions; FP32, or FP64 with exact_delta), merged
+//                  afterwards into the two-float grid (hi, lo).
 #include <cub/cub.cuh>
 
 #include <algorithm>
@@ -1177,6 +1177,36 @@ __global__ void k_split(const int *__restrict__ bounds, const int *__restrict__ 
 // Compensated merge of one call's FP64 contribution into the two-float grid:
 // (hi + lo) + delta evaluated in FP64 and split back into the float pair.  One
 // pass over the cells, no atomics; cells the call did not touch are skipped.
+// FP32 delta grid (default): hi + lo += delta with the rounding error of
+// hi + delta kept in lo (TwoSum).
+__global__ void k_merge_delta32(float4 *__restrict__ hi, float4 *__restrict__ lo, const float4 *__restrict__ delta,
+                                size_t n4) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n4; i += (size_t)gridDim.x * blockDim.x) {
+        const float4 d = delta[i];
+        if (d.x == 0.f && d.y == 0.f && d.z == 0.f && d.w == 0.f) continue;
+        float4 h = hi[i], e = lo[i];
+        float sx, bp;
+        sx = h.x + d.x; bp = sx - h.x; e.x += (h.x - (sx - bp)) + (d.x - bp); h.x = sx;
+        sx = h.y + d.y; bp = sx - h.y; e.y += (h.y - (sx - bp)) + (d.y - bp); h.y = sx;
+        sx = h.z + d.z; bp = sx - h.z; e.z += (h.z - (sx - bp)) + (d.z - bp); h.z = sx;
+        sx = h.w + d.w; bp = sx - h.w; e.w += (h.w - (sx - bp)) + (d.w - bp); h.w = sx;
+        hi[i] = h;
+        lo[i] = e;
+    }
+}
+
+// the last complex value when the float count is not a multiple of 4 (npol 1)
+__global__ void k_merge_delta32_tail(float2 *hi, float2 *lo, const float2 *delta, size_t i) {
+    const float2 d = delta[i];
+    float2 h = hi[i], e = lo[i];
+    float sx, bp;
+    sx = h.x + d.x; bp = sx - h.x; e.x += (h.x - (sx - bp)) + (d.x - bp); h.x = sx;
+    sx = h.y + d.y; bp = sx - h.y; e.y += (h.y - (sx - bp)) + (d.y - bp); h.y = sx;
+    hi[i] = h;
+    lo[i] = e;
+}
+
+// FP64 delta grid (exact_delta = 1)
 __global__ void k_merge_delta(float2 *__restrict__ hi, float2 *__restrict__ lo, const double2 *__restrict__ delta,
                               size_t n2) {
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n2; i += (size_t)gridDim.x * blockDim.x) {
@@ -1220,7 +1250,7 @@ struct GridSpace {
     int *split;          // first work item of k_grid4
     int *counter4;       // k_grid4 work counter
     int *err;            // gridder pipeline error flag
-    double *delta;       // this call's grid contribution (compensated mode), FP64
+    double *delta;       // this call's grid contribution (compensated mode; FP64 or FP32)
 };
 
 static size_t cub_bytes(int n) {
@@ -1454,11 +1484,13 @@ static int prepare_grid(const mtb_grid_params *p, const GridPlan &plan, const fl
     MTB_LAUNCHED();
     MTB_CUDA_TRY(cudaMemsetAsync(s.counter4, 0, sizeof(int), st));
     MTB_CUDA_TRY(cudaMemsetAsync(s.err, 0, sizeof(int), st));
-    // compensated mode: the call's flushes go to a zeroed FP64 delta grid
-    // with plain reductions (no returned values, so no stall at a flush)
-    // and one pass merges it into the float pair (grid, grid_lo)
+    // compensated mode: the call's flushes go to a zeroed delta grid with
+    // plain reductions (no returned values, so no stall at a flush) and one
+    // pass merges it into the float pair (grid, grid_lo)
     if (compensated)
-        MTB_CUDA_TRY(cudaMemsetAsync(s.delta, 0, (size_t)p->nx * p->ny * 2 * P * sizeof(double), st));
+        MTB_CUDA_TRY(cudaMemsetAsync(s.delta, 0,
+                                     (size_t)p->nx * p->ny * 2 * P * (p->exact_delta ? sizeof(double) : sizeof(float)),
+                                     st));
     return MTB_OK;
 }
 
@@ -1468,8 +1500,10 @@ static GridJobDesc job_desc(const mtb_grid_params *p, float *grid, bool compensa
     d.wpos = s.wpos;
     d.wvis4 = (const float4 *)s.wvis;
     d.table2 = s.table2;
-    d.grid = grid;
-    d.dgrid = compensated ? s.delta : nullptr;
+    // compensated: flushes go to the call's delta grid, FP32 (vector
+    // reductions, the default) or FP64 (exact_delta)
+    d.grid = (compensated && !p->exact_delta) ? (float *)s.delta : grid;
+    d.dgrid = (compensated && p->exact_delta) ? s.delta : nullptr;
     d.M = s.moduli;
     d.nx = p->nx;
     d.pad_ = 0;
@@ -1484,10 +1518,23 @@ static int finish_grid(const mtb_grid_params *p, float *grid, float *grid_lo, fl
     const int sms = sm_count();
     if (grid_lo) {
         const size_t n2 = (size_t)p->nx * p->ny * P;     // complex values
-        int mb = (int)std::min<size_t>((n2 + 255) / 256, (size_t)sms * 16);
-        k_merge_delta<<<mb > 0 ? mb : 1, 256, 0, st>>>((float2 *)grid, (float2 *)grid_lo,
-                                                     (const double2 *)s.delta, n2);
-        MTB_LAUNCHED();
+        if (p->exact_delta) {
+            int mb = (int)std::min<size_t>((n2 + 255) / 256, (size_t)sms * 16);
+            k_merge_delta<<<mb > 0 ? mb : 1, 256, 0, st>>>((float2 *)grid, (float2 *)grid_lo,
+                                                         (const double2 *)s.delta, n2);
+            MTB_LAUNCHED();
+        } else {
+            const size_t n4 = n2 / 2;
+            int mb = (int)std::min<size_t>((n4 + 255) / 256, (size_t)sms * 16);
+            k_merge_delta32<<<mb > 0 ? mb : 1, 256, 0, st>>>((float4 *)grid, (float4 *)grid_lo,
+                                                           (const float4 *)s.delta, n4);
+            MTB_LAUNCHED();
+            if (n2 & 1) {
+                k_merge_delta32_tail<<<1, 1, 0, st>>>((float2 *)grid, (float2 *)grid_lo, (const float2 *)s.delta,
+                                                      n2 - 1);
+                MTB_LAUNCHED();
+            }
+        }
     }
     k_finish<<<1, 32, 0, st>>>(P, s.norm_acc, normalizer, s.stats, stats);
     MTB_LAUNCHED();
@@ -1551,7 +1598,7 @@ static int run_grid(const mtb_grid_params *p, const GridPlan &plan, const float2
     g4.wpos = s.wpos;
     g4.wvis4 = (const float4 *)s.wvis;
     g4.ptab = s.ptab;
-    g4.grid = grid;
+    g4.grid = g2.jobs[0].grid;
     g4.dgrid = g2.jobs[0].dgrid;
     g4.nx = p->nx;
     g4.bt = plan.bt;

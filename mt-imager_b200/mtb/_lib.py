@@ -57,7 +57,7 @@ class GridParams(ctypes.Structure):
                 ("w_sq_increment", ctypes.c_double), ("initialize_output", ctypes.c_int), ("tile", ctypes.c_int),
                 ("support_bucket", ctypes.c_int), ("max_chunk", ctypes.c_int), ("merge", ctypes.c_int),
                 ("gridder_start_event", ctypes.c_void_p), ("gridder_end_event", ctypes.c_void_p),
-                ("bulk_min_support", ctypes.c_int), ("psf", ctypes.c_int)]
+                ("bulk_min_support", ctypes.c_int), ("psf", ctypes.c_int), ("exact_delta", ctypes.c_int)]
 
 
 class GridStats(ctypes.Structure):
@@ -94,7 +94,7 @@ class ImageRequest(ctypes.Structure):
     _fields_ = [("geometry", WKernelParams), ("npol", ctypes.c_int), ("pol_type", ctypes.c_int),
                 ("compensated", ctypes.c_int), ("nrecords", ctypes.c_int), ("uvw", ctypes.c_void_p),
                 ("freq", ctypes.c_void_p), ("vis", ctypes.c_void_p), ("weights", ctypes.c_void_p),
-                ("flags", ctypes.c_void_p), ("image", ctypes.c_void_p)]
+                ("flags", ctypes.c_void_p), ("image", ctypes.c_void_p), ("exact_delta", ctypes.c_int)]
 
 
 class ImageResult(ctypes.Structure):

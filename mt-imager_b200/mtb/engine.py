@@ -40,7 +40,8 @@ class Engine:
         self._pending = {}
 
     def _request(self, nx, ny, l_increment, m_increment, wplanes, sampling, uvw, freq, vis, weights, flags,
-                 trial_support=0, max_support=0, w_max=0.0, pol_type=L.MTB_POL_LINEAR, compensated=True):
+                 trial_support=0, max_support=0, w_max=0.0, pol_type=L.MTB_POL_LINEAR, compensated=True,
+                 exact_delta=False):
         uvw = _c(uvw, np.float32)
         freq = _c(freq, np.float32)
         vis = _c(vis, np.complex64)
@@ -55,7 +56,7 @@ class Engine:
                             max_support, float(w_max))
         ptr = lambda a: a.ctypes.data_as(ctypes.c_void_p)  # noqa: E731
         req = L.ImageRequest(g, P, pol_type, int(bool(compensated)), R, ptr(uvw), ptr(freq), ptr(vis),
-                             ptr(weights), ptr(flags), ptr(image))
+                             ptr(weights), ptr(flags), ptr(image), int(bool(exact_delta)))
         return req, (uvw, freq, vis, weights, flags, image)
 
     def request_bytes(self, *args, **kw) -> int:

@@ -113,7 +113,8 @@ class WProjectionImager:
     def __init__(self, nx, ny, l_increment, m_increment=None, wplanes=32, sampling=8, npol=4,
                  trial_support=0, max_support=0, w_max=0.0, pol_type=L.MTB_POL_LINEAR, compensated=True,
                  tile=0, support_bucket=0, max_chunk=0, merge=0, bulk_min_support=0, device="cuda",
-                 kernels: KernelTable | None = None, psf=False, mode="wproj", taper_support=7):
+                 kernels: KernelTable | None = None, psf=False, mode="wproj", taper_support=7,
+                 exact_delta=False):
         """mode "wproj" (W-projection kernels) or "normal" (taper-only kernel of
         support taper_support at oversampling `sampling`, one plane); psf
         grids every visibility as 1 + 0i (mt-imager's psf=true)."""
@@ -124,6 +125,7 @@ class WProjectionImager:
         if mode not in ("wproj", "normal"):
             raise ValueError("mode must be 'wproj' or 'normal'")
         self.mode, self.psf, self.taper_support = mode, bool(psf), taper_support
+        self.exact_delta = bool(exact_delta)
         if mode == "normal":
             wplanes = 1
         self.params = wkernel_params(nx, ny, l_increment, m_increment, wplanes, sampling, trial_support,
@@ -163,6 +165,7 @@ class WProjectionImager:
                           self.tuning["merge"])
         gp.bulk_min_support = self.tuning["bulk_min_support"]
         gp.psf = int(self.psf)
+        gp.exact_delta = int(self.exact_delta)
         if self.gridder_events is not None:
             gp.gridder_start_event = self.gridder_events[0].cuda_event
             gp.gridder_end_event = self.gridder_events[1].cuda_event

@@ -43,7 +43,8 @@ int main(int argc, char **argv) {
         mtb::cuda_check(cudaStreamCreate(&st), "stream");
         mtb_wkernel_params kp{nx, ny, dl, dl, nw, s, 0, 0, 0.0};
         auto k = mtb::KernelTable::build(kp, st);
-        mtb::Imager im(k, P, pol, comp != 0, st);
+        // FP64 per-call delta grid: an order-independent, reproducible image
+        mtb::Imager im(k, P, pol, comp != 0, st, nullptr, /*exact_delta=*/true);
         mtb::DeviceArray<float> d_uvw(uvw.size(), st), d_freq(freq.size(), st), d_vis(vis.size(), st),
             d_wt(wt.size(), st), d_img((size_t)P * nx * ny, st);
         mtb::DeviceArray<int> d_fl(fl.size(), st);

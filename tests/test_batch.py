@@ -1,8 +1,8 @@
 """mtb_grid_batch: several images -- different geometries, kernel tables and
 record counts, one of them empty -- gridded with one persistent launch must
 equal mtb_grid image by image; the batch and the finaliser replay correctly
-from a captured CUDA graph.  Compensated gridding is order-independent (FP64
-delta grid), so the bound is tight."""
+from a captured CUDA graph.  With the FP64 per-call delta grid the result is
+order-independent, so the bound is tight."""
 import numpy as np
 import pytest
 import torch
@@ -30,7 +30,9 @@ def cases():
 
 
 def imager(setup):
-    return WProjectionImager(setup.nx, setup.ny, setup.dl, wplanes=setup.wplanes, sampling=setup.sampling)
+    # FP64 per-call delta grid: the result does not depend on the order of the reductions
+    return WProjectionImager(setup.nx, setup.ny, setup.dl, wplanes=setup.wplanes, sampling=setup.sampling,
+                             exact_delta=True)
 
 
 def test_batch_equals_single():

@@ -55,7 +55,9 @@ def test_engine_image_matches_oracle(oracle):
 def test_alone_equals_in_mix():
     from mtb.engine import Engine
     cases = [case(41, 128, 4)[0], case(42, 96, 2, s=3, nw=6)[0], case(43, 64, 1, nw=4)[0], case(44, 128, 4)[0]]
-    kws = [dict(), dict(pol_type=L.MTB_POL_CIRCULAR), dict(compensated=True), dict(compensated=True)]
+    # exact_delta: order-independent accumulation, so alone and mixed agree to rounding of the merge
+    kws = [dict(exact_delta=True), dict(pol_type=L.MTB_POL_CIRCULAR, exact_delta=True), dict(exact_delta=True),
+           dict(exact_delta=True)]
     alone = []
     with Engine(slots=1, chunk_records=1500) as e:
         for c, kw in zip(cases, kws):
@@ -112,7 +114,7 @@ def test_cpp_host_api(tmp_path):
     subprocess.run([str(exe), str(inp), str(out)], check=True)
     raw = np.fromfile(out, np.uint8)
     img = raw[: 4 * P * 128 * 128].view(np.float32).reshape(P, 128, 128)
-    im = WProjectionImager(128, 128, setup.dl, wplanes=8, sampling=4)
+    im = WProjectionImager(128, 128, setup.dl, wplanes=8, sampling=4, exact_delta=True)
     im.build_kernels()
     im.grid_chunk(c["uvw"], c["freq"], c["vis"], c["weights"], c["flags"])
     ref = im.finalize().cpu().numpy()
