@@ -29,9 +29,10 @@
 //                  positions (Romein's assignment: cell x belongs to the slot
 //                  with a == x mod M), accumulate V * C in registers with packed
 //                  f32x2 FMAs while their cell is unchanged, and flush a cell
-//                  when it changes -- no global atomic per sample.  Kernel taps
-//                  are fetched a few records ahead into a per-thread
-//                  shared-memory ring with cp.async.
+//                  when it changes -- no global atomic per sample.  Each item's
+//                  (support-box unit, record stream) jobs are balanced over
+//                  the block's threads.  Kernel taps are fetched a few records
+//                  ahead into a per-thread shared-memory ring with cp.async.
 //   k_grid4        opt-in gridder for large supports: one producer warp copies
 //                  the needed kernel rows of every record into a shared-memory
 //                  ring with cp.async.bulk (mbarrier pipeline); 11 consumer
@@ -533,7 +534,7 @@ __global__ void __launch_bounds__(KMAX >= 8 ? 576 : 1024) k_grid(GridArgs a) {
 // f32x2 FMAs and merges into the grid (vector reductions) only when its cell
 // changes and at the end of a pass.
 static const int kG2Threads = 256;
-static const int kG3Threads = kG2Threads;   // block size (layout_for assumes it)
+static const int kG3Threads = kG2Threads;   // block size
 static const int kG3Chunk = 512;            // records of one work item, staged at once
 static const int kG3Depth = 4;              // records of kernel values fetched ahead
 static const int kG3KS = 4;                 // support-box slots per thread
@@ -612,24 +613,36 @@ __device__ __forceinline__ void flush2(float *grid, double *dgrid, int cell, con
     flush_cell<P>(grid, dgrid, cell, v);
 }
 
-// Thread layout for modulus M (KS slots per thread, all in one support-box
-// column so the column offset is computed once per record):
-//   G  = ceil(M / KS) row groups; a thread of row group g owns rows g + j*G.
-//   Gp = row groups one pass covers (<= kG2Threads / M); passes = ceil(G / Gp).
-//   With a single pass, kG2Threads / (M*G) independent streams split the
-//   item's records into contiguous runs (small supports fill the block that
-//   way; every flush is an atomic merge, so streams may share cells).
-struct Layout {
-    int G, Gp, npass, nstream;
-};
-__device__ __forceinline__ Layout layout_for(int M, int KS) {
-    Layout L;
-    L.G = (M + KS - 1) / KS;
-    int gmax = kG2Threads / M;
-    L.Gp = L.G < gmax ? L.G : gmax;
-    L.npass = (L.G + L.Gp - 1) / L.Gp;
-    L.nstream = (L.npass == 1) ? kG2Threads / (M * L.G) : 1;
-    return L;
+// Work schedule of one item for modulus M (KS slots per thread, all in one
+// support-box column so the column offset is computed once per record):
+//   G = ceil(M / KS) row groups; a unit (column c, row group g) owns the rows
+//   g + j*G of column c; U = M * G units cover the support box.
+//   The item's N records are split into ns contiguous streams; a job is one
+//   (stream, unit) pair, jobs are numbered unit-fastest (so the threads of a
+//   warp share records) and thread t takes jobs t, t + T, t + 2T, ...
+//   ns minimises rounds * (ceil(N / ns) + kSegCost), rounds = ceil(ns*U / T):
+//   the slowest thread's time, each job paying a fixed cost for filling its
+//   look-ahead and flushing its slots.  Every flush is an atomic merge, so
+//   streams may share cells.
+static const int kSegCost = 4;        // per-job overhead in record times
+
+// ns in [1, min(N, 64)]; all lanes of a warp return the same value
+// (warp-wide argmin, two candidates per lane).
+__device__ __forceinline__ int pick_streams(int U, int N, int T) {
+    const int lane = threadIdx.x & 31;
+    unsigned best = 0xFFFFFFFFu;
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+        const int c = lane + 1 + 32 * h;
+        if (c <= N) {
+            const unsigned rounds = (unsigned)((c * U + T - 1) / T);
+            const unsigned cost = rounds * (unsigned)((N + c - 1) / c + kSegCost);
+            const unsigned key = (cost << 7) | (unsigned)c;
+            best = key < best ? key : best;
+        }
+    }
+    best = __reduce_min_sync(0xFFFFFFFFu, best);
+    return best == 0xFFFFFFFFu ? 1 : (int)(best & 127u);
 }
 
 // Row-padded copy of the kernel table for the direct gridders: every
@@ -714,20 +727,21 @@ __global__ void __launch_bounds__(kG3Threads, 2) k_grid3(Grid2Args a) {
         cp_async_wait<0>();
         __syncthreads();
         const int M = J.M[(unsigned)it.z >> 24];
-        const Layout L = layout_for(M, KS);
-        const int per_stream = M * L.Gp;
-        const int stream = t / per_stream;
-        const int r = t - stream * per_stream;
-        const int col = r % M;
-        const int gl = r / M;
-        const bool live = stream < L.nstream;
-        const int i0 = live ? (int)(((long)it.y * stream) / L.nstream) : 0;
-        const int i1 = live ? (int)(((long)it.y * (stream + 1)) / L.nstream) : 0;
-        for (int pass = 0; pass < L.npass; pass++) {
-            const int g = pass * L.Gp + gl;
+        const int G = (M + KS - 1) / KS;
+        const int U = M * G;
+        const int N = it.y;
+        const int ns = pick_streams(U, N, kG3Threads);
+        const int njobs = ns * U;
+        for (int job = t; job < njobs; job += kG3Threads) {
+            const int stream = job / U;
+            const int u = job - stream * U;
+            const int g = u / M;
+            const int col = u - g * M;
+            const int i0 = (int)(((long)N * stream) / ns);
+            const int i1 = (int)(((long)N * (stream + 1)) / ns);
             // rows g + j*G that exist: j < nrow
-            const int nrow = (live && g < L.G) ? (M - g + L.G - 1) / L.G : 0;
-            if (nrow == 0 || i0 >= i1) continue;
+            const int nrow = (M - g + G - 1) / G;
+            if (i0 >= i1) continue;
             // Slot geometry depends only on the record's corner and support;
             // vmul = 0 marks a slot outside the record's box.
             auto geometry = [&](const int4 &rec, int *cell, int *toff, int *vmul) {
@@ -743,7 +757,7 @@ __global__ void __launch_bounds__(kG3Threads, 2) k_grid3(Grid2Args a) {
                     cell[j] = ok ? rec.x + sy * gnx + sx : -1;
                     toff[j] = ok ? sy * (S + 1) + sx : 0;
                     vmul[j] = ok ? 1 : 0;
-                    sy += L.G;
+                    sy += G;
                     sy -= (sy >= M) ? M : 0;
                 }
             };
