@@ -582,6 +582,13 @@ __device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sa), "l"(gmem) : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+// Copies 16 bytes, or writes 16 zero bytes (nothing is read) when !valid;
+// gmem must be a mapped address either way.
+__device__ __forceinline__ void cp_async16_zfill(void *smem, const void *gmem, bool valid) {
+    unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(sa), "l"(gmem), "r"(valid ? 16 : 0)
+                 : "memory");
+}
 template <int N>
 __device__ __forceinline__ void cp_async_wait() {
     asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
@@ -599,6 +606,17 @@ __device__ __forceinline__ void flush_cell(float *grid, double *dgrid, int cell,
     } else {
         merge_cell<P>(grid + g, nullptr, v);
     }
+}
+
+template <int P>
+__device__ __forceinline__ void flush2(float *grid, double *dgrid, int cell, const float2 *acc) {
+    float v[2 * P];
+#pragma unroll
+    for (int p = 0; p < P; p++) {
+        v[2 * p] = acc[p].x;
+        v[2 * p + 1] = acc[p].y;
+    }
+    flush_cell<P>(grid, dgrid, cell, v);
 }
 
 template <int P>
@@ -622,19 +640,22 @@ __device__ __forceinline__ void flush2(float *grid, double *dgrid, int cell, con
 //   warp share records) and thread t takes jobs t, t + T, t + 2T, ...
 //   ns minimises rounds * (ceil(N / ns) + kSegCost), rounds = ceil(ns*U / T):
 //   the slowest thread's time, each job paying a fixed cost for filling its
-//   look-ahead and flushing its slots.  Every flush is an atomic merge, so
-//   streams may share cells.
-static const int kSegCost = 4;        // per-job overhead in record times
+//   look-ahead and flushing its slots.  Streams keep at least kMinStreamRecords
+//   records (each stream's flushes are extra FP32 reductions into the same
+//   cells).  Every flush is an atomic merge, so streams may share cells.
+static const int kSegCost = 4;          // per-job overhead in record times
+static const int kMinStreamRecords = 4;
 
-// ns in [1, min(N, 64)]; all lanes of a warp return the same value
-// (warp-wide argmin, two candidates per lane).
+// ns in [1, min(N / kMinStreamRecords, 64)]; all lanes of a warp return the
+// same value (warp-wide argmin, two candidates per lane).
 __device__ __forceinline__ int pick_streams(int U, int N, int T) {
     const int lane = threadIdx.x & 31;
+    const int cmax = N / kMinStreamRecords;
     unsigned best = 0xFFFFFFFFu;
 #pragma unroll
     for (int h = 0; h < 2; h++) {
         const int c = lane + 1 + 32 * h;
-        if (c <= N) {
+        if (c <= cmax) {
             const unsigned rounds = (unsigned)((c * U + T - 1) / T);
             const unsigned cost = rounds * (unsigned)((N + c - 1) / c + kSegCost);
             const unsigned key = (cost << 7) | (unsigned)c;
@@ -771,11 +792,9 @@ __global__ void __launch_bounds__(kG3Threads, 2) k_grid3(Grid2Args a) {
                     keyLw = rec.w;
                 }
                 ulonglong2 *dst = ring + (size_t)(k % D) * KS * kG3Threads + t;
+                // slots outside the box get zeros (toff = 0 keeps the address valid)
 #pragma unroll
-                for (int j = 0; j < KS; j++) {
-                    if (vmulL[j]) cp_async16(dst + j * kG3Threads, &tab[rec.z + toffL[j]]);
-                    else dst[j * kG3Threads] = make_ulonglong2(0ull, 0ull);
-                }
+                for (int j = 0; j < KS; j++) cp_async16_zfill(dst + j * kG3Threads, &tab[rec.z + toffL[j]], vmulL[j]);
             };
 #pragma unroll
             for (int d = 0; d < D; d++) {
@@ -783,16 +802,19 @@ __global__ void __launch_bounds__(kG3Threads, 2) k_grid3(Grid2Args a) {
                 cp_async_commit();
             }
             int last[KS], keyx = -1, keyw = -1;
-            u64 acc[KS][P];
+            float2 acc[KS][P];
 #pragma unroll
             for (int j = 0; j < KS; j++) {
                 last[j] = -1;
 #pragma unroll
-                for (int p = 0; p < P; p++) acc[j][p] = 0ull;
+                for (int p = 0; p < P; p++) acc[j][p] = make_float2(0.f, 0.f);
             }
-            for (int i = i0; i < i1; i++) {
-                const int4 rec = s_rec[i];
-                if (rec.x != keyx || rec.w != keyw) {
+            // Runs of records with the same corner and support: the flushes sit
+            // between runs, so the accumulators stay in place inside a run.
+            int i = i0;
+            int4 rec = s_rec[i0];
+            for (;;) {
+                {
                     // corner or support changed: flush the slots whose cell changes
                     int cellN[KS], toffN[KS], vN[KS];
                     geometry(rec, cellN, toffN, vN);
@@ -804,31 +826,39 @@ __global__ void __launch_bounds__(kG3Threads, 2) k_grid3(Grid2Args a) {
                             if (last[j] >= 0) flush2<P>(ggrid, gdelta, last[j], acc[j]);
                             last[j] = cellN[j];
 #pragma unroll
-                            for (int p = 0; p < P; p++) acc[j][p] = 0ull;
+                            for (int p = 0; p < P; p++) acc[j][p] = make_float2(0.f, 0.f);
                         }
                     }
                 }
-                cp_async_wait<D - 1>();     // this thread's copies for record i have landed
-                u64 vp[P], wp[P];
-#pragma unroll
-                for (int p = 0; p < P; p++) {
-                    ulonglong2 q = s_v[(size_t)i * P + p];
-                    vp[p] = q.x;
-                    wp[p] = q.y;
-                }
-                const ulonglong2 *src = ring + (size_t)(i % D) * KS * kG3Threads + t;
-#pragma unroll
-                for (int j = 0; j < KS; j++) {
-                    const ulonglong2 c = src[j * kG3Threads];
-                    // ConvolutionGridder.cu:153-181: to += vis * wt (no conjugate)
+                bool more;
+                do {
+                    cp_async_wait<D - 1>();     // this thread's copies for record i have landed
+                    float2 vp[P], wp[P];
 #pragma unroll
                     for (int p = 0; p < P; p++) {
-                        ffma2(acc[j][p], c.x, vp[p]);
-                        ffma2(acc[j][p], c.y, wp[p]);
+                        const float4 q = ((const float4 *)s_v)[(size_t)i * P + p];
+                        vp[p] = make_float2(q.x, q.y);
+                        wp[p] = make_float2(q.z, q.w);
                     }
-                }
-                if (i + D < i1) prefetch(i + D);
-                cp_async_commit();
+                    const float4 *src = (const float4 *)(ring + (size_t)(i % D) * KS * kG3Threads + t);
+#pragma unroll
+                    for (int j = 0; j < KS; j++) {
+                        const float4 c = src[j * kG3Threads];
+                        const float2 cre = make_float2(c.x, c.y), cim = make_float2(c.z, c.w);
+                        // ConvolutionGridder.cu:153-181: to += vis * wt (no conjugate)
+#pragma unroll
+                        for (int p = 0; p < P; p++) {
+                            acc[j][p] = __ffma2_rn(cre, vp[p], acc[j][p]);
+                            acc[j][p] = __ffma2_rn(cim, wp[p], acc[j][p]);
+                        }
+                    }
+                    if (i + D < i1) prefetch(i + D);
+                    cp_async_commit();
+                    ++i;
+                    more = i < i1;
+                    if (more) rec = s_rec[i];
+                } while (more && rec.x == keyx && rec.w == keyw);
+                if (!more) break;
             }
             cp_async_wait<0>();
 #pragma unroll
