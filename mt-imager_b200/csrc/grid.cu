@@ -582,11 +582,10 @@ __device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sa), "l"(gmem) : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-// Copies 16 bytes, or writes 16 zero bytes (nothing is read) when !valid;
-// gmem must be a mapped address either way.
-__device__ __forceinline__ void cp_async16_zfill(void *smem, const void *gmem, bool valid) {
-    unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(sa), "l"(gmem), "r"(valid ? 16 : 0)
+// Copies 16 bytes (bytes = 16), or writes 16 zero bytes and reads nothing
+// (bytes = 0); gmem must be a mapped address either way.
+__device__ __forceinline__ void cp_async16_zfill_n(unsigned smem_addr, const void *gmem, int bytes) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_addr), "l"(gmem), "r"(bytes)
                  : "memory");
 }
 template <int N>
@@ -721,12 +720,15 @@ template <int P>
 __global__ void __launch_bounds__(kG3Threads, 2) k_grid3(Grid2Args a) {
     extern __shared__ uint4 smem3[];
     int4 *s_rec = (int4 *)smem3;                                  // [kG3Chunk]
-    ulonglong2 *s_v = (ulonglong2 *)(s_rec + kG3Chunk);           // [kG3Chunk][P]
-    ulonglong2 *ring = s_v + (size_t)kG3Chunk * P;                // [kG3Depth][kG3KS][kG3Threads]
+    float4 *s_v = (float4 *)(s_rec + kG3Chunk);                   // [kG3Chunk][P]
+    ulonglong2 *ring = (ulonglong2 *)(s_v + kG3Chunk * P);        // [kG3Depth][kG3KS][kG3Threads]
     __shared__ int s_item;
+    __shared__ unsigned s_start[kG3Chunk / 32];    // bit k: record k starts a run
+    __shared__ unsigned short s_runend[kG3Chunk];  // first record after k's run
     const int t = threadIdx.x;
+    const int lane = t & 31;
     const int nitems = a.n_items[0];
-    constexpr int KS = kG3KS, D = kG3Depth;
+    constexpr int KS = kG3KS, D = kG3Depth, T = kG3Threads;
     for (;;) {
         __syncthreads();
         if (t == 0) s_item = atomicAdd(a.counter, 1);
@@ -737,35 +739,57 @@ __global__ void __launch_bounds__(kG3Threads, 2) k_grid3(Grid2Args a) {
         const GridJobDesc &J = a.jobs[it.w];
         const ulonglong2 *tab = (const ulonglong2 *)J.table2;
         const int4 *grec = J.wpos;
-        const uint4 *gvis = (const uint4 *)J.wvis4;
+        const float4 *gvis = J.wvis4;
         float *const ggrid = J.grid;
         double *const gdelta = J.dgrid;
         const int gnx = J.nx;
+        const int N = it.y;
         // stage the item's records (gridder layout, 16-byte pieces)
-        for (int k = t; k < it.y; k += kG3Threads) cp_async16(&s_rec[k], &grec[it.x + k]);
-        for (int k = t; k < it.y * P; k += kG3Threads) cp_async16(&s_v[k], &gvis[(size_t)it.x * P + k]);
+        for (int k = t; k < N; k += T) cp_async16(&s_rec[k], &grec[it.x + k]);
+        for (int k = t; k < N * P; k += T) cp_async16(&s_v[k], &gvis[(size_t)it.x * P + k]);
         cp_async_commit();
         cp_async_wait<0>();
+        __syncthreads();
+        // Runs: maximal ranges of records with the same corner and support
+        // (the slots' cells and table offsets within the sub-kernel are fixed
+        // over a run).  s_runend[k] = first record after the run holding k.
+        for (int k0 = 0; k0 < N; k0 += T) {
+            const int k = k0 + t;
+            bool start = false;
+            if (k < N) {
+                const int4 r = s_rec[k];
+                start = (k == 0) || r.x != s_rec[k - 1].x || r.w != s_rec[k - 1].w;
+            }
+            const unsigned m = __ballot_sync(0xFFFFFFFFu, start);
+            if (lane == 0) s_start[k >> 5] = m;
+        }
+        __syncthreads();
+        const int nw = (N + 31) >> 5;
+        for (int k = t; k < N; k += T) {
+            int w = k >> 5;
+            unsigned m = (k & 31) == 31 ? 0u : s_start[w] & (0xFFFFFFFFu << ((k & 31) + 1));
+            while (m == 0 && ++w < nw) m = s_start[w];
+            s_runend[k] = (unsigned short)(m == 0 ? N : (w << 5) + __ffs(m) - 1);
+        }
         __syncthreads();
         const int M = J.M[(unsigned)it.z >> 24];
         const int G = (M + KS - 1) / KS;
         const int U = M * G;
-        const int N = it.y;
-        const int ns = pick_streams(U, N, kG3Threads);
+        const int ns = pick_streams(U, N, T);
         const int njobs = ns * U;
-        for (int job = t; job < njobs; job += kG3Threads) {
+        for (int job = t; job < njobs; job += T) {
             const int stream = job / U;
             const int u = job - stream * U;
             const int g = u / M;
             const int col = u - g * M;
-            const int i0 = (int)(((long)N * stream) / ns);
-            const int i1 = (int)(((long)N * (stream + 1)) / ns);
+            const int i0 = (N * stream) / ns;
+            const int i1 = (N * (stream + 1)) / ns;
             // rows g + j*G that exist: j < nrow
             const int nrow = (M - g + G - 1) / G;
             if (i0 >= i1) continue;
             // Slot geometry depends only on the record's corner and support;
-            // vmul = 0 marks a slot outside the record's box.
-            auto geometry = [&](const int4 &rec, int *cell, int *toff, int *vmul) {
+            // vbytes = 0 marks a slot outside the record's box.
+            auto geometry = [&](const int4 &rec, int *cell, int *toff, int *vbytes) {
                 const int S = rec.w;
                 int sx = col + (rec.y & 0xFFFF);
                 sx -= (sx >= M) ? M : 0;
@@ -777,31 +801,33 @@ __global__ void __launch_bounds__(kG3Threads, 2) k_grid3(Grid2Args a) {
                     const bool ok = xok && (j < nrow) && (sy < S);
                     cell[j] = ok ? rec.x + sy * gnx + sx : -1;
                     toff[j] = ok ? sy * (S + 1) + sx : 0;
-                    vmul[j] = ok ? 1 : 0;
+                    vbytes[j] = ok ? 16 : 0;
                     sy += G;
                     sy -= (sy >= M) ? M : 0;
                 }
             };
-            // look-ahead: the kernel values of record k go to ring slot k % D
-            int keyLx = -1, keyLw = -1, toffL[KS], cellL[KS], vmulL[KS];
+            // Look-ahead: the kernel values of record k go to ring slot k % D;
+            // the geometry is recomputed when k enters a new run (k == pend).
+            int pend = i0, toffL[KS], cellL[KS], vbL[KS];
+            const unsigned ring_s = (unsigned)__cvta_generic_to_shared(ring) + t * 16;
             auto prefetch = [&](int k) {
-                const int4 rec = s_rec[k];
-                if (rec.x != keyLx || rec.w != keyLw) {
-                    geometry(rec, cellL, toffL, vmulL);
-                    keyLx = rec.x;
-                    keyLw = rec.w;
+                if (k == pend) {
+                    geometry(s_rec[k], cellL, toffL, vbL);
+                    const int e = s_runend[k];
+                    pend = e < i1 ? e : i1;
                 }
-                ulonglong2 *dst = ring + (size_t)(k % D) * KS * kG3Threads + t;
+                const int z = s_rec[k].z;
+                const unsigned dst = ring_s + (unsigned)(k & (D - 1)) * (KS * T * 16);
                 // slots outside the box get zeros (toff = 0 keeps the address valid)
 #pragma unroll
-                for (int j = 0; j < KS; j++) cp_async16_zfill(dst + j * kG3Threads, &tab[rec.z + toffL[j]], vmulL[j]);
+                for (int j = 0; j < KS; j++) cp_async16_zfill_n(dst + j * (T * 16), tab + (z + toffL[j]), vbL[j]);
             };
 #pragma unroll
             for (int d = 0; d < D; d++) {
                 if (i0 + d < i1) prefetch(i0 + d);
                 cp_async_commit();
             }
-            int last[KS], keyx = -1, keyw = -1;
+            int last[KS];
             float2 acc[KS][P];
 #pragma unroll
             for (int j = 0; j < KS; j++) {
@@ -812,14 +838,11 @@ __global__ void __launch_bounds__(kG3Threads, 2) k_grid3(Grid2Args a) {
             // Runs of records with the same corner and support: the flushes sit
             // between runs, so the accumulators stay in place inside a run.
             int i = i0;
-            int4 rec = s_rec[i0];
-            for (;;) {
+            while (i < i1) {
                 {
                     // corner or support changed: flush the slots whose cell changes
                     int cellN[KS], toffN[KS], vN[KS];
-                    geometry(rec, cellN, toffN, vN);
-                    keyx = rec.x;
-                    keyw = rec.w;
+                    geometry(s_rec[i], cellN, toffN, vN);
 #pragma unroll
                     for (int j = 0; j < KS; j++) {
                         if (cellN[j] >= 0 && cellN[j] != last[j]) {
@@ -830,20 +853,22 @@ __global__ void __launch_bounds__(kG3Threads, 2) k_grid3(Grid2Args a) {
                         }
                     }
                 }
-                bool more;
-                do {
+                const int e = s_runend[i];
+                const int re = e < i1 ? e : i1;
+                for (; i < re; ++i) {
                     cp_async_wait<D - 1>();     // this thread's copies for record i have landed
                     float2 vp[P], wp[P];
+                    const float4 *vr = s_v + i * P;
 #pragma unroll
                     for (int p = 0; p < P; p++) {
-                        const float4 q = ((const float4 *)s_v)[(size_t)i * P + p];
+                        const float4 q = vr[p];
                         vp[p] = make_float2(q.x, q.y);
                         wp[p] = make_float2(q.z, q.w);
                     }
-                    const float4 *src = (const float4 *)(ring + (size_t)(i % D) * KS * kG3Threads + t);
+                    const float4 *src = (const float4 *)(ring + ((i & (D - 1)) * KS * T + t));
 #pragma unroll
                     for (int j = 0; j < KS; j++) {
-                        const float4 c = src[j * kG3Threads];
+                        const float4 c = src[j * T];
                         const float2 cre = make_float2(c.x, c.y), cim = make_float2(c.z, c.w);
                         // ConvolutionGridder.cu:153-181: to += vis * wt (no conjugate)
 #pragma unroll
@@ -854,11 +879,7 @@ __global__ void __launch_bounds__(kG3Threads, 2) k_grid3(Grid2Args a) {
                     }
                     if (i + D < i1) prefetch(i + D);
                     cp_async_commit();
-                    ++i;
-                    more = i < i1;
-                    if (more) rec = s_rec[i];
-                } while (more && rec.x == keyx && rec.w == keyw);
-                if (!more) break;
+                }
             }
             cp_async_wait<0>();
 #pragma unroll
