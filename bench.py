@@ -261,10 +261,13 @@ def main():
     ap.add_argument("--cube-images", type=int, default=16)
     ap.add_argument("--cube-min-hours", type=float, default=0.25)
     ap.add_argument("--cube-max-hours", type=float, default=2.0)
-    ap.add_argument("--serve-requests", type=int, default=24)
+    ap.add_argument("--serve-requests", type=int, default=500)
     ap.add_argument("--serve-rate", type=float, default=20.0, help="Poisson arrival rate, requests per second")
     ap.add_argument("--serve-min-records", type=float, default=1e5)
-    ap.add_argument("--serve-max-records", type=float, default=2e6)
+    ap.add_argument("--serve-max-records", type=float, default=5e7)
+    ap.add_argument("--serve-sample-requests", type=int, default=40,
+                    help="requests of the shortened stream the default (mid-size) run measures")
+    ap.add_argument("--serve-sample-max-records", type=float, default=5e6)
     ap.add_argument("--serve-slots", type=int, default=4)
     ap.add_argument("--profile-range", action="store_true",
                     help="bracket the timed steps with cudaProfilerStart/Stop (for ncu --profile-from-start off)")
@@ -434,7 +437,12 @@ def main():
         imagers.clear()
         images.clear()
         torch.cuda.empty_cache()
-        serve = run_serve(args, torch, dev)
+        # a shortened stream of the serving configuration (same arrivals, image
+        # sizes and record distribution, fewer and smaller requests)
+        sample = argparse.Namespace(**vars(args))
+        sample.serve_requests = args.serve_sample_requests
+        sample.serve_max_records = args.serve_sample_max_records
+        serve = run_serve(sample, torch, dev)
 
     if rank == 0:
         sup = kern.supports
@@ -534,19 +542,46 @@ def run_e2e(args, torch, dev, uvw_d, chans, imagers, images, samples_per_step, w
 SERVE_WPLANES = {512: 32, 1024: 64, 2048: 96, 4096: 128}
 
 
+def make_request_pool(torch, dev, rng, records):
+    """Host record arrays the serving requests take slices of (views, no
+    copies): the 64-antenna 8 h, 2 s track repeated over channels between 1.3
+    and 1.5 GHz until it holds `records` records (records stay baseline-major
+    within a channel), 4 pol visibilities of a 3-source sky per channel, 10 %
+    of records flagged."""
+    from mtb import synth
+    spec = workload_spec(argparse.Namespace(config="mid", channels=1, hours=8.0))
+    uvw1, _, _ = make_uvw(spec, dev, torch, rng)
+    R1 = uvw1.shape[1]
+    nch = max(1, -(-int(records) // R1))
+    Rp = nch * R1
+    freqs = np.linspace(1.3e9, 1.5e9, nch) if nch > 1 else np.array([1.4e9])
+    uv_max = float(uvw1[:2].abs().max())
+    gen = torch.Generator(device=dev).manual_seed(11)
+    pool = dict(uvw=np.empty((3, Rp), np.float32), freq=np.empty(Rp, np.float32),
+                vis=np.empty((Rp, 4), np.complex64), weights=np.ones((Rp, 4), np.float32),
+                flags=np.empty((Rp, 4), np.int32), uv_max=uv_max)
+    u1 = uvw1.cpu().numpy()
+    srcs = synth.random_sources(3, 4096 * cell_for(dict(spec, nx=4096, f_hi=1.5e9), uv_max, torch), rng,
+                                flux=(0.1, 1.0))
+    for c, f in enumerate(freqs):
+        sl = slice(c * R1, (c + 1) * R1)
+        pool["uvw"][:, sl] = u1
+        pool["freq"][sl] = f / C_LIGHT
+        pool["vis"][sl] = make_vis(uvw1, f, srcs, torch, gen).cpu().numpy()
+        pool["flags"][sl] = (torch.rand(R1, device=dev, generator=gen) < 0.1).int()[:, None].repeat(1, 4).cpu().numpy()
+    return pool
+
+
 def make_requests(args, torch, dev, rng):
     """A stream of imaging requests in the shape of the serving configuration:
     image size uniform over {512, 1024, 2048, 4096}^2, record counts
-    log-uniform in [serve_min_records, serve_max_records] (synthetic 64-antenna
-    tracks: a contiguous slice of an 8 h, 2 s track, so records keep their
-    baseline-major order), 4 pol, point-source skies, 10 % of records flagged,
-    w-planes 32-128 by image size, Poisson arrivals at serve_rate per second."""
-    from mtb import synth
+    log-uniform in [serve_min_records, serve_max_records], each a contiguous
+    slice of the request pool (synthetic 64-antenna tracks, 4 pol, point-source
+    sky, 10 % flagged), w-planes 32-128 by image size, Poisson arrivals at
+    serve_rate per second."""
     spec = workload_spec(argparse.Namespace(config="mid", channels=1, hours=8.0))
-    pool, _, _ = make_uvw(spec, dev, torch, rng)
-    Rp = pool.shape[1]
-    uv_max = float(pool[:2].abs().max())
-    gen = torch.Generator(device=dev).manual_seed(11)
+    pool = make_request_pool(torch, dev, rng, args.serve_max_records)
+    Rp = pool["freq"].size
     reqs = []
     t = 0.0
     for k in range(args.serve_requests):
@@ -554,17 +589,12 @@ def make_requests(args, torch, dev, rng):
         R = int(math.exp(rng.uniform(math.log(args.serve_min_records), math.log(args.serve_max_records))))
         R = min(R, Rp)
         s0 = int(rng.integers(0, Rp - R + 1))
-        f = float(rng.uniform(1.3e9, 1.5e9))
-        sp = dict(spec, nx=n, f_hi=1.5e9)
-        dl = cell_for(sp, uv_max, torch)
-        uvw = pool[:, s0:s0 + R].contiguous()
-        srcs = synth.random_sources(3, n * dl, rng, flux=(0.1, 1.0))
-        vis = make_vis(uvw, f, srcs, torch, gen)
-        flags = (torch.rand(R, device=dev, generator=gen) < 0.1).int()[:, None].repeat(1, 4)
+        dl = cell_for(dict(spec, nx=n, f_hi=1.5e9), pool["uv_max"], torch)
         t += float(rng.exponential(1.0 / args.serve_rate))
-        reqs.append(dict(nx=n, dl=dl, wplanes=SERVE_WPLANES[n], arrival=t, uvw=uvw.cpu().numpy(),
-                         freq=np.full(R, f / C_LIGHT, np.float32), vis=vis.cpu().numpy(),
-                         weights=np.ones((R, 4), np.float32), flags=flags.cpu().numpy()))
+        sl = slice(s0, s0 + R)
+        reqs.append(dict(nx=n, dl=dl, wplanes=SERVE_WPLANES[n], arrival=t, uvw=pool["uvw"][:, sl],
+                         freq=pool["freq"][sl], vis=pool["vis"][sl], weights=pool["weights"][sl],
+                         flags=pool["flags"][sl]))
     return reqs
 
 
@@ -651,11 +681,15 @@ def run_serve(args, torch, dev):
     (b) the plain path, one request at a time in arrival order, each building
     its w-kernels as the reference does per run.  Reports p50/p99 latency
     (arrival to image on the host) and samples/s over the stream for both."""
+    import queue
+    import threading
     from mtb.engine import Engine
     from mtb.imager import WProjectionImager
     rng = np.random.default_rng(5)
+    t_gen = time.perf_counter()
     reqs = make_requests(args, torch, dev, rng)
     torch.cuda.synchronize()
+    t_gen = time.perf_counter() - t_gen
     common = dict(sampling=8, trial_support=67, max_support=65)
     # warm-up (untimed, both paths): the smallest request of every image size
     warm = []
@@ -692,45 +726,58 @@ def run_serve(args, torch, dev):
         lat_plain.append((done - r["arrival"]) * 1e3)
     span_plain = done - reqs[0]["arrival"]
 
-    # (a) engine, real-time arrivals
+    # (a) engine, real-time arrivals; a waiter thread collects results as they
+    # finish (images dropped) while this thread submits
+    def submit(eng, r):
+        return eng.submit(r["nx"], r["nx"], r["dl"], r["dl"], r["wplanes"], 8, r["uvw"], r["freq"], r["vis"],
+                          r["weights"], r["flags"], trial_support=67, max_support=65)
+
     results = []
     with Engine(slots=args.serve_slots) as eng:
-        wt = [eng.submit(r["nx"], r["nx"], r["dl"], r["dl"], r["wplanes"], 8, r["uvw"], r["freq"], r["vis"],
-                         r["weights"], r["flags"], trial_support=67, max_support=65) for r in warm]
-        for t in wt:
+        for t in [submit(eng, r) for r in warm]:
             eng.wait(t)
+        tickets = queue.Queue()
+
+        def waiter():
+            for sub, tk in iter(tickets.get, None):
+                res = eng.wait(tk)
+                results.append((sub, res.status, res.latency_ms, res.kernel_cache_hit,
+                                res.stats["gridded_records"] + res.stats["compressed_records"]))
+
+        th = threading.Thread(target=waiter)
+        th.start()
         t_base = time.perf_counter()
-        tickets = []
         for r in reqs:
             now = time.perf_counter() - t_base
             if r["arrival"] > now:
                 time.sleep(r["arrival"] - now)
             sub = time.perf_counter() - t_base
-            tickets.append((sub, eng.submit(r["nx"], r["nx"], r["dl"], r["dl"], r["wplanes"], 8, r["uvw"], r["freq"],
-                                            r["vis"], r["weights"], r["flags"], trial_support=67,
-                                            max_support=65)))
-        for sub, tk in tickets:
-            res = eng.wait(tk)
-            if res.status != 0:
-                raise RuntimeError("engine request failed: status %d" % res.status)
-            results.append((sub, res))
-    samples_eng = sum((res.stats["gridded_records"] + res.stats["compressed_records"]) * 4 for _, res in results)
-    lat_eng = [res.latency_ms for _, res in results]
-    end = max(sub + res.latency_ms * 1e-3 for sub, res in results)
-    span_eng = end - results[0][0]
-    hits = sum(res.kernel_cache_hit for _, res in results)
+            tickets.put((sub, submit(eng, r)))
+        tickets.put(None)
+        th.join()
+    bad = [st for _, st, _, _, _ in results if st != 0]
+    if bad:
+        raise RuntimeError("engine request failed: status %d" % bad[0])
+    samples_eng = sum(4 * n for *_, n in results)
+    lat_eng = [lat for _, _, lat, _, _ in results]
+    end = max(sub + lat * 1e-3 for sub, _, lat, _, _ in results)
+    span_eng = end - min(sub for sub, *_ in results)
+    hits = sum(h for _, _, _, h, _ in results)
     recs = [r["freq"].size for r in reqs]
     return {
         "requests": len(reqs), "arrival_rate_per_s": args.serve_rate, "slots": args.serve_slots,
         "image_sizes": [512, 1024, 2048, 4096],
         "warm_up": "one untimed request per image size through each path (engine: w-kernel cache resident, "
                    "slot buffers grown; plain path: allocator and FFT plans warm, w-kernels rebuilt per request)",
-        "records": {"min": int(min(recs)), "max": int(max(recs)), "total": int(sum(recs))},
+        "records": {"min": int(min(recs)), "max": int(max(recs)), "total": int(sum(recs)),
+                    "range": [args.serve_min_records, args.serve_max_records]},
         "engine": {"samples_per_s": samples_eng / span_eng, "p50_ms": float(np.percentile(lat_eng, 50)),
                    "p99_ms": float(np.percentile(lat_eng, 99)), "makespan_s": span_eng, "kernel_cache_hits": hits},
         "plain": {"samples_per_s": samples_plain / span_plain, "p50_ms": float(np.percentile(lat_plain, 50)),
-                  "p99_ms": float(np.percentile(lat_plain, 99)), "makespan_s": span_plain},
+                  "p99_ms": float(np.percentile(lat_plain, 99)), "makespan_s": span_plain,
+                  "mean_service_ms": float(np.mean(service)) * 1e3},
         "speedup_samples_per_s": (samples_eng / span_eng) / (samples_plain / span_plain),
+        "datagen_s": t_gen,
     }
 
 

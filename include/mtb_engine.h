@@ -13,7 +13,8 @@
  *   - w-kernel tables are cached by geometry (LRU within a byte budget) and
  *     shared by every request of that geometry;
  *   - a request's records are streamed in chunks from host memory through
- *     pinned, double-buffered staging, each chunk gridded by mtb_grid.
+ *     pinned, double-buffered staging, each chunk gridded by mtb_grid; host
+ *     copies to and from pinned memory are split over a pool of threads.
  * The image of a request is the same whether it runs alone or in a mix (to
  * the rounding of the FP32 reductions, or exactly with exact_delta).
  */
@@ -33,6 +34,8 @@ typedef struct mtb_engine_config {
     size_t hbm_budget_bytes;      /* device memory for admitted requests; 0: 70% of free   */
     size_t kernel_cache_bytes;    /* w-kernel tables kept resident; 0: 4 GiB               */
     int chunk_records;            /* records per mtb_grid call; 0: 4,194,304               */
+    int host_threads;             /* threads copying between the caller's host arrays and
+                                     pinned memory (shared by the slots); 0: min(8, cores/2) */
 } mtb_engine_config;
 
 typedef struct mtb_image_request {
@@ -50,6 +53,8 @@ typedef struct mtb_image_request {
     float *image;                 /* host output [P][ny][nx]                               */
     int exact_delta;              /* compensated gridding with an FP64 per-call delta grid
                                      (order-independent result); see mtb_grid_params       */
+    long long uvw_row_stride;     /* floats between the u, v and w rows of uvw (a slice of
+                                     a longer uvw array); 0: nrecords                      */
 } mtb_image_request;
 
 typedef struct mtb_image_result {

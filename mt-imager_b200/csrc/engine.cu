@@ -9,6 +9,13 @@
 // through pinned double-buffered staging in chunks of chunk_records, grids
 // every chunk with mtb_grid, finalises with mtb_finalize and copies the image
 // to the request's host buffer.
+//
+// Host copies between the caller's (pageable) arrays and pinned memory run on
+// a pool of host threads: one thread copies a few GB/s, more so into pages
+// touched for the first time, while DMA from pinned memory runs at tens of
+// GB/s.  Inputs are copied array by array, each array's H2D issued as soon as
+// it is staged; the image comes back in pieces through two pinned buffers,
+// each piece copied out while the next one is in flight.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -40,6 +47,78 @@ double ms_between(Clock::time_point a, Clock::time_point b) {
 
 // Bytes of one record's inputs for P polarisations (uvw, nu/c, vis, weights, flags).
 size_t record_bytes(int P) { return 3 * 4 + 4 + (size_t)P * (8 + 4 + 4); }
+
+// Host threads that split large memcpys.  copy() returns when every piece is
+// done; the calling thread copies one piece itself.
+class CopyPool {
+public:
+    explicit CopyPool(int threads) {
+        for (int i = 0; i < threads; i++) th_.emplace_back([this] { loop(); });
+    }
+    ~CopyPool() {
+        {
+            std::lock_guard<std::mutex> lk(m_);
+            stop_ = true;
+        }
+        cv_.notify_all();
+        for (auto &t : th_) t.join();
+    }
+    void copy(void *dst, const void *src, size_t bytes) {
+        const size_t min_piece = (size_t)1 << 20;
+        size_t pieces = std::min((size_t)th_.size() + 1, (bytes + min_piece - 1) / min_piece);
+        if (pieces <= 1) {
+            std::memcpy(dst, src, bytes);
+            return;
+        }
+        const size_t step = (bytes / pieces + 63) & ~(size_t)63;
+        Batch b;
+        b.left = 0;
+        {
+            std::lock_guard<std::mutex> lk(m_);
+            for (size_t off = step; off < bytes; off += step) {
+                tasks_.push_back(Task{(char *)dst + off, (const char *)src + off, std::min(step, bytes - off), &b});
+                b.left++;
+            }
+        }
+        cv_.notify_all();
+        std::memcpy(dst, src, std::min(step, bytes));
+        std::unique_lock<std::mutex> lk(b.m);
+        b.cv.wait(lk, [&] { return b.left == 0; });
+    }
+
+private:
+    struct Batch {
+        std::mutex m;
+        std::condition_variable cv;
+        int left;
+    };
+    struct Task {
+        char *dst;
+        const char *src;
+        size_t n;
+        Batch *b;
+    };
+    void loop() {
+        for (;;) {
+            Task t;
+            {
+                std::unique_lock<std::mutex> lk(m_);
+                cv_.wait(lk, [&] { return stop_ || !tasks_.empty(); });
+                if (tasks_.empty()) return;
+                t = tasks_.front();
+                tasks_.pop_front();
+            }
+            std::memcpy(t.dst, t.src, t.n);
+            std::lock_guard<std::mutex> lk(t.b->m);
+            if (--t.b->left == 0) t.b->cv.notify_all();
+        }
+    }
+    std::vector<std::thread> th_;
+    std::mutex m_;
+    std::condition_variable cv_;
+    std::deque<Task> tasks_;
+    bool stop_ = false;
+};
 
 struct Job {
     long long ticket = 0;
@@ -126,11 +205,24 @@ struct mtb_engine {
     long long next_ticket = 1;
     bool stop = false;
     std::unique_ptr<mtb::KernelCache> cache;
+    std::unique_ptr<mtb::CopyPool> copier;
     std::vector<std::thread> workers;
 
+    // per-slot resources of a worker thread
+    struct Slot {
+        cudaStream_t st = nullptr;
+        unsigned char *pinned[2] = {nullptr, nullptr};   // input staging (chunk)
+        unsigned char *dstage[2] = {nullptr, nullptr};
+        cudaEvent_t ev[2] = {nullptr, nullptr};
+        float *out[2] = {nullptr, nullptr};              // image pieces on the way back
+        cudaEvent_t out_ev[2] = {nullptr, nullptr};
+        mtb::ImagerBuffers bufs;
+        mtb::DeviceArray<float> img;
+    };
+    static constexpr size_t kOutPiece = (size_t)8 << 20; // floats per image piece (32 MiB)
+
     void worker(int slot);
-    void run(mtb::Job *j, cudaStream_t st, unsigned char *const pinned[2], unsigned char *const dstage[2],
-             cudaEvent_t const ev[2], mtb::ImagerBuffers &bufs, mtb::DeviceArray<float> &img);
+    void run(mtb::Job *j, Slot &sl);
 };
 
 namespace {
@@ -178,6 +270,7 @@ int check_request(const mtb_image_request *r) {
     if (!r->image) return MTB_ERR_NULL;
     if (r->nrecords > 0 && (!r->uvw || !r->freq || !r->vis || !r->weights || !r->flags)) return MTB_ERR_NULL;
     if (r->pol_type != MTB_POL_LINEAR && r->pol_type != MTB_POL_CIRCULAR) return MTB_ERR_BAD_PARAM;
+    if (r->uvw_row_stride != 0 && r->uvw_row_stride < r->nrecords) return MTB_ERR_BAD_SHAPE;
     return MTB_OK;
 }
 
@@ -186,20 +279,16 @@ int check_request(const mtb_image_request *r) {
 void mtb_engine::worker(int slot) {
     (void)slot;
     cudaSetDevice(device);
-    cudaStream_t st = nullptr;
-    unsigned char *pinned[2] = {nullptr, nullptr}, *dstage[2] = {nullptr, nullptr};
-    cudaEvent_t ev[2] = {nullptr, nullptr};
     const size_t sbytes = (size_t)cfg.chunk_records * mtb::record_bytes(4);
-    bool ok = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) == cudaSuccess;
+    Slot sl;
+    bool ok = cudaStreamCreateWithFlags(&sl.st, cudaStreamNonBlocking) == cudaSuccess;
     for (int b = 0; b < 2 && ok; b++) {
-        ok = cudaMallocHost((void **)&pinned[b], sbytes) == cudaSuccess &&
-             cudaMalloc((void **)&dstage[b], sbytes) == cudaSuccess &&
-             cudaEventCreateWithFlags(&ev[b], cudaEventDisableTiming) == cudaSuccess;
+        ok = cudaMallocHost((void **)&sl.pinned[b], sbytes) == cudaSuccess &&
+             cudaMalloc((void **)&sl.dstage[b], sbytes) == cudaSuccess &&
+             cudaEventCreateWithFlags(&sl.ev[b], cudaEventDisableTiming) == cudaSuccess &&
+             cudaMallocHost((void **)&sl.out[b], kOutPiece * sizeof(float)) == cudaSuccess &&
+             cudaEventCreateWithFlags(&sl.out_ev[b], cudaEventDisableTiming) == cudaSuccess;
     }
-    {
-    // device buffers of this slot, reused (grow-only) by every request it runs
-    mtb::ImagerBuffers bufs;
-    mtb::DeviceArray<float> img;
     for (;;) {
         mtb::Job *j = nullptr;
         {
@@ -212,7 +301,7 @@ void mtb_engine::worker(int slot) {
             j->t_admit = mtb::Clock::now();
         }
         if (ok) {
-            run(j, st, pinned, dstage, ev, bufs, img);
+            run(j, sl);
         } else {
             j->res.status = MTB_ERR_CUDA;
         }
@@ -227,58 +316,74 @@ void mtb_engine::worker(int slot) {
         }
         cv.notify_all();
     }
-    if (st) cudaStreamSynchronize(st);
-    }   // slot buffers released on the slot's stream
+    if (sl.st) cudaStreamSynchronize(sl.st);
+    // slot buffers are released on the slot's stream before it is destroyed
+    sl.bufs = mtb::ImagerBuffers();
+    sl.img = mtb::DeviceArray<float>();
+    if (sl.st) cudaStreamSynchronize(sl.st);
     for (int b = 0; b < 2; b++) {
-        if (pinned[b]) cudaFreeHost(pinned[b]);
-        if (dstage[b]) cudaFree(dstage[b]);
-        if (ev[b]) cudaEventDestroy(ev[b]);
+        if (sl.pinned[b]) cudaFreeHost(sl.pinned[b]);
+        if (sl.dstage[b]) cudaFree(sl.dstage[b]);
+        if (sl.ev[b]) cudaEventDestroy(sl.ev[b]);
+        if (sl.out[b]) cudaFreeHost(sl.out[b]);
+        if (sl.out_ev[b]) cudaEventDestroy(sl.out_ev[b]);
     }
-    if (st) cudaStreamDestroy(st);
+    if (sl.st) cudaStreamDestroy(sl.st);
 }
 
-void mtb_engine::run(mtb::Job *j, cudaStream_t st, unsigned char *const pinned[2], unsigned char *const dstage[2],
-                     cudaEvent_t const ev[2], mtb::ImagerBuffers &bufs, mtb::DeviceArray<float> &img) {
+void mtb_engine::run(mtb::Job *j, Slot &sl) {
     const mtb_image_request &r = j->req;
     const int P = r.npol, R = r.nrecords;
+    cudaStream_t st = sl.st;
     try {
         bool hit = false;
         std::shared_ptr<mtb::KernelTable> k = cache->get(r.geometry, st, &hit);
         j->res.kernel_cache_hit = hit ? 1 : 0;
-        mtb::Imager im(k, P, r.pol_type, r.compensated != 0, st, &bufs, r.exact_delta != 0);
+        mtb::Imager im(k, P, r.pol_type, r.compensated != 0, st, &sl.bufs, r.exact_delta != 0);
         const int chunk = cfg.chunk_records;
         int b = 0;
         for (int c0 = 0; c0 < R; c0 += chunk, b ^= 1) {
             const int n = std::min(chunk, R - c0);
             // staging b is free once the copy issued from it two chunks ago is done
-            mtb::cuda_check(cudaEventSynchronize(ev[b]), "staging");
-            unsigned char *h = pinned[b];
-            float *h_uvw = (float *)h;
-            float *h_freq = h_uvw + 3 * (size_t)n;
-            float2 *h_vis = (float2 *)(h_freq + n);
-            float *h_wt = (float *)(h_vis + (size_t)n * P);
-            int *h_fl = (int *)(h_wt + (size_t)n * P);
-            for (int row = 0; row < 3; row++)
-                std::memcpy(h_uvw + (size_t)row * n, r.uvw + (size_t)row * R + c0, (size_t)n * 4);
-            std::memcpy(h_freq, r.freq + c0, (size_t)n * 4);
-            std::memcpy(h_vis, (const float2 *)r.vis + (size_t)c0 * P, (size_t)n * P * 8);
-            std::memcpy(h_wt, r.weights + (size_t)c0 * P, (size_t)n * P * 4);
-            std::memcpy(h_fl, r.flags + (size_t)c0 * P, (size_t)n * P * 4);
-            const size_t bytes = (size_t)n * mtb::record_bytes(P);
-            unsigned char *d = dstage[b];
-            mtb::cuda_check(cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, st), "H2D");
-            mtb::cuda_check(cudaEventRecord(ev[b], st), "event");
+            mtb::cuda_check(cudaEventSynchronize(sl.ev[b]), "staging");
+            unsigned char *h = sl.pinned[b], *d = sl.dstage[b];
             const size_t off_freq = 12 * (size_t)n, off_vis = off_freq + 4 * (size_t)n;
             const size_t off_wt = off_vis + 8 * (size_t)n * P, off_fl = off_wt + 4 * (size_t)n * P;
+            // one array (or uvw row) at a time: its H2D runs while the next is staged
+            auto stage = [&](size_t off, const void *src, size_t bytes) {
+                copier->copy(h + off, src, bytes);
+                mtb::cuda_check(cudaMemcpyAsync(d + off, h + off, bytes, cudaMemcpyHostToDevice, st), "H2D");
+            };
+            const size_t us = r.uvw_row_stride ? (size_t)r.uvw_row_stride : (size_t)R;
+            for (int row = 0; row < 3; row++) stage((size_t)row * n * 4, r.uvw + row * us + c0, (size_t)n * 4);
+            stage(off_freq, r.freq + c0, (size_t)n * 4);
+            stage(off_vis, (const float2 *)r.vis + (size_t)c0 * P, (size_t)n * P * 8);
+            stage(off_wt, r.weights + (size_t)c0 * P, (size_t)n * P * 4);
+            stage(off_fl, r.flags + (size_t)c0 * P, (size_t)n * P * 4);
+            mtb::cuda_check(cudaEventRecord(sl.ev[b], st), "event");
             im.grid((const float *)d, (const float *)(d + off_freq), d + off_vis, (const float *)(d + off_wt),
                     (const int *)(d + off_fl), n);
         }
         if (R == 0) im.grid(nullptr, nullptr, nullptr, nullptr, nullptr, 0);
         const size_t npix = (size_t)P * r.geometry.nx * r.geometry.ny;
-        mtb::ImagerBuffers::ensure(img, npix, st);
-        im.finalize(img.data());
-        mtb::cuda_check(cudaMemcpyAsync(r.image, img.data(), npix * sizeof(float), cudaMemcpyDeviceToHost, st),
-                        "D2H");
+        mtb::ImagerBuffers::ensure(sl.img, npix, st);
+        im.finalize(sl.img.data());
+        // image pieces: D2H of piece q + 2 goes out once piece q has left pinned buffer q % 2
+        const size_t npiece = (npix + kOutPiece - 1) / kOutPiece;
+        auto d2h = [&](size_t q) {
+            const size_t o = q * kOutPiece, n = std::min(kOutPiece, npix - o);
+            mtb::cuda_check(cudaMemcpyAsync(sl.out[q & 1], sl.img.data() + o, n * sizeof(float),
+                                            cudaMemcpyDeviceToHost, st),
+                            "D2H");
+            mtb::cuda_check(cudaEventRecord(sl.out_ev[q & 1], st), "event");
+        };
+        for (size_t q = 0; q < npiece && q < 2; q++) d2h(q);
+        for (size_t q = 0; q < npiece; q++) {
+            mtb::cuda_check(cudaEventSynchronize(sl.out_ev[q & 1]), "D2H");
+            const size_t o = q * kOutPiece, n = std::min(kOutPiece, npix - o);
+            copier->copy(r.image + o, sl.out[q & 1], n * sizeof(float));
+            if (q + 2 < npiece) d2h(q + 2);
+        }
         j->res.stats = im.stats();   // synchronises the stream
         j->res.status = MTB_OK;
     } catch (const mtb::Error &e) {
@@ -315,6 +420,11 @@ extern "C" int mtb_engine_create(const mtb_engine_config *cfg, mtb_engine **engi
         cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
     }
     e->cache.reset(new mtb::KernelCache(e->cfg.kernel_cache_bytes));
+    if (e->cfg.host_threads <= 0) {
+        const int hw = (int)std::thread::hardware_concurrency();
+        e->cfg.host_threads = std::max(1, std::min(8, hw > 0 ? hw / 2 : 1));
+    }
+    e->copier.reset(new mtb::CopyPool(e->cfg.host_threads - 1));
     for (int s = 0; s < e->cfg.slots; s++) e->workers.emplace_back(&mtb_engine::worker, e.get(), s);
     *engine = e.release();
     return MTB_OK;
@@ -377,6 +487,7 @@ extern "C" int mtb_engine_destroy(mtb_engine *engine) {
     for (auto &t : engine->workers) t.join();
     for (auto &kv : engine->jobs) delete kv.second;
     engine->cache.reset();
+    engine->copier.reset();
     delete engine;
     return MTB_OK;
 }

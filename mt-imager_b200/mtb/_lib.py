@@ -87,14 +87,16 @@ class FitsHeader(ctypes.Structure):
 
 class EngineConfig(ctypes.Structure):
     _fields_ = [("slots", ctypes.c_int), ("hbm_budget_bytes", ctypes.c_size_t),
-                ("kernel_cache_bytes", ctypes.c_size_t), ("chunk_records", ctypes.c_int)]
+                ("kernel_cache_bytes", ctypes.c_size_t), ("chunk_records", ctypes.c_int),
+                ("host_threads", ctypes.c_int)]
 
 
 class ImageRequest(ctypes.Structure):
     _fields_ = [("geometry", WKernelParams), ("npol", ctypes.c_int), ("pol_type", ctypes.c_int),
                 ("compensated", ctypes.c_int), ("nrecords", ctypes.c_int), ("uvw", ctypes.c_void_p),
                 ("freq", ctypes.c_void_p), ("vis", ctypes.c_void_p), ("weights", ctypes.c_void_p),
-                ("flags", ctypes.c_void_p), ("image", ctypes.c_void_p), ("exact_delta", ctypes.c_int)]
+                ("flags", ctypes.c_void_p), ("image", ctypes.c_void_p), ("exact_delta", ctypes.c_int),
+                ("uvw_row_stride", ctypes.c_longlong)]
 
 
 class ImageResult(ctypes.Structure):

@@ -32,9 +32,9 @@ def _c(a, dtype):
 
 
 class Engine:
-    def __init__(self, slots=4, hbm_budget_bytes=0, kernel_cache_bytes=0, chunk_records=0):
+    def __init__(self, slots=4, hbm_budget_bytes=0, kernel_cache_bytes=0, chunk_records=0, host_threads=0):
         self.lib = L.load()
-        cfg = L.EngineConfig(slots, hbm_budget_bytes, kernel_cache_bytes, chunk_records)
+        cfg = L.EngineConfig(slots, hbm_budget_bytes, kernel_cache_bytes, chunk_records, host_threads)
         self._h = ctypes.c_void_p()
         L.check(self.lib.mtb_engine_create(ctypes.byref(cfg), ctypes.byref(self._h)), "mtb_engine_create")
         self._pending = {}
@@ -42,7 +42,14 @@ class Engine:
     def _request(self, nx, ny, l_increment, m_increment, wplanes, sampling, uvw, freq, vis, weights, flags,
                  trial_support=0, max_support=0, w_max=0.0, pol_type=L.MTB_POL_LINEAR, compensated=True,
                  exact_delta=False):
-        uvw = _c(uvw, np.float32)
+        uvw = np.asarray(uvw)
+        # a [3][R] slice of a longer float32 uvw array is passed as it is, with its row stride
+        row_stride = 0
+        if (uvw.dtype == np.float32 and uvw.ndim == 2 and uvw.strides[1] == 4 and uvw.strides[0] % 4 == 0
+                and uvw.strides[0] >= 4 * uvw.shape[1]):
+            row_stride = uvw.strides[0] // 4
+        else:
+            uvw = _c(uvw, np.float32)
         freq = _c(freq, np.float32)
         vis = _c(vis, np.complex64)
         weights = _c(weights, np.float32)
@@ -56,7 +63,7 @@ class Engine:
                             max_support, float(w_max))
         ptr = lambda a: a.ctypes.data_as(ctypes.c_void_p)  # noqa: E731
         req = L.ImageRequest(g, P, pol_type, int(bool(compensated)), R, ptr(uvw), ptr(freq), ptr(vis),
-                             ptr(weights), ptr(flags), ptr(image), int(bool(exact_delta)))
+                             ptr(weights), ptr(flags), ptr(image), int(bool(exact_delta)), row_stride)
         return req, (uvw, freq, vis, weights, flags, image)
 
     def request_bytes(self, *args, **kw) -> int:
