@@ -258,9 +258,10 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-serve", action="store_true", help="skip the request-stream measurement")
-    ap.add_argument("--cube-images", type=int, default=16)
-    ap.add_argument("--cube-min-hours", type=float, default=0.25)
-    ap.add_argument("--cube-max-hours", type=float, default=2.0)
+    ap.add_argument("--cube-images", type=int, default=64)
+    ap.add_argument("--cube-min-hours", type=float, default=1.0)
+    ap.add_argument("--cube-max-hours", type=float, default=8.0)
+    ap.add_argument("--cube-chunk", type=float, default=1 << 22, help="records per image per batched call")
     ap.add_argument("--serve-requests", type=int, default=500)
     ap.add_argument("--serve-rate", type=float, default=20.0, help="Poisson arrival rate, requests per second")
     ap.add_argument("--serve-min-records", type=float, default=1e5)
@@ -602,49 +603,65 @@ def run_cube(args, torch, dev):
     """Batched cubes: independent channel images with uneven record counts
     (64-antenna tracks of U(cube_min_hours, cube_max_hours) at 2 s, flagging
     U(0, 60 %)), image size 1024^2 or 2048^2 per image, 64 w-planes, supports
-    up to 49.  Gridded (a) image by image with mtb_grid, (b) all images with
-    one mtb_grid_batch launch, (c) that batch replayed from a captured CUDA
-    graph.  Inputs resident in HBM; samples/s of the gridding of every image."""
-    from mtb.imager import WProjectionImager, build_wkernels, grid_batch, wkernel_params
+    up to 49, inputs resident in HBM.  Every image's records are gridded in
+    chunks of cube_chunk records: (a) image by image with mtb_grid, (b) chunk
+    by chunk for all images at once with mtb_grid_batch (one persistent
+    gridder launch per chunk index), with default knobs and then with the
+    knobs the autotuner picks on the cube's first chunks, (c) the tuned chunk
+    sequence replayed from one captured CUDA graph.  Samples/s of the gridding
+    of every image."""
+    from mtb.imager import WProjectionImager, autotune, build_wkernels, grid_batch, wkernel_params
     rng = np.random.default_rng(4)
     spec = workload_spec(argparse.Namespace(config="mid", channels=1, hours=8.0))
     pool, nbl, nt = make_uvw(spec, dev, torch, rng)
     uv_max = float(pool[:2].abs().max())
     gen = torch.Generator(device=dev).manual_seed(13)
+    chunk = int(args.cube_chunk)
+    ones = torch.ones((min(chunk, nbl * nt), 4), dtype=torch.float32, device=dev)   # shared weights
     kern = {}
-    entries = []
+    images = []      # (imager, [chunk arrays])
     for k in range(args.cube_images):
         n = int(rng.choice([1024, 2048]))
         hours = float(rng.uniform(args.cube_min_hours, args.cube_max_hours))
-        ntk = max(1, int(hours * 1800))
+        ntk = max(1, min(nt, int(hours * 1800)))
         # the first ntk integrations of every baseline (records stay baseline-major)
-        sel = pool.reshape(3, nbl, nt)[:, :, :ntk].reshape(3, -1).contiguous()
+        sel = pool.reshape(3, nbl, nt)[:, :, :ntk].reshape(3, -1)
         R = sel.shape[1]
         dl = cell_for(dict(spec, nx=n, max_support=49), uv_max, torch)
         if n not in kern:
             kern[n] = build_wkernels(wkernel_params(n, n, dl, dl, 64, 8, 51, 49), dev)
         f = float(rng.uniform(1.3e9, 1.5e9))
         srcs = sources_for(dict(spec, nsrc=20), n * dl, rng)
-        vis = make_vis(sel, f, srcs, torch, gen)
         frac = float(rng.uniform(0.0, 0.6))
-        flags = (torch.rand(R, device=dev, generator=gen) < frac).int()[:, None].repeat(1, 4).contiguous()
         im = WProjectionImager(n, n, dl, wplanes=64, sampling=8, trial_support=51, max_support=49, kernels=kern[n],
                                device=dev)
-        entries.append((im, sel, torch.full((R,), f / C_LIGHT, dtype=torch.float32, device=dev), vis,
-                        torch.ones((R, 4), dtype=torch.float32, device=dev), flags))
+        chunks = []
+        for a0 in range(0, R, chunk):
+            b0 = min(R, a0 + chunk)
+            u = sel[:, a0:b0].contiguous()
+            chunks.append((u, torch.full((b0 - a0,), f / C_LIGHT, dtype=torch.float32, device=dev),
+                           make_vis(u, f, srcs, torch, gen), ones[:b0 - a0],
+                           (torch.rand(b0 - a0, device=dev, generator=gen) < frac).int()[:, None].repeat(1, 4)
+                           .contiguous()))
+        images.append((im, chunks))
+    del pool
     torch.cuda.synchronize()
+    nchunks = max(len(c) for _, c in images)
 
     def single():
-        for im, *arrs in entries:
+        for im, chunks in images:
             im.reset()
-            im.grid_device(*arrs)
+            for arrs in chunks:
+                im.grid_device(*arrs)
+            im._ws = None    # one workspace at a time (the allocator reuses it)
 
     ws = [None]
 
     def batched():
-        for im, *_ in entries:
+        for im, _ in images:
             im.reset()
-        ws[0] = grid_batch(entries, workspace=ws[0])
+        for c in range(nchunks):
+            ws[0] = grid_batch([(im, *chunks[c]) for im, chunks in images if c < len(chunks)], workspace=ws[0])
 
     def timed(fn, reps=3):
         for _ in range(2):
@@ -659,19 +676,34 @@ def run_cube(args, torch, dev):
         return a.elapsed_time(b) / reps
 
     ms_single = timed(single)
-    stats = [im.statistics() for im, *_ in entries]
+    stats = [im.statistics() for im, _ in images]
     samples = sum((s["gridded_records"] + s["compressed_records"]) * 4 for s in stats)
+    torch.cuda.empty_cache()
+    ms_default = timed(batched)
+    # autotune the batch's knobs on the cube's first chunks, then time the tuned batch
+    for im, _ in images:
+        im.reset()
+    ws[0] = None              # the autotuner sizes its own (largest-candidate) workspace
+    torch.cuda.empty_cache()
+    t0 = time.perf_counter()
+    best, cands, ws[0] = autotune([(im, *chunks[0]) for im, chunks in images])
+    tune_s = time.perf_counter() - t0
     ms_batch = timed(batched)
     graph = torch.cuda.CUDAGraph()
     with torch.cuda.graph(graph):
         batched()
     ms_graph = timed(graph.replay)
     del graph
-    recs = [arrs[1].numel() for _, *arrs in entries]
-    return {"images": len(entries), "records": {"min": int(min(recs)), "max": int(max(recs)), "total": int(sum(recs))},
-            "image_sizes": sorted({im.nx for im, *_ in entries}), "samples_per_image_set": int(samples),
+    recs = [sum(a[1].numel() for a in chunks) for _, chunks in images]
+    return {"images": len(images), "records": {"min": int(min(recs)), "max": int(max(recs)), "total": int(sum(recs))},
+            "image_sizes": sorted({im.nx for im, _ in images}), "chunk_records": chunk, "chunk_calls": nchunks,
+            "samples_per_image_set": int(samples),
             "per_image_launches": {"ms": ms_single, "samples_per_s": samples / (ms_single * 1e-3)},
-            "one_batched_launch": {"ms": ms_batch, "samples_per_s": samples / (ms_batch * 1e-3)},
+            "one_batched_launch_default_knobs": {"ms": ms_default, "samples_per_s": samples / (ms_default * 1e-3)},
+            "autotune": {"best": best, "seconds": tune_s,
+                         "fastest_candidates": sorted(cands, key=lambda c: c["ms"])[:4]},
+            "one_batched_launch": {"ms": ms_batch, "samples_per_s": samples / (ms_batch * 1e-3),
+                                   "knobs": "autotuned"},
             "batched_cuda_graph": {"ms": ms_graph, "samples_per_s": samples / (ms_graph * 1e-3)}}
 
 

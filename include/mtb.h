@@ -153,6 +153,8 @@ typedef struct mtb_grid_params {
                                   flushes accumulate in an FP32 delta grid merged into
                                   (grid, grid_lo) with TwoSum; 1 they accumulate in FP64
                                   (order-independent, about half the grid error, slower)   */
+    int gridder_threads;       /* 0: 256; threads of a gridder block, which grids one work
+                                  item at a time (256 or 512)                              */
 } mtb_grid_params;
 
 typedef struct mtb_grid_stats {
@@ -202,6 +204,29 @@ typedef struct mtb_grid_job {
 
 /* Workspace for mtb_grid_batch over these jobs. */
 int mtb_grid_batch_workspace_size(const mtb_grid_job *jobs, int njobs, size_t *bytes);
+
+/* Gridder knobs the autotuner chooses among (fields of mtb_grid_params). */
+typedef struct mtb_grid_tuning {
+    int tile;             /* bin tile edge                                            */
+    int support_bucket;   /* odd supports per bin bucket                              */
+    int max_chunk;        /* records per work item                                    */
+    int gridder_threads;  /* threads per gridder block (one work item at a time)      */
+    float ms;             /* measured time of one mtb_grid_batch call with these knobs */
+} mtb_grid_tuning;
+
+/* Autotuner.  No counterpart in the reference, whose gridder launch shapes are
+ * fixed.  Grids the jobs (as mtb_grid_batch) once with every candidate of
+ * tile {16, 32, 64} x support_bucket {1, 2} x max_chunk {256, 512} x
+ * gridder_threads {256, 512}, times each call with CUDA events on `stream`
+ * (after one untimed call), and writes the fastest to *best and to every
+ * job's params.  Every job must start a fresh image (initialize_output = 1):
+ * the grids, normalisers and statistics hold the result of a call with the
+ * chosen knobs when it returns.  Synchronises `stream` after every call.
+ * `candidates` (may be NULL) receives all 24 timings.  Workspace:
+ * mtb_grid_autotune_workspace_size. */
+int mtb_grid_autotune_workspace_size(const mtb_grid_job *jobs, int njobs, size_t *bytes);
+int mtb_grid_autotune(mtb_grid_job *jobs, int njobs, void *d_workspace, size_t workspace_bytes,
+                      mtb_stream_t stream, mtb_grid_tuning *best, mtb_grid_tuning *candidates);
 
 /* Grids one chunk of records into each of up to 64 images -- channels of a cube
  * or unrelated images of any geometry -- with ONE persistent gridder launch fed

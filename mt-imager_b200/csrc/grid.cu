@@ -523,18 +523,18 @@ __global__ void __launch_bounds__(KMAX >= 8 ? 576 : 1024) k_grid(GridArgs a) {
 }
 
 // ------------------------------------------------------- direct gridder --
-// One persistent launch for every support bucket.  A block of kG2Threads
-// threads takes a work item (up to max_chunk records of one (support bucket,
-// tile) bin, original record order) and walks the M x M support box in passes
-// of kG2Threads*KS slots: slot q -> (a, b) = (q % M, q / M).  For a record with
-// corner (cx, cy) the slot touches cell (cx + sx, cy + sy), sx = (a - cx) mod M,
-// sy = (b - cy) mod M (Romein's assignment: a slot keeps its cell while the
-// record moves less than a cell, and no two slots of a pass share a cell).
-// Each slot accumulates V * C for all polarisations in registers with packed
-// f32x2 FMAs and merges into the grid (vector reductions) only when its cell
-// changes and at the end of a pass.
+// One persistent launch for every support bucket.  A block takes a work item
+// (up to max_chunk records of one (support bucket, tile) bin, original record
+// order) and splits it into (support-box unit, record stream) jobs over its
+// threads.  A unit is one column of the M x M support box and every G-th row
+// of it; for a record with corner (cx, cy) a slot (a, b) touches cell
+// (cx + sx, cy + sy), sx = (a - cx) mod M, sy = (b - cy) mod M (Romein's
+// assignment: a slot keeps its cell while the record moves less than a cell,
+// and no two slots of a unit share a cell).  Each slot accumulates V * C for
+// all polarisations in registers with packed f32x2 FMAs and merges into the
+// grid (vector reductions) only when its cell changes and at the end of a job.
 static const int kG2Threads = 256;
-static const int kG3Threads = kG2Threads;   // block size
+static const int kG3Threads = kG2Threads;   // default block size (threads per work item)
 static const int kG3Chunk = 512;            // records of one work item, staged at once
 static const int kG3Depth = 4;              // records of kernel values fetched ahead
 static const int kG3KS = 4;                 // support-box slots per thread
@@ -716,19 +716,19 @@ __global__ void k_expand_table(const float2 *__restrict__ t, float4 *__restrict_
 // per thread with commit/wait groups, so no block barrier per record).  A slot
 // outside a record's support box gets zeros in its ring entry, which keeps the
 // accumulation loop free of per-slot branches.
-template <int P>
-__global__ void __launch_bounds__(kG3Threads, 2) k_grid3(Grid2Args a) {
+template <int P, int T>
+__global__ void __launch_bounds__(T, 512 / T) k_grid3(Grid2Args a) {
     extern __shared__ uint4 smem3[];
     int4 *s_rec = (int4 *)smem3;                                  // [kG3Chunk]
     float4 *s_v = (float4 *)(s_rec + kG3Chunk);                   // [kG3Chunk][P]
-    ulonglong2 *ring = (ulonglong2 *)(s_v + kG3Chunk * P);        // [kG3Depth][kG3KS][kG3Threads]
+    ulonglong2 *ring = (ulonglong2 *)(s_v + kG3Chunk * P);        // [kG3Depth][kG3KS][T]
     __shared__ int s_item;
     __shared__ unsigned s_start[kG3Chunk / 32];    // bit k: record k starts a run
     __shared__ unsigned short s_runend[kG3Chunk];  // first record after k's run
     const int t = threadIdx.x;
     const int lane = t & 31;
     const int nitems = a.n_items[0];
-    constexpr int KS = kG3KS, D = kG3Depth, T = kG3Threads;
+    constexpr int KS = kG3KS, D = kG3Depth;
     for (;;) {
         __syncthreads();
         if (t == 0) s_item = atomicAdd(a.counter, 1);
@@ -889,17 +889,24 @@ __global__ void __launch_bounds__(kG3Threads, 2) k_grid3(Grid2Args a) {
     }
 }
 
-template <int P>
-static int launch_grid3(const Grid2Args &a, cudaStream_t st) {
-    auto kern = k_grid3<P>;
-    const size_t smem = (size_t)kG3Chunk * 16 * (1 + P) + (size_t)kG3Depth * kG3KS * kG3Threads * 16;
+template <int P, int T>
+static int launch_grid3_t(const Grid2Args &a, cudaStream_t st) {
+    auto kern = k_grid3<P, T>;
+    const size_t smem = (size_t)kG3Chunk * 16 * (1 + P) + (size_t)kG3Depth * kG3KS * T * 16;
     MTB_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
-    MTB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kG3Threads, smem));
+    MTB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, T, smem));
     if (per_sm < 1) return MTB_ERR_BAD_SHAPE;
-    kern<<<per_sm * sm_count(), kG3Threads, smem, st>>>(a);
+    kern<<<per_sm * sm_count(), T, smem, st>>>(a);
     MTB_LAUNCHED();
     return MTB_OK;
+}
+
+// threads: gridder block size (0: default, 256 or 512)
+template <int P>
+static int launch_grid3(const Grid2Args &a, int threads, cudaStream_t st) {
+    if (threads == 512) return launch_grid3_t<P, 512>(a, st);
+    return launch_grid3_t<P, kG3Threads>(a, st);
 }
 
 // ---------------------------------------------------------------------------
@@ -1400,6 +1407,7 @@ static int check_params(const mtb_grid_params *p) {
     if (p->tile < 0 || p->support_bucket < 0 || p->max_chunk < 0) return MTB_ERR_BAD_PARAM;
     if (p->merge < 0 || p->merge > 2) return MTB_ERR_BAD_PARAM;
     if (p->bulk_min_support < 0) return MTB_ERR_BAD_PARAM;
+    if (p->gridder_threads != 0 && p->gridder_threads != 256 && p->gridder_threads != 512) return MTB_ERR_BAD_PARAM;
     return MTB_OK;
 }
 
@@ -1643,18 +1651,21 @@ static int run_grid(const mtb_grid_params *p, const GridPlan &plan, const float2
         MTB_LAUNCHED();
         return MTB_OK;
     }
-    // k_grid4 is opt-in: it measured slower than k_grid3 on the mid-size
-    // workload (45.6 vs 30.7 ms per 29 M-record call)
-    const int min_m = p->bulk_min_support > 0 ? p->bulk_min_support : (1 << 30);
-    k_split<<<1, 1, 0, st>>>(s.bounds, s.n_items, plan.bt, min_m < kG4MinM ? kG4MinM : min_m, s.split);
-    MTB_LAUNCHED();
+    // k_grid4 is opt-in (bulk_min_support > 0): it measured slower than
+    // k_grid3 on the mid-size workload
+    const bool bulk = p->bulk_min_support > 0;
+    if (bulk) {
+        const int min_m = p->bulk_min_support;
+        k_split<<<1, 1, 0, st>>>(s.bounds, s.n_items, plan.bt, min_m < kG4MinM ? kG4MinM : min_m, s.split);
+        MTB_LAUNCHED();
+    }
     Grid2Args g2;
     g2.items = s.items;
-    g2.n_items = s.split;            // k_grid3 takes the items before the split
+    g2.n_items = bulk ? s.split : s.n_items;   // k_grid3 takes the items before the split
     g2.counter = s.counters;
     g2.njobs = 1;
     g2.jobs[0] = job_desc<P>(p, grid, grid_lo != nullptr, s);
-    MTB_TRY(launch_grid3<P>(g2, st));
+    MTB_TRY(launch_grid3<P>(g2, p->gridder_threads, st));
     Grid4Args g4;
     g4.items = s.items;
     g4.first = s.split;
@@ -1668,8 +1679,8 @@ static int run_grid(const mtb_grid_params *p, const GridPlan &plan, const float2
     g4.nx = p->nx;
     g4.bt = plan.bt;
     g4.err = s.err;
-    MTB_TRY(launch_grid4<P>(g4, st));
-    if (check_gridder()) {
+    if (bulk) MTB_TRY(launch_grid4<P>(g4, st));
+    if (bulk && check_gridder()) {
         int e = 0;
         MTB_CUDA_TRY(cudaMemcpyAsync(&e, s.err, sizeof(int), cudaMemcpyDeviceToHost, st));
         MTB_CUDA_TRY(cudaStreamSynchronize(st));
@@ -1791,6 +1802,7 @@ static int check_batch(const mtb_grid_job *jobs, int njobs) {
     for (int j = 0; j < njobs; j++) {
         MTB_TRY(check_params(&jobs[j].params));
         if (jobs[j].params.npol != jobs[0].params.npol) return MTB_ERR_BAD_SHAPE;
+        if (jobs[j].params.gridder_threads != jobs[0].params.gridder_threads) return MTB_ERR_BAD_PARAM;
         if (jobs[j].nrecords < 0) return MTB_ERR_BAD_SHAPE;
         if (!jobs[j].h_conv_info) return MTB_ERR_NULL;
     }
@@ -1864,7 +1876,7 @@ static int run_batch(const mtb_grid_job *jobs, int njobs, const GridPlan *plans,
     g2.items = items;
     g2.n_items = n_total;
     g2.counter = counter;
-    MTB_TRY(launch_grid3<P>(g2, st));
+    MTB_TRY(launch_grid3<P>(g2, jobs[0].params.gridder_threads, st));
     if (p0.gridder_end_event) MTB_CUDA_TRY(cudaEventRecord((cudaEvent_t)p0.gridder_end_event, st));
     for (int j = 0; j < njobs; j++) {
         const mtb_grid_job &J = jobs[j];

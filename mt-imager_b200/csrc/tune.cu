@@ -1,0 +1,101 @@
+// Gridder autotuner: picks the binning tile, support bucket, work-item length
+// and gridder block size of a batch of images by timing mtb_grid_batch with
+// each candidate (include/mtb.h).  Host code over the C ABI; no kernels.
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <vector>
+
+#include "mtb.h"
+#include "mtb_internal.cuh"
+
+namespace {
+
+const int kTiles[] = {16, 32, 64};
+const int kBuckets[] = {1, 2};
+const int kChunks[] = {256, 512};
+const int kThreads[] = {256, 512};
+const int kCandidates = 3 * 2 * 2 * 2;
+
+mtb_grid_tuning candidate(int c) {
+    mtb_grid_tuning t;
+    t.tile = kTiles[c / 8];
+    t.support_bucket = kBuckets[(c / 4) % 2];
+    t.max_chunk = kChunks[(c / 2) % 2];
+    t.gridder_threads = kThreads[c % 2];
+    t.ms = 0.f;
+    return t;
+}
+
+void apply(const mtb_grid_tuning &t, mtb_grid_job *jobs, int njobs) {
+    for (int j = 0; j < njobs; j++) {
+        jobs[j].params.tile = t.tile;
+        jobs[j].params.support_bucket = t.support_bucket;
+        jobs[j].params.max_chunk = t.max_chunk;
+        jobs[j].params.gridder_threads = t.gridder_threads;
+    }
+}
+
+struct Events {
+    cudaEvent_t a = nullptr, b = nullptr;
+    ~Events() {
+        if (a) cudaEventDestroy(a);
+        if (b) cudaEventDestroy(b);
+    }
+};
+
+}  // namespace
+
+extern "C" int mtb_grid_autotune_workspace_size(const mtb_grid_job *jobs, int njobs, size_t *bytes) {
+    if (!jobs || !bytes) return MTB_ERR_NULL;
+    if (njobs < 1 || njobs > 64) return MTB_ERR_BAD_SHAPE;
+    std::vector<mtb_grid_job> js(jobs, jobs + njobs);
+    size_t most = 0;
+    for (int c = 0; c < kCandidates; c++) {
+        apply(candidate(c), js.data(), njobs);
+        size_t b = 0;
+        MTB_TRY(mtb_grid_batch_workspace_size(js.data(), njobs, &b));
+        if (b > most) most = b;
+    }
+    *bytes = most;
+    return MTB_OK;
+}
+
+extern "C" int mtb_grid_autotune(mtb_grid_job *jobs, int njobs, void *d_workspace, size_t workspace_bytes,
+                                 mtb_stream_t stream, mtb_grid_tuning *best, mtb_grid_tuning *candidates) {
+    if (!jobs || !best) return MTB_ERR_NULL;
+    if (njobs < 1 || njobs > 64) return MTB_ERR_BAD_SHAPE;
+    for (int j = 0; j < njobs; j++)
+        if (!jobs[j].params.initialize_output) return MTB_ERR_BAD_PARAM;
+    cudaStream_t st = (cudaStream_t)stream;
+    Events ev;
+    MTB_CUDA_TRY(cudaEventCreate(&ev.a));
+    MTB_CUDA_TRY(cudaEventCreate(&ev.b));
+    // untimed first call: one-time costs (function attributes, module load)
+    apply(candidate(0), jobs, njobs);
+    MTB_TRY(mtb_grid_batch(jobs, njobs, d_workspace, workspace_bytes, stream));
+    int win = -1;
+    mtb_grid_tuning t_best{};
+    for (int c = 0; c < kCandidates; c++) {
+        mtb_grid_tuning t = candidate(c);
+        apply(t, jobs, njobs);
+        MTB_CUDA_TRY(cudaEventRecord(ev.a, st));
+        MTB_TRY(mtb_grid_batch(jobs, njobs, d_workspace, workspace_bytes, stream));
+        MTB_CUDA_TRY(cudaEventRecord(ev.b, st));
+        MTB_CUDA_TRY(cudaEventSynchronize(ev.b));
+        MTB_CUDA_TRY(cudaEventElapsedTime(&t.ms, ev.a, ev.b));
+        if (candidates) candidates[c] = t;
+        if (win < 0 || t.ms < t_best.ms) {
+            win = c;
+            t_best = t;
+        }
+    }
+    apply(t_best, jobs, njobs);
+    // the grids hold the last candidate's result; redo the winner unless it was last
+    if (win != kCandidates - 1) {
+        MTB_TRY(mtb_grid_batch(jobs, njobs, d_workspace, workspace_bytes, stream));
+        MTB_CUDA_TRY(cudaStreamSynchronize(st));
+    }
+    *best = t_best;
+    return MTB_OK;
+}

@@ -25,7 +25,8 @@ EXPORTS = (
     "mtb_preprocess_uvw_noalloc", "mtb_preprocess_uvw_noalloc_capacity",
     "mtb_finalize_workspace_size", "mtb_finalize", "mtb_status_string", "mtb_version",
     "mtb_release_caches", "mtb_kernel_launch_count", "mtb_calibrate_fp32",
-    "mtb_taper_kernel_build", "mtb_grid_batch_workspace_size", "mtb_grid_batch", "mtb_fits_create", "mtb_fits_write_channel", "mtb_fits_close",
+    "mtb_taper_kernel_build", "mtb_grid_batch_workspace_size", "mtb_grid_batch",
+    "mtb_grid_autotune_workspace_size", "mtb_grid_autotune", "mtb_fits_create", "mtb_fits_write_channel", "mtb_fits_close",
     "mtb_engine_create", "mtb_engine_submit", "mtb_engine_wait", "mtb_engine_request_bytes", "mtb_engine_destroy",
 )
 
@@ -57,7 +58,8 @@ class GridParams(ctypes.Structure):
                 ("w_sq_increment", ctypes.c_double), ("initialize_output", ctypes.c_int), ("tile", ctypes.c_int),
                 ("support_bucket", ctypes.c_int), ("max_chunk", ctypes.c_int), ("merge", ctypes.c_int),
                 ("gridder_start_event", ctypes.c_void_p), ("gridder_end_event", ctypes.c_void_p),
-                ("bulk_min_support", ctypes.c_int), ("psf", ctypes.c_int), ("exact_delta", ctypes.c_int)]
+                ("bulk_min_support", ctypes.c_int), ("psf", ctypes.c_int), ("exact_delta", ctypes.c_int),
+                ("gridder_threads", ctypes.c_int)]
 
 
 class GridStats(ctypes.Structure):
@@ -83,6 +85,11 @@ class FitsHeader(ctypes.Structure):
                 ("l_increment", ctypes.c_double), ("m_increment", ctypes.c_double), ("ra_deg", ctypes.c_double),
                 ("dec_deg", ctypes.c_double), ("freqs_hz", ctypes.c_void_p), ("stokes", ctypes.c_void_p),
                 ("telescope", ctypes.c_char_p), ("observer", ctypes.c_char_p), ("obs_mjd", ctypes.c_double)]
+
+
+class GridTuning(ctypes.Structure):
+    _fields_ = [("tile", ctypes.c_int), ("support_bucket", ctypes.c_int), ("max_chunk", ctypes.c_int),
+                ("gridder_threads", ctypes.c_int), ("ms", ctypes.c_float)]
 
 
 class EngineConfig(ctypes.Structure):
@@ -139,6 +146,9 @@ def load(path: str = LIB_PATH):
     L.mtb_calibrate_fp32.argtypes = [ctypes.POINTER(ctypes.c_double), p]
     L.mtb_grid_batch_workspace_size.argtypes = [ctypes.POINTER(GridJob), i, ctypes.POINTER(sz)]
     L.mtb_grid_batch.argtypes = [ctypes.POINTER(GridJob), i, p, sz, p]
+    L.mtb_grid_autotune_workspace_size.argtypes = [ctypes.POINTER(GridJob), i, ctypes.POINTER(sz)]
+    L.mtb_grid_autotune.argtypes = [ctypes.POINTER(GridJob), i, p, sz, p, ctypes.POINTER(GridTuning),
+                                    ctypes.POINTER(GridTuning)]
     L.mtb_fits_create.argtypes = [ctypes.c_char_p, ctypes.POINTER(FitsHeader), ctypes.POINTER(p)]
     L.mtb_fits_write_channel.argtypes = [p, i, p]
     L.mtb_fits_close.argtypes = [p]

@@ -114,7 +114,7 @@ class WProjectionImager:
                  trial_support=0, max_support=0, w_max=0.0, pol_type=L.MTB_POL_LINEAR, compensated=True,
                  tile=0, support_bucket=0, max_chunk=0, merge=0, bulk_min_support=0, device="cuda",
                  kernels: KernelTable | None = None, psf=False, mode="wproj", taper_support=7,
-                 exact_delta=False):
+                 exact_delta=False, gridder_threads=0):
         """mode "wproj" (W-projection kernels) or "normal" (taper-only kernel of
         support taper_support at oversampling `sampling`, one plane); psf
         grids every visibility as 1 + 0i (mt-imager's psf=true)."""
@@ -134,7 +134,7 @@ class WProjectionImager:
         self.compensated = compensated
         self.pol_type = pol_type
         self.tuning = dict(tile=tile, support_bucket=support_bucket, max_chunk=max_chunk, merge=merge,
-                           bulk_min_support=bulk_min_support)
+                           bulk_min_support=bulk_min_support, gridder_threads=gridder_threads)
         self.grid = torch.zeros((ny, nx, npol), dtype=torch.complex64, device=self.device)
         self.grid_lo = torch.zeros_like(self.grid) if compensated else None
         self.normalizer = torch.zeros(npol, dtype=torch.float32, device=self.device)
@@ -166,6 +166,7 @@ class WProjectionImager:
         gp.bulk_min_support = self.tuning["bulk_min_support"]
         gp.psf = int(self.psf)
         gp.exact_delta = int(self.exact_delta)
+        gp.gridder_threads = self.tuning["gridder_threads"]
         if self.gridder_events is not None:
             gp.gridder_start_event = self.gridder_events[0].cuda_event
             gp.gridder_end_event = self.gridder_events[1].cuda_event
@@ -241,15 +242,7 @@ class WProjectionImager:
                     compressed_points=int(s[3]))
 
 
-def grid_batch(entries, workspace=None, stream=None):
-    """Grid one chunk into each of several images with one persistent gridder
-    launch (mtb_grid_batch).  entries: (WProjectionImager, uvw, freq, vis,
-    weights, flags) with device tensors in the layouts of grid_device; every
-    imager must have the same npol.  Returns the workspace tensor so a caller
-    can pass it back (or keep it alive across a CUDA graph replay)."""
-    if not entries:
-        return workspace
-    lib = L.load()
+def _batch_jobs(entries):
     jobs = (L.GridJob * len(entries))()
     keep = []
     for j, (im, uvw, freq, vis, weights, flags) in enumerate(entries):
@@ -266,6 +259,20 @@ def grid_batch(entries, workspace=None, stream=None):
         J.d_grid, J.d_grid_lo = _ptr(im.grid), _ptr(im.grid_lo)
         J.d_normalizer, J.d_stats = _ptr(im.normalizer), _ptr(im.stats)
         keep.append(k)
+    return jobs, keep
+
+
+def grid_batch(entries, workspace=None, stream=None):
+    """Grid one chunk into each of several images with one persistent gridder
+    launch (mtb_grid_batch).  entries: (WProjectionImager, uvw, freq, vis,
+    weights, flags) with device tensors in the layouts of grid_device; every
+    imager must have the same npol and gridder_threads.  Returns the workspace
+    tensor so a caller can pass it back (or keep it alive across a CUDA graph
+    replay)."""
+    if not entries:
+        return workspace
+    lib = L.load()
+    jobs, keep = _batch_jobs(entries)
     need = ctypes.c_size_t(0)
     L.check(lib.mtb_grid_batch_workspace_size(jobs, len(entries), ctypes.byref(need)),
             "mtb_grid_batch_workspace_size")
@@ -276,3 +283,35 @@ def grid_batch(entries, workspace=None, stream=None):
     for im, *_ in entries:
         im._fresh = False
     return workspace
+
+
+TUNING_KEYS = ("tile", "support_bucket", "max_chunk", "gridder_threads")
+
+
+def autotune(entries, workspace=None, stream=None):
+    """Choose the gridder knobs (tile, support_bucket, max_chunk,
+    gridder_threads) for a batch by timing every candidate on this chunk
+    (mtb_grid_autotune).  entries as for grid_batch; every imager must start a
+    fresh image.  The chosen knobs are set on every imager (later chunks use
+    them) and its grid holds this chunk gridded with them.  Returns (best,
+    candidates, workspace): dicts with the knobs and the measured ms."""
+    if not entries:
+        raise ValueError("no images to tune")
+    if not all(im._fresh for im, *_ in entries):
+        raise ValueError("autotune needs fresh images (reset() first)")
+    lib = L.load()
+    jobs, keep = _batch_jobs(entries)
+    need = ctypes.c_size_t(0)
+    L.check(lib.mtb_grid_autotune_workspace_size(jobs, len(entries), ctypes.byref(need)),
+            "mtb_grid_autotune_workspace_size")
+    if workspace is None or workspace.numel() < need.value:
+        workspace = torch.empty(max(1, need.value), dtype=torch.uint8, device=entries[0][0].device)
+    best = L.GridTuning()
+    cands = (L.GridTuning * 24)()
+    L.check(lib.mtb_grid_autotune(jobs, len(entries), _ptr(workspace), need.value, _stream(stream),
+                                  ctypes.byref(best), cands), "mtb_grid_autotune")
+    as_dict = lambda t: dict({k: getattr(t, k) for k in TUNING_KEYS}, ms=t.ms)  # noqa: E731
+    for im, *_ in entries:
+        im.tuning.update({k: getattr(best, k) for k in TUNING_KEYS})
+        im._fresh = False
+    return as_dict(best), [as_dict(c) for c in cands], workspace

@@ -8,7 +8,7 @@ import pytest
 import torch
 
 from mtb import synth
-from mtb.imager import WProjectionImager, grid_batch
+from mtb.imager import TUNING_KEYS, WProjectionImager, autotune, grid_batch
 
 pytestmark = pytest.mark.gpu
 TOL = 1e-6
@@ -84,3 +84,44 @@ def test_batch_and_finalize_replay_from_cuda_graph():
         for o, r in zip(outs, ref):
             assert np.abs(o.cpu().numpy() - r).max() <= TOL * np.abs(r[0]).max()
     del g
+
+
+def test_autotune_grids_with_the_chosen_knobs():
+    """The autotuner times every candidate, applies the fastest to every
+    imager, and leaves the chunk gridded with it: equal to image-by-image
+    gridding with those knobs.  (Different knobs split the records
+    differently over FP32 register sums, so results of different knobs agree
+    only to the FP32 tolerance of the parity tests.)"""
+    cs = cases()[:3]
+    ims = [imager(setup) for setup, *_ in cs]
+    best, cands, ws = autotune([(im, *arrs) for im, (setup, *arrs) in zip(ims, cs)])
+    assert len(cands) == 24 and all(c["ms"] > 0 for c in cands)
+    assert best["ms"] == min(c["ms"] for c in cands)
+    assert {c["tile"] for c in cands} == {16, 32, 64} and {c["gridder_threads"] for c in cands} == {256, 512}
+    knobs = {k: best[k] for k in TUNING_KEYS}
+    single = []
+    for setup, *arrs in cs:
+        im = imager(setup)
+        im.tuning.update(knobs)
+        im.grid_device(*arrs)
+        single.append((im.finalize().cpu().numpy(), im.statistics()))
+    for im, (img1, st1) in zip(ims, single):
+        assert {k: im.tuning[k] for k in TUNING_KEYS} == knobs
+        assert im.statistics() == st1
+        img = im.finalize().cpu().numpy()
+        assert np.abs(img - img1).max() <= TOL * np.abs(img1[0]).max()
+    # later chunks use the chosen knobs
+    for im in ims:
+        im.reset()
+    grid_batch([(im, *arrs) for im, (setup, *arrs) in zip(ims, cs)], workspace=ws)
+    for im, (img1, _) in zip(ims, single):
+        img = im.finalize().cpu().numpy()
+        assert np.abs(img - img1).max() <= TOL * np.abs(img1[0]).max()
+
+
+def test_autotune_needs_fresh_images():
+    setup, *arrs = cases()[0]
+    im = imager(setup)
+    im.grid_device(*arrs)
+    with pytest.raises(ValueError):
+        autotune([(im, *arrs)])

@@ -163,7 +163,8 @@ def test_chunked_equals_single(cfg1):
 @pytest.mark.parametrize("tuning", [dict(tile=16), dict(tile=64), dict(support_bucket=3),
                                     dict(max_chunk=37, exact_delta=True),
                                     dict(merge=1), dict(merge=2), dict(merge=1, tile=16),
-                                    dict(bulk_min_support=17), dict(bulk_min_support=25), dict(exact_delta=True)])
+                                    dict(bulk_min_support=17), dict(bulk_min_support=25), dict(exact_delta=True),
+                                    dict(gridder_threads=512), dict(gridder_threads=512, tile=16, max_chunk=256)])
 def test_tuning_does_not_change_result(cfg1, tuning):
     obs, setup, geo, kern, img_o, grid_o, norm_o = cfg1
     im, img = run_gpu(obs, setup, **tuning)
