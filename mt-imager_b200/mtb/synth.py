@@ -193,3 +193,76 @@ def small_config(seed=0, n_ant=8, ntimes=40, nx=64, cell_arcsec=20.0, wplanes=8,
                            dt_s=60.0, nsrc=nsrc, fov_rad=nx * cell_arcsec * ARCSEC, noise=0.0,
                            flag_frac=flag_frac, seed=seed, dec_deg=dec_deg)
     return obs, setup
+
+
+def config3(seed=3, full=True):
+    """Precision stress, wide field: 64 antennas within 10 km, 1 channel at
+    725 MHz (|u| up to ~48 klambda fits the 8192^2 grid at 1.5 arcsec, and
+    |w| reaches ~5e4 lambda), 12 h at 4 s (2016 x 10,800 = 21,772,800
+    records), 20 point sources out to the field edge, 256 w-planes,
+    oversampling 8, support <= 129 (trial support 131), w_max = max |w|.
+    full=False keeps the field, the array extent and the kernels' support
+    range with 12 antennas, 12 h at 120 s (66 x 360 = 23,760 records) and 64
+    w-planes: a case the FP64 oracle finishes in about a minute."""
+    freq = 725e6
+    nx, cell = 8192, 1.5
+    obs = make_observation(n_ant=64 if full else 12, radius_m=10000.0, freqs_hz=(freq,), hours=12.0,
+                           dt_s=4.0 if full else 120.0, dec_deg=-45.0, nsrc=20, fov_rad=nx * cell * ARCSEC,
+                           noise=0.0, seed=seed)
+    w_max = float(np.abs(obs.uvw[2].astype(np.float64)).max() * freq / C_LIGHT)
+    setup = ImagingSetup(nx=nx, ny=nx, cell_arcsec=cell, wplanes=256 if full else 64, sampling=8,
+                         trial_support=131, max_support=129, w_max=w_max)
+    return obs, setup
+
+
+def predict_vis_torch(uvw_m, freq_hz: float, sources: np.ndarray, torch):
+    """predict_vis on the device: uvw_m a float32 torch tensor [3][R] (metres),
+    float64 phases, complex64 [R][4] out (linear feeds)."""
+    lam_inv = freq_hz / C_LIGHT
+    u, v, w = (uvw_m.double() * lam_inv)
+    out = torch.zeros((uvw_m.shape[1], 4), dtype=torch.complex128, device=uvw_m.device)
+    for l, m, si, sq, su, sv in sources:
+        n = math.sqrt(1.0 - l * l - m * m)
+        ph = torch.exp(-2j * math.pi * (u * l + v * m + w * (n - 1.0)))
+        out[:, 0] += (si + sq) * ph
+        out[:, 1] += complex(su, sv) * ph
+        out[:, 2] += complex(su, -sv) * ph
+        out[:, 3] += (si - sq) * ph
+    return out.to(torch.complex64)
+
+
+def config2_channel(seed=2, full=True, torch=None):
+    """One channel (1.4 GHz) of the mid-size configuration: 64 antennas within
+    4 km, 8 h at 2 s (2016 x 14,400 = 29,030,400 records), 200 power-law
+    sources (index -1.5, 1 mJy-1 Jy), 25 % of records flagged, 4096^2 at the
+    largest cell with max|u|/du + 65/2 < N/2 at 1.5 GHz, 128 w-planes,
+    oversampling 8, supports 7-65 (trial support 67).  Visibilities are
+    predicted on the device when `torch` is given.  full=False: 16 antennas,
+    8 h at 60 s (120 x 480 = 57,600 records)."""
+    rng = np.random.default_rng(seed)
+    n_ant = 64 if full else 16
+    enu = antenna_layout(n_ant, 4000.0, rng)
+    dt = 2.0 if full else 60.0
+    nt = int(round(8.0 * 3600.0 / dt))
+    ha = (np.arange(nt) - (nt - 1) / 2.0) * dt * (2 * np.pi / 86164.0905)
+    uvw = track_uvw(enu, -30.0, -45.0, ha).astype(np.float32)
+    R = uvw.shape[1]
+    n = 4096
+    uv_max = float(np.abs(uvw[:2]).max()) * 1.5e9 / C_LIGHT
+    du = uv_max / (n / 2 - (65 / 2 + 1))
+    dl = 1.0 / (n * du)
+    srcs = random_sources(200, n * dl, rng, flux=(1e-3, 1.0), powerlaw=-1.5)
+    f = 1.4e9
+    if torch is not None:
+        vis = predict_vis_torch(torch.from_numpy(uvw).cuda(), f, srcs, torch).cpu().numpy()
+    else:
+        vis = predict_vis(uvw, f, srcs).astype(np.complex64)
+    fl = np.zeros((R, 4), np.int32)
+    fl[rng.random(R) < 0.25, :] = 1
+    obs = Observation(uvw=uvw, freqs_hz=np.array([f]), vis=[vis], weights=[np.ones((R, 4), np.float32)],
+                      flags=[fl], nbaselines=n_ant * (n_ant - 1) // 2, ntimes=nt,
+                      meta=dict(n_ant=n_ant, sources=srcs))
+    setup = ImagingSetup(nx=n, ny=n, cell_arcsec=dl / ARCSEC, wplanes=128, sampling=8, trial_support=67,
+                         max_support=65)
+    return obs, setup
+

@@ -1,0 +1,65 @@
+"""Stated image errors at the large configurations: the sm_100a path against
+the FP64 W-projection oracle, with the RMS error of every Stokes image
+relative to the Stokes I peak printed and held to 1e-5, and the kernel table
+held to 1e-6.
+  wide  precision stress, wide field: 8192^2, 256 w-planes, support <= 129,
+        |w| to ~5e4 lambda (synth.config3)
+  mid   one channel of the mid-size configuration: 4096^2, 128 w-planes,
+        supports 7-65, 25 % flagged (synth.config2_channel)
+
+By default both run with fewer records (and the wide field with fewer
+w-planes); MTB_PRECISION_FULL=1 runs the full configurations (21.8 M and
+29.0 M records; minutes of FP64 oracle work on the host).  The GPU grids in
+chunks of 4,194,304 records into the compensated two-float grid, as a long
+observation is imaged.
+"""
+import os
+import time
+
+import numpy as np
+import pytest
+import torch
+
+from mtb import synth
+from mtb.imager import WProjectionImager
+
+pytestmark = pytest.mark.gpu
+
+KERNEL_TOL = 1e-6
+IMAGE_RMS_TOL = 1e-5
+CHUNK = 1 << 22
+
+
+@pytest.mark.parametrize("case", ["wide", "mid"])
+def test_stated_image_error(oracle, case):
+    full = os.environ.get("MTB_PRECISION_FULL") == "1"
+    if case == "wide":
+        obs, setup = synth.config3(full=full)
+    else:
+        obs, setup = synth.config2_channel(full=full, torch=torch)
+    t0 = time.perf_counter()
+    geo = oracle.geometry_for(setup)
+    kern = oracle.wkernels(geo)
+    img_o, _, _ = oracle.image_channel(obs, 0, setup, kern, geo)
+    t_oracle = time.perf_counter() - t0
+
+    im = WProjectionImager(setup.nx, setup.ny, setup.dl, wplanes=setup.wplanes, sampling=setup.sampling,
+                           trial_support=setup.trial_support, max_support=setup.max_support, w_max=setup.w_max)
+    k = im.build_kernels()
+    assert np.array_equal(k.conv_info, kern["conv_info"])
+    assert np.abs(k.table.cpu().numpy() - kern["table"]).max() <= KERNEL_TOL
+    f = obs.freq_over_c(0)
+    for a in range(0, obs.nrec, CHUNK):
+        b = min(obs.nrec, a + CHUNK)
+        im.grid_chunk(obs.uvw[:, a:b], f[a:b], obs.vis[0][a:b], obs.weights[0][a:b], obs.flags[0][a:b])
+    img = im.finalize().cpu().numpy()
+    torch.cuda.synchronize()
+
+    peak = np.abs(img_o[0]).max()
+    errs = [float(np.sqrt(np.mean((img[p] - img_o[p]) ** 2)) / peak) for p in range(4)]
+    st = im.statistics()
+    print("\n%s (%s): %d records, %d gridded, supports %d-%d, w_max %.0f lambda, oracle %.0f s; "
+          "RMS error / Stokes I peak: I %.2e Q %.2e U %.2e V %.2e"
+          % (case, "full" if full else "reduced", obs.nrec, st["gridded_records"], int(kern["supports"].min()),
+             int(kern["supports"].max()), geo["w_max"], t_oracle, *errs))
+    assert max(errs) <= IMAGE_RMS_TOL
