@@ -42,6 +42,22 @@ C_LIGHT = 299792458.0
 ARCSEC = math.pi / (180.0 * 3600.0)
 
 
+# ------------------------------------------------------------ replicas ----
+def max_over_ranks(ms, world, dist, torch, device):
+    """The slowest rank's time, returned on every rank (an all-reduce MAX;
+    every rank takes this step in the same order)."""
+    if world <= 1:
+        return float(ms)
+    tt = torch.tensor([float(ms)], dtype=torch.float64, device=device)
+    dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+    return float(tt.item())
+
+
+def job_throughput(samples_per_rank_step, world, ms_per_step):
+    """Whole-job samples/s: every replica grids the same work per step."""
+    return samples_per_rank_step * world / (ms_per_step * 1e-3)
+
+
 # ------------------------------------------------------------- workload ----
 def workload_spec(args):
     if args.config == "small":
@@ -402,13 +418,9 @@ def main():
         torch.cuda.profiler.stop()
     clk = clocks.stop()
     launches = (lib.mtb_kernel_launch_count() - launches0) // max(1, args.steps)
-    ms = t_start.elapsed_time(t_end)
-    if world > 1:
-        tt = torch.tensor([ms], device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms = float(tt.item())
+    ms = max_over_ranks(t_start.elapsed_time(t_end), world, dist, torch, dev)
     ms_per_step = ms / args.steps
-    value = samples_per_step * world / (ms_per_step * 1e-3)
+    value = job_throughput(samples_per_step, world, ms_per_step)
 
     # ---- roofline of the gridder (FP32 FMA pipe; peak measured on this GPU)
     peak = ctypes.c_double(0)
@@ -530,12 +542,8 @@ def run_e2e(args, torch, dev, uvw_d, chans, imagers, images, samples_per_step, w
         step()
     b.record()
     torch.cuda.synchronize()
-    ms = a.elapsed_time(b) / args.e2e_steps
-    if world > 1:
-        tt = torch.tensor([ms], device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms = float(tt.item())
-    return {"value": samples_per_step * world / (ms * 1e-3), "unit": "samples/s", "h2d_bytes_per_step": int(h2d),
+    ms = max_over_ranks(a.elapsed_time(b) / args.e2e_steps, world, dist, torch, dev)
+    return {"value": job_throughput(samples_per_step, world, ms), "unit": "samples/s", "h2d_bytes_per_step": int(h2d),
             "d2h_bytes_per_step": int(d2h), "ms_per_step": ms}
 
 
