@@ -140,14 +140,23 @@ class ClockSampler:
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, gpu_index):
+    def __init__(self, gpu_index, log_dir=None):
+        """Samples nvidia-smi every 200 ms into log_dir/clocks_rank<i>.csv, or
+        into a temporary file when log_dir is None."""
         self.proc = None
         self.gpu = gpu_index
-        self.path = os.path.join(ROOT, "gpurun_out", "clocks_rank%d.csv" % gpu_index)
+        self.keep = bool(log_dir)
+        if log_dir:
+            self.path = os.path.join(log_dir, "clocks_rank%d.csv" % gpu_index)
+        else:
+            import tempfile
+            fd, self.path = tempfile.mkstemp(prefix="mtb_clocks_", suffix=".csv")
+            os.close(fd)
 
     def start(self):
         try:
-            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            if os.path.dirname(self.path):
+                os.makedirs(os.path.dirname(self.path), exist_ok=True)
             self.fh = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
                                           "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.fh,
@@ -178,6 +187,8 @@ class ClockSampler:
             for nme, v in zip(names, f[5:9]):
                 if v.lower().startswith("active"):
                     reasons.add(nme)
+        if not self.keep:
+            os.remove(self.path)
         if not sm:
             return None
         return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
@@ -286,6 +297,8 @@ def main():
                     help="requests of the shortened stream the default (mid-size) run measures")
     ap.add_argument("--serve-sample-max-records", type=float, default=5e6)
     ap.add_argument("--serve-slots", type=int, default=4)
+    ap.add_argument("--clock-log", default=None,
+                    help="directory that keeps the nvidia-smi clock samples of the timed region")
     ap.add_argument("--profile-range", action="store_true",
                     help="bracket the timed steps with cudaProfilerStart/Stop (for ncu --profile-from-start off)")
     args = ap.parse_args()
@@ -393,7 +406,7 @@ def main():
     samples_per_step = sum((s["gridded_records"] + s["compressed_records"]) * 4 for s in stats)
     flops_per_step = sum(8.0 * 4 * s["gridded_points"] for s in stats)
 
-    clocks = ClockSampler(local)
+    clocks = ClockSampler(local, args.clock_log)
     launches0 = lib.mtb_kernel_launch_count()
     lat, gms = [], []
     if world > 1:
