@@ -155,6 +155,9 @@ typedef struct mtb_grid_params {
                                   (order-independent, about half the grid error, slower)   */
     int gridder_threads;       /* 0: 256; threads of a gridder block, which grids one work
                                   item at a time (256 or 512)                              */
+    int flags_u8;              /* 0: d_flags is int32 [R][P] (the reference's layout); 1: it
+                                  is one byte per flag, uint8 [R][P] (0 = keep, 1 = flagged;
+                                  a quarter of the bytes to move), passed cast to int *    */
 } mtb_grid_params;
 
 typedef struct mtb_grid_stats {

@@ -150,10 +150,11 @@ class Imager {
 public:
     // buffers: kept by the caller and reused across images, or nullptr to let
     // the imager own its own
+    // flags_u8: grid() receives one byte per flag instead of int32
     Imager(std::shared_ptr<const KernelTable> k, int npol, int pol_type, bool compensated, cudaStream_t stream,
-           ImagerBuffers *buffers = nullptr, bool exact_delta = false)
+           ImagerBuffers *buffers = nullptr, bool exact_delta = false, bool flags_u8 = false)
         : k_(std::move(k)), npol_(npol), pol_type_(pol_type), compensated_(compensated), exact_delta_(exact_delta),
-          s_(stream) {
+          flags_u8_(flags_u8), s_(stream) {
         if (!buffers) {
             own_.reset(new ImagerBuffers());
             buffers = own_.get();
@@ -186,6 +187,7 @@ public:
         gp.w_sq_increment = k_->info.w_sq_increment;
         gp.initialize_output = fresh_ ? 1 : 0;
         gp.exact_delta = exact_delta_ ? 1 : 0;
+        gp.flags_u8 = flags_u8_ ? 1 : 0;
         return gp;
     }
 
@@ -197,7 +199,8 @@ public:
         return b;
     }
 
-    // One WImager chunk from device arrays (layouts of mtb.h).
+    // One WImager chunk from device arrays (layouts of mtb.h; flags int32, or
+    // bytes passed cast to int * when the imager was made with flags_u8).
     void grid(const float *uvw, const float *freq, const void *vis, const float *weights, const int *flags,
               int records) {
         mtb_grid_params gp = grid_params();
@@ -237,7 +240,7 @@ public:
 private:
     std::shared_ptr<const KernelTable> k_;
     int npol_, pol_type_;
-    bool compensated_, exact_delta_;
+    bool compensated_, exact_delta_, flags_u8_;
     cudaStream_t s_;
     bool fresh_ = true;
     std::unique_ptr<ImagerBuffers> own_;

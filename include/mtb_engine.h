@@ -55,6 +55,8 @@ typedef struct mtb_image_request {
                                      (order-independent result); see mtb_grid_params       */
     long long uvw_row_stride;     /* floats between the u, v and w rows of uvw (a slice of
                                      a longer uvw array); 0: nrecords                      */
+    int flags_u8;                 /* 1: flags is uint8 [R][P] (one byte per flag), passed
+                                     cast to int *; 0: int32 [R][P]                        */
 } mtb_image_request;
 
 typedef struct mtb_image_result {

@@ -339,7 +339,8 @@ void mtb_engine::run(mtb::Job *j, Slot &sl) {
         bool hit = false;
         std::shared_ptr<mtb::KernelTable> k = cache->get(r.geometry, st, &hit);
         j->res.kernel_cache_hit = hit ? 1 : 0;
-        mtb::Imager im(k, P, r.pol_type, r.compensated != 0, st, &sl.bufs, r.exact_delta != 0);
+        mtb::Imager im(k, P, r.pol_type, r.compensated != 0, st, &sl.bufs, r.exact_delta != 0, r.flags_u8 != 0);
+        const size_t flag_bytes = r.flags_u8 ? 1 : 4;
         const int chunk = cfg.chunk_records;
         int b = 0;
         for (int c0 = 0; c0 < R; c0 += chunk, b ^= 1) {
@@ -359,7 +360,7 @@ void mtb_engine::run(mtb::Job *j, Slot &sl) {
             stage(off_freq, r.freq + c0, (size_t)n * 4);
             stage(off_vis, (const float2 *)r.vis + (size_t)c0 * P, (size_t)n * P * 8);
             stage(off_wt, r.weights + (size_t)c0 * P, (size_t)n * P * 4);
-            stage(off_fl, r.flags + (size_t)c0 * P, (size_t)n * P * 4);
+            stage(off_fl, (const unsigned char *)r.flags + (size_t)c0 * P * flag_bytes, (size_t)n * P * flag_bytes);
             mtb::cuda_check(cudaEventRecord(sl.ev[b], st), "event");
             im.grid((const float *)d, (const float *)(d + off_freq), d + off_vis, (const float *)(d + off_wt),
                     (const int *)(d + off_fl), n);

@@ -70,9 +70,10 @@ struct BucketTable {
 __device__ __forceinline__ int bucket_of(int S, int half) { return (S - 1) / (2 * half); }
 
 // ------------------------------------------------------------- preprocess --
-template <int P>
+// F: flag element type, int (the reference's layout) or unsigned char
+template <int P, typename F>
 __global__ void k_preprocess(int R, const float *__restrict__ uvw, const float *__restrict__ freq,
-                             const float *__restrict__ weights, const int *__restrict__ flags,
+                             const float *__restrict__ weights, const F *__restrict__ flags,
                              const int *__restrict__ conv_info, const float *__restrict__ conv_sums,
                              int nw, double w_inc, int s, int T, int nx, int ny, double du, double dv,
                              int4 *__restrict__ pos, int *__restrict__ meta, double *__restrict__ norm_acc,
@@ -86,7 +87,7 @@ __global__ void k_preprocess(int R, const float *__restrict__ uvw, const float *
         bool grid = false;
 #pragma unroll
         for (int p = 0; p < P; p++) {
-            fl[p] = flags[(size_t)r * P + p];
+            fl[p] = (int)flags[(size_t)r * P + p];
             wt[p] = weights[(size_t)r * P + p];
             if (fl[p] == 0) grid = true;
         }
@@ -260,11 +261,11 @@ __device__ __forceinline__ int padded_index(int ci, int S, const int *__restrict
     return __ldg(&pbase[lo]) + sub * S * (S + 1);
 }
 
-template <int P, bool DIRECT>
+template <int P, bool DIRECT, typename F>
 __global__ void k_gather(int R, const unsigned *__restrict__ skeys, const int *__restrict__ sidx,
                          const int4 *__restrict__ pos, const int *__restrict__ meta,
                          const float2 *__restrict__ vis, const float *__restrict__ weights,
-                         const int *__restrict__ flags, int4 *__restrict__ wpos, void *__restrict__ wvis,
+                         const F *__restrict__ flags, int4 *__restrict__ wpos, void *__restrict__ wvis,
                          BucketTable bt, int nx, const int *__restrict__ conv_info, const int *__restrict__ pbase,
                          int nw, int psf) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < R; i += gridDim.x * blockDim.x) {
@@ -856,7 +857,8 @@ __global__ void __launch_bounds__(T, 512 / T) k_grid3(Grid2Args a) {
                 const int e = s_runend[i];
                 const int re = e < i1 ? e : i1;
                 for (; i < re; ++i) {
-                    cp_async_wait<D - 1>();     // this thread's copies for record i have landed
+                    // the visibilities were staged before the item started: load
+                    // them ahead of the wait so their latency overlaps it
                     float2 vp[P], wp[P];
                     const float4 *vr = s_v + i * P;
 #pragma unroll
@@ -865,6 +867,7 @@ __global__ void __launch_bounds__(T, 512 / T) k_grid3(Grid2Args a) {
                         vp[p] = make_float2(q.x, q.y);
                         wp[p] = make_float2(q.z, q.w);
                     }
+                    cp_async_wait<D - 1>();     // this thread's copies for record i have landed
                     const float4 *src = (const float4 *)(ring + ((i & (D - 1)) * KS * T + t));
 #pragma unroll
                     for (int j = 0; j < KS; j++) {
@@ -1490,6 +1493,36 @@ static bool check_gridder() {
     return v == 1;
 }
 
+// k_preprocess / k_gather with the caller's flag element type: int32 (the
+// reference's layout) or bytes (mtb_grid_params.flags_u8).
+template <int P>
+static void launch_preprocess(const mtb_grid_params *p, int blocks, cudaStream_t st, int R, const float *uvw,
+                              const float *freq, const float *weights, const int *flags, const int *conv_info,
+                              const float *conv_sums, int T, int4 *pos, int *meta, double *norm_acc,
+                              float *convsum_out) {
+    if (p->flags_u8)
+        k_preprocess<P, unsigned char><<<blocks, 256, 0, st>>>(
+            R, uvw, freq, weights, (const unsigned char *)flags, conv_info, conv_sums, p->wplanes, p->w_sq_increment,
+            p->sampling, T, p->nx, p->ny, p->u_increment, p->v_increment, pos, meta, norm_acc, convsum_out);
+    else
+        k_preprocess<P, int><<<blocks, 256, 0, st>>>(R, uvw, freq, weights, flags, conv_info, conv_sums, p->wplanes,
+                                                     p->w_sq_increment, p->sampling, T, p->nx, p->ny, p->u_increment,
+                                                     p->v_increment, pos, meta, norm_acc, convsum_out);
+}
+
+template <int P, bool DIRECT>
+static void launch_gather(const mtb_grid_params *p, int blocks, cudaStream_t st, int R, const GridSpace &s,
+                          const float2 *vis, const float *weights, const int *flags, const GridPlan &plan,
+                          const int *conv_info, const int *pbase, int nw) {
+    if (p->flags_u8)
+        k_gather<P, DIRECT, unsigned char><<<blocks, 256, 0, st>>>(
+            R, s.skeys, s.sidx, s.pos, s.meta, vis, weights, (const unsigned char *)flags, s.wpos, s.wvis, plan.bt,
+            p->nx, conv_info, pbase, nw, p->psf);
+    else
+        k_gather<P, DIRECT, int><<<blocks, 256, 0, st>>>(R, s.skeys, s.sidx, s.pos, s.meta, vis, weights, flags,
+                                                         s.wpos, s.wvis, plan.bt, p->nx, conv_info, pbase, nw, p->psf);
+}
+
 // Everything of one mtb_grid call before the gridder kernels: preprocessing,
 // compression, binning into work items, the gathered records and
 // visibilities, and (direct gridders) the padded and expanded kernel tables,
@@ -1507,9 +1540,8 @@ static int prepare_grid(const mtb_grid_params *p, const GridPlan &plan, const fl
     MTB_CUDA_TRY(cudaMemsetAsync(s.counters, 0, kMaxBuckets * sizeof(int), st));
     int blocks = std::min((R + 255) / 256, sms * 8);
     if (blocks < 1) blocks = 1;
-    k_preprocess<P><<<blocks, 256, 0, st>>>(R, uvw, freq, weights, flags, conv_info, conv_sums, p->wplanes,
-                                            p->w_sq_increment, p->sampling, T, p->nx, p->ny, p->u_increment,
-                                            p->v_increment, s.pos, s.meta, s.norm_acc, nullptr);
+    launch_preprocess<P>(p, blocks, st, R, uvw, freq, weights, flags, conv_info, conv_sums, T, s.pos, s.meta,
+                         s.norm_acc, nullptr);
     MTB_LAUNCHED();
     k_compress<<<blocks, 256, 0, st>>>(R, p->nx, s.pos, s.meta, s.keys, s.iota, plan.bt, s.stats);
     MTB_LAUNCHED();
@@ -1533,16 +1565,14 @@ static int prepare_grid(const mtb_grid_params *p, const GridPlan &plan, const fl
                                             s.n_items);
     MTB_LAUNCHED();
     if (p->merge == 1) {
-        k_gather<P, false><<<blocks, 256, 0, st>>>(R, s.skeys, s.sidx, s.pos, s.meta, vis, weights, flags, s.wpos,
-                                                   s.wvis, plan.bt, p->nx, nullptr, nullptr, 0, p->psf);
+        launch_gather<P, false>(p, blocks, st, R, s, vis, weights, flags, plan, nullptr, nullptr, 0);
         MTB_LAUNCHED();
         (void)end_bit;
         return MTB_OK;
     }
     k_pad_bases<<<1, 1, 0, st>>>(conv_info, p->wplanes, T, s.pbase);
     MTB_LAUNCHED();
-    k_gather<P, true><<<blocks, 256, 0, st>>>(R, s.skeys, s.sidx, s.pos, s.meta, vis, weights, flags, s.wpos,
-                                              s.wvis, plan.bt, p->nx, conv_info, s.pbase, p->wplanes, p->psf);
+    launch_gather<P, true>(p, blocks, st, R, s, vis, weights, flags, plan, conv_info, s.pbase, p->wplanes);
     MTB_LAUNCHED();
     (void)end_bit;
     {
@@ -1948,10 +1978,8 @@ extern "C" int mtb_preprocess_uvw(const mtb_grid_params *p, const int *d_conv_in
     MTB_CUDA_TRY(cudaMemsetAsync(s.norm_acc, 0, 4 * sizeof(double), st));
     MTB_CUDA_TRY(cudaMemsetAsync(s.stats, 0, 4 * sizeof(unsigned long long), st));
 #define MTB_PRE(PP)                                                                                           \
-    k_preprocess<PP><<<blocks, 256, 0, st>>>(R, d_uvw, d_freq, d_weights, d_flags, d_conv_info, d_conv_sums,   \
-                                             p->wplanes, p->w_sq_increment, p->sampling, T, p->nx, p->ny,     \
-                                             p->u_increment, p->v_increment, s.pos, s.meta, s.norm_acc,       \
-                                             d_conv_sum)
+    launch_preprocess<PP>(p, blocks, st, R, d_uvw, d_freq, d_weights, d_flags, d_conv_info, d_conv_sums, T,     \
+                          s.pos, s.meta, s.norm_acc, d_conv_sum)
     if (p->npol == 1) MTB_PRE(1);
     else if (p->npol == 2) MTB_PRE(2);
     else MTB_PRE(4);
@@ -2036,9 +2064,8 @@ extern "C" int mtb_preprocess_uvw_noalloc(const mtb_grid_params *p, const int *d
     MTB_CUDA_TRY(cudaMemsetAsync(norm_acc, 0, 4 * sizeof(double), st));
     MTB_CUDA_TRY(cudaMemsetAsync(stats, 0, 4 * sizeof(unsigned long long), st));
 #define MTB_PRE(PP)                                                                                           \
-    k_preprocess<PP><<<blocks, 256, 0, st>>>(R, d_uvw, d_freq, d_weights, d_flags, d_conv_info, d_conv_sums,   \
-                                             p->wplanes, p->w_sq_increment, p->sampling, T, p->nx, p->ny,     \
-                                             p->u_increment, p->v_increment, pos, meta, norm_acc, d_conv_sum)
+    launch_preprocess<PP>(p, blocks, st, R, d_uvw, d_freq, d_weights, d_flags, d_conv_info, d_conv_sums, T,     \
+                          pos, meta, norm_acc, d_conv_sum)
     if (p->npol == 1) MTB_PRE(1);
     else if (p->npol == 2) MTB_PRE(2);
     else MTB_PRE(4);

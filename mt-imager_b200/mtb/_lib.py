@@ -59,7 +59,7 @@ class GridParams(ctypes.Structure):
                 ("support_bucket", ctypes.c_int), ("max_chunk", ctypes.c_int), ("merge", ctypes.c_int),
                 ("gridder_start_event", ctypes.c_void_p), ("gridder_end_event", ctypes.c_void_p),
                 ("bulk_min_support", ctypes.c_int), ("psf", ctypes.c_int), ("exact_delta", ctypes.c_int),
-                ("gridder_threads", ctypes.c_int)]
+                ("gridder_threads", ctypes.c_int), ("flags_u8", ctypes.c_int)]
 
 
 class GridStats(ctypes.Structure):
@@ -103,7 +103,7 @@ class ImageRequest(ctypes.Structure):
                 ("compensated", ctypes.c_int), ("nrecords", ctypes.c_int), ("uvw", ctypes.c_void_p),
                 ("freq", ctypes.c_void_p), ("vis", ctypes.c_void_p), ("weights", ctypes.c_void_p),
                 ("flags", ctypes.c_void_p), ("image", ctypes.c_void_p), ("exact_delta", ctypes.c_int),
-                ("uvw_row_stride", ctypes.c_longlong)]
+                ("uvw_row_stride", ctypes.c_longlong), ("flags_u8", ctypes.c_int)]
 
 
 class ImageResult(ctypes.Structure):

@@ -53,7 +53,8 @@ class Engine:
         freq = _c(freq, np.float32)
         vis = _c(vis, np.complex64)
         weights = _c(weights, np.float32)
-        flags = _c(flags, np.int32)
+        byte_flags = np.asarray(flags).dtype in (np.uint8, np.bool_)
+        flags = _c(flags, np.uint8 if byte_flags else np.int32)
         R = int(freq.size)
         P = int(vis.shape[1]) if vis.ndim == 2 else 1
         if uvw.shape != (3, R) or vis.shape != (R, P) or weights.shape != (R, P) or flags.shape != (R, P):
@@ -63,7 +64,8 @@ class Engine:
                             max_support, float(w_max))
         ptr = lambda a: a.ctypes.data_as(ctypes.c_void_p)  # noqa: E731
         req = L.ImageRequest(g, P, pol_type, int(bool(compensated)), R, ptr(uvw), ptr(freq), ptr(vis),
-                             ptr(weights), ptr(flags), ptr(image), int(bool(exact_delta)), row_stride)
+                             ptr(weights), ptr(flags), ptr(image), int(bool(exact_delta)), row_stride,
+                             int(byte_flags))
         return req, (uvw, freq, vis, weights, flags, image)
 
     def request_bytes(self, *args, **kw) -> int:

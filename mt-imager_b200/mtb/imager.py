@@ -32,6 +32,20 @@ def _dev(x, dtype, device):
     return torch.from_numpy(np.ascontiguousarray(x)).to(device=device, dtype=dtype)
 
 
+def _is_byte_flags(flags):
+    dt = getattr(flags, "dtype", None)
+    return dt in (np.uint8, np.bool_, torch.uint8, torch.bool)
+
+
+def _flags_u8(flags):
+    """mtb_grid_params.flags_u8 for a device flag tensor (int32 or uint8)."""
+    if flags.dtype == torch.uint8:
+        return 1
+    if flags.dtype == torch.int32:
+        return 0
+    raise TypeError("flags must be int32 or uint8 on the device")
+
+
 @dataclasses.dataclass
 class KernelTable:
     """AmalgamatedConvFunction, convInfo and ConvSums
@@ -188,13 +202,14 @@ class WProjectionImager:
     # -- WImager
     def grid_chunk(self, uvw, freq, vis, weights, flags, stream=None):
         """Grid one chunk: uvw [3][R] float32 metres, freq [R] nu/c, vis [R][P]
-        complex64, weights [R][P] float32, flags [R][P] int32 (numpy or torch)."""
+        complex64, weights [R][P] float32, flags [R][P] int32, or uint8 / bool
+        (one byte per flag, mtb_grid_params.flags_u8) -- numpy or torch."""
         dev = self.device
         uvw = _dev(uvw, torch.float32, dev)
         freq = _dev(freq, torch.float32, dev)
         vis = _dev(vis, torch.complex64, dev)
         weights = _dev(weights, torch.float32, dev)
-        flags = _dev(flags, torch.int32, dev)
+        flags = _dev(flags, torch.uint8 if _is_byte_flags(flags) else torch.int32, dev)
         R = int(freq.numel())
         if vis.shape != (R, self.npol) or weights.shape != (R, self.npol) or flags.shape != (R, self.npol):
             raise ValueError("record arrays must be [R][npol]")
@@ -206,6 +221,7 @@ class WProjectionImager:
         k = self.build_kernels()
         R = int(freq.numel())
         gp = self.grid_params(self._fresh)
+        gp.flags_u8 = _flags_u8(flags)
         ws, nbytes = self._workspace(R, gp)
         st = L.check(self.lib.mtb_grid(ctypes.byref(gp), _ptr(k.table), _ptr(k.d_conv_info),
                                        k.conv_info.ctypes.data_as(ctypes.c_void_p), _ptr(k.conv_sums),
@@ -249,6 +265,7 @@ def _batch_jobs(entries):
         k = im.build_kernels()
         gp = im.grid_params(im._fresh)
         J = jobs[j]
+        gp.flags_u8 = _flags_u8(flags)
         J.params = gp
         J.d_table, J.d_conv_info = _ptr(k.table), _ptr(k.d_conv_info)
         J.h_conv_info = k.conv_info.ctypes.data_as(ctypes.c_void_p)
