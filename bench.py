@@ -360,7 +360,8 @@ def main():
     chans = []
     for c, f in enumerate(freqs):
         vis = make_vis(uvw, f, srcs, torch, gen)
-        flags = (torch.rand(R, device=dev, generator=gen) < spec["flag"]).int()[:, None].repeat(1, 4).contiguous()
+        # one byte per flag (mtb_grid_params.flags_u8): a quarter of the int32 layout's bytes to move
+        flags = (torch.rand(R, device=dev, generator=gen) < spec["flag"]).to(torch.uint8)[:, None].repeat(1, 4).contiguous()
         weights = torch.ones((R, 4), dtype=torch.float32, device=dev)
         freq = torch.full((R,), f / C_LIGHT, dtype=torch.float32, device=dev)
         chans.append((freq, vis, weights, flags))
@@ -480,7 +481,8 @@ def main():
             "config": {"workload": workload_name(spec), "records_per_channel": R, "channels": len(freqs),
                        "image": n, "cell_arcsec": dl / ARCSEC, "wplanes": spec["wplanes"],
                        "sampling": spec["sampling"], "supports": [int(sup.min()), int(sup.max())],
-                       "samples_per_step": samples_per_step, "l2": "inputs larger than L2 (2 GB per channel)",
+                       "samples_per_step": samples_per_step, "l2": "inputs larger than L2 (1.6 GB per channel)",
+                       "flags": "uint8 [R][4] (flags_u8)",
                        "parallelism": "replicas" if world > 1 else "single GPU"},
             "images_per_s": len(freqs) * world / (ms_per_step * 1e-3),
             "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
@@ -581,7 +583,7 @@ def make_request_pool(torch, dev, rng, records):
     gen = torch.Generator(device=dev).manual_seed(11)
     pool = dict(uvw=np.empty((3, Rp), np.float32), freq=np.empty(Rp, np.float32),
                 vis=np.empty((Rp, 4), np.complex64), weights=np.ones((Rp, 4), np.float32),
-                flags=np.empty((Rp, 4), np.int32), uv_max=uv_max)
+                flags=np.empty((Rp, 4), np.uint8), uv_max=uv_max)
     u1 = uvw1.cpu().numpy()
     srcs = synth.random_sources(3, 4096 * cell_for(dict(spec, nx=4096, f_hi=1.5e9), uv_max, torch), rng,
                                 flux=(0.1, 1.0))
@@ -590,7 +592,8 @@ def make_request_pool(torch, dev, rng, records):
         pool["uvw"][:, sl] = u1
         pool["freq"][sl] = f / C_LIGHT
         pool["vis"][sl] = make_vis(uvw1, f, srcs, torch, gen).cpu().numpy()
-        pool["flags"][sl] = (torch.rand(R1, device=dev, generator=gen) < 0.1).int()[:, None].repeat(1, 4).cpu().numpy()
+        pool["flags"][sl] = ((torch.rand(R1, device=dev, generator=gen) < 0.1).to(torch.uint8)[:, None].repeat(1, 4)
+                             .cpu().numpy())
     return pool
 
 
@@ -662,7 +665,7 @@ def run_cube(args, torch, dev):
             u = sel[:, a0:b0].contiguous()
             chunks.append((u, torch.full((b0 - a0,), f / C_LIGHT, dtype=torch.float32, device=dev),
                            make_vis(u, f, srcs, torch, gen), ones[:b0 - a0],
-                           (torch.rand(b0 - a0, device=dev, generator=gen) < frac).int()[:, None].repeat(1, 4)
+                           (torch.rand(b0 - a0, device=dev, generator=gen) < frac).to(torch.uint8)[:, None].repeat(1, 4)
                            .contiguous()))
         images.append((im, chunks))
     del pool
@@ -846,7 +849,7 @@ def cpu_baseline(args, spec, uvw_d, chans, kern, dl, torch, min_seconds=12.0, ma
     fq = np.ascontiguousarray(freq[:n_rec].cpu().numpy())
     vs = np.ascontiguousarray(vis[:n_rec].cpu().numpy())
     wt = np.ascontiguousarray(weights[:n_rec].cpu().numpy())
-    fl = np.ascontiguousarray(flags[:n_rec].cpu().numpy())
+    fl = np.ascontiguousarray(flags[:n_rec].cpu().numpy(), dtype=np.int32)
     table = kern.table.cpu().numpy()
     sums = kern.conv_sums.cpu().numpy()
     ci = kern.conv_info
