@@ -296,7 +296,7 @@ def main():
     ap.add_argument("--serve-sample-requests", type=int, default=40,
                     help="requests of the shortened stream the default (mid-size) run measures")
     ap.add_argument("--serve-sample-max-records", type=float, default=5e6)
-    ap.add_argument("--serve-slots", type=int, default=4)
+    ap.add_argument("--serve-slots", type=int, default=8)
     ap.add_argument("--clock-log", default=None,
                     help="directory that keeps the nvidia-smi clock samples of the timed region")
     ap.add_argument("--profile-range", action="store_true",
@@ -790,8 +790,11 @@ def run_serve(args, torch, dev):
 
     results = []
     with Engine(slots=args.serve_slots) as eng:
-        for t in [submit(eng, r) for r in warm]:
-            eng.wait(t)
+        # every slot runs one request of every image size (slot buffers grow
+        # to the largest geometry; w-kernels and FFT plans built)
+        for r in warm:
+            for t in [submit(eng, r) for _ in range(args.serve_slots)]:
+                eng.wait(t)
         tickets = queue.Queue()
 
         def waiter():
@@ -823,8 +826,9 @@ def run_serve(args, torch, dev):
     return {
         "requests": len(reqs), "arrival_rate_per_s": args.serve_rate, "slots": args.serve_slots,
         "image_sizes": [512, 1024, 2048, 4096],
-        "warm_up": "one untimed request per image size through each path (engine: w-kernel cache resident, "
-                   "slot buffers grown; plain path: allocator and FFT plans warm, w-kernels rebuilt per request)",
+        "warm_up": "untimed requests of every image size through each path (engine: one per slot and size, so "
+                   "w-kernels are cached and every slot's buffers are grown; plain path: one per size, allocator "
+                   "and FFT plans warm, w-kernels rebuilt per request)",
         "records": {"min": int(min(recs)), "max": int(max(recs)), "total": int(sum(recs)),
                     "range": [args.serve_min_records, args.serve_max_records]},
         "engine": {"samples_per_s": samples_eng / span_eng, "p50_ms": float(np.percentile(lat_eng, 50)),
