@@ -13,8 +13,16 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 PKG = os.path.dirname(HERE)
 LIB_PATH = os.path.join(PKG, "libmtb.so")
 
+# status codes (include/mtb.h)
 MTB_OK = 0
+MTB_ERR_BAD_PARAM = 1
+MTB_ERR_BAD_SHAPE = 2
+MTB_ERR_WORKSPACE = 3
 MTB_ERR_CAPACITY = 4
+MTB_ERR_CUDA = 5
+MTB_ERR_CUFFT = 6
+MTB_ERR_KERNEL = 7
+MTB_ERR_NULL = 8
 MTB_ERR_TOO_LARGE = 9
 MTB_POL_LINEAR = 0
 MTB_POL_CIRCULAR = 1

@@ -1,0 +1,91 @@
+"""Every struct the Python binding passes across the C ABI has the size and
+field offsets the C headers give it (a C program compiled with gcc against
+include/*.h prints them), and host-side parameter checks refuse bad input
+before any CUDA call.  No GPU."""
+import ctypes
+import os
+import subprocess
+
+import pytest
+
+from mtb import _lib as L
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+STRUCTS = {
+    "mtb_wkernel_params": L.WKernelParams,
+    "mtb_wkernel_info": L.WKernelInfo,
+    "mtb_grid_params": L.GridParams,
+    "mtb_grid_stats": L.GridStats,
+    "mtb_finalize_params": L.FinalizeParams,
+    "mtb_grid_job": L.GridJob,
+    "mtb_grid_tuning": L.GridTuning,
+    "mtb_fits_header": L.FitsHeader,
+    "mtb_engine_config": L.EngineConfig,
+    "mtb_image_request": L.ImageRequest,
+    "mtb_image_result": L.ImageResult,
+}
+
+
+@pytest.fixture(scope="module")
+def c_layouts(tmp_path_factory):
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "mtb.h"', '#include "mtb_engine.h"',
+             '#include "mtb_fits.h"', 'int main(void) {']
+    for cname, py in STRUCTS.items():
+        lines.append('printf("%s size %%zu\\n", sizeof(%s));' % (cname, cname))
+        for f, _ in py._fields_:
+            lines.append('printf("%s %s %%zu\\n", offsetof(%s, %s));' % (cname, f, cname, f))
+    lines += ['return 0;', '}']
+    d = tmp_path_factory.mktemp("abi")
+    src, exe = d / "layout.c", d / "layout"
+    src.write_text("\n".join(lines))
+    subprocess.run(["gcc", "-std=c11", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    out = {}
+    for line in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.splitlines():
+        a, b, v = line.split()
+        out[(a, b)] = int(v)
+    return out
+
+
+@pytest.mark.parametrize("cname", sorted(STRUCTS))
+def test_struct_matches_header(c_layouts, cname):
+    py = STRUCTS[cname]
+    assert ctypes.sizeof(py) == c_layouts[(cname, "size")], cname
+    for f, _ in py._fields_:
+        assert getattr(py, f).offset == c_layouts[(cname, f)], (cname, f)
+
+
+def test_autotune_refuses_images_that_are_not_fresh(mtblib):
+    jobs = (L.GridJob * 1)()
+    jobs[0].params.initialize_output = 0
+    best = L.GridTuning()
+    rc = mtblib.mtb_grid_autotune(jobs, 1, None, 0, None, ctypes.byref(best), None)
+    assert rc == L.MTB_ERR_BAD_PARAM
+    assert mtblib.mtb_grid_autotune(jobs, 0, None, 0, None, ctypes.byref(best), None) == L.MTB_ERR_BAD_SHAPE
+    n = ctypes.c_size_t(0)
+    assert mtblib.mtb_grid_autotune_workspace_size(jobs, 65, ctypes.byref(n)) == L.MTB_ERR_BAD_SHAPE
+
+
+def test_batch_refuses_mixed_gridder_block_sizes(mtblib):
+    jobs = (L.GridJob * 2)()
+    info = (ctypes.c_int * 2)(7, 0)
+    for j, thr in enumerate((256, 512)):
+        p = jobs[j].params
+        p.nx = p.ny = 64
+        p.npol, p.sampling, p.wplanes = 4, 4, 1
+        p.u_increment = p.v_increment = p.w_sq_increment = 1.0
+        p.gridder_threads = thr
+        jobs[j].h_conv_info = ctypes.cast(info, ctypes.c_void_p)
+    n = ctypes.c_size_t(0)
+    assert mtblib.mtb_grid_batch_workspace_size(jobs, 2, ctypes.byref(n)) == L.MTB_ERR_BAD_PARAM
+    jobs[1].params.gridder_threads = 300
+    assert mtblib.mtb_grid_batch_workspace_size(jobs, 2, ctypes.byref(n)) == L.MTB_ERR_BAD_PARAM
+
+
+def test_status_codes_match_header():
+    import re
+    src = open(os.path.join(ROOT, "include", "mtb.h")).read()
+    codes = {m.group(1): int(m.group(2)) for m in re.finditer(r"\b(MTB_(?:OK|ERR_\w+))\s*=\s*(\d+)", src)}
+    assert len(codes) == 10
+    for name, v in codes.items():
+        assert getattr(L, name) == v, name
