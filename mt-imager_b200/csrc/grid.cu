@@ -669,44 +669,65 @@ __device__ __forceinline__ int pick_streams(int U, int N, int T) {
 // Row-padded copy of the kernel table for the direct gridders: every
 // sub-kernel row gets one zero tap (S + 1 taps, S odd), so each row and each
 // sub-kernel starts on a 16-byte boundary and rows can be moved with bulk
-// copies.  pbase[k] = first padded element of plane k.
+// copies.  pbase[k] = first padded element of plane k; pbase[nw + k] = first
+// row (of S taps) of plane k, pbase[2 nw] = every plane's rows.
 __global__ void k_pad_bases(const int *__restrict__ conv_info, int nw, int T, int *__restrict__ pbase) {
     if (blockIdx.x == 0 && threadIdx.x == 0) {
-        int b = 0;
+        int b = 0, rows = 0;
         for (int k = 0; k < nw; k++) {
             pbase[k] = b;
+            pbase[nw + k] = rows;
             const int S = conv_info[2 * k];
             b += T * T * S * (S + 1);
+            rows += T * T * S;
         }
+        pbase[2 * nw] = rows;
     }
 }
 
-__global__ void k_pad_table(const float2 *__restrict__ t, size_t n, const int *__restrict__ conv_info,
-                            const int *__restrict__ pbase, int nw, float2 *__restrict__ pt) {
-    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
-        int lo = 0, hi = nw - 1;
-        while (lo < hi) {
-            int mid = (lo + hi + 1) >> 1;
-            if ((size_t)__ldg(&conv_info[2 * mid + 1]) <= e) lo = mid;
-            else hi = mid - 1;
-        }
-        const int S = __ldg(&conv_info[2 * lo]);
-        const size_t rel = e - (size_t)__ldg(&conv_info[2 * lo + 1]);
-        const size_t S2 = (size_t)S * S;
-        const size_t sub = rel / S2, w = rel % S2;
-        const int y = (int)(w / S), x = (int)(w % S);
-        const size_t dst = (size_t)__ldg(&pbase[lo]) + sub * S * (S + 1) + (size_t)y * (S + 1) + x;
-        pt[dst] = t[e];
-        if (x == S - 1) pt[dst + 1] = make_float2(0.f, 0.f);
+// Row-padded, expanded table in one pass: each warp copies a contiguous range
+// of kernel rows (S taps of one sub-kernel row each), so the plane is found
+// once per warp and then followed across plane boundaries.  t2 gets every tap
+// as {re, re, im, im} (one 128-bit load gives both packed operands of the
+// f32x2 complex multiply-add) with a zero tap closing each row; pt (when not
+// null) gets the same rows compact (the bulk-copy gridder reads those).
+__global__ void k_pad_expand(const float2 *__restrict__ t, const int *__restrict__ conv_info,
+                             const int *__restrict__ pbase, int nw, int rows, float2 *__restrict__ pt,
+                             float4 *__restrict__ t2) {
+    const int lane = threadIdx.x & 31;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int per = (rows + nwarps - 1) / nwarps;
+    const int r0 = warp * per, r1 = min(rows, r0 + per);
+    if (r0 >= r1) return;
+    const int *rbase = pbase + nw;
+    int lo = 0, hi = nw - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(&rbase[mid]) <= r0) lo = mid;
+        else hi = mid - 1;
     }
-}
-
-// {re, re, im, im} copy of the table: one 128-bit load gives both packed
-// operands of the f32x2 complex multiply-add
-__global__ void k_expand_table(const float2 *__restrict__ t, float4 *__restrict__ t2, size_t n) {
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-        float2 c = t[i];
-        t2[i] = make_float4(c.x, c.x, c.y, c.y);
+    int k = lo;
+    int S = __ldg(&conv_info[2 * k]), rb = __ldg(&rbase[k]), next = __ldg(&rbase[k + 1]);
+    size_t cbase = (size_t)__ldg(&conv_info[2 * k + 1]), pb = (size_t)__ldg(&pbase[k]);
+    for (int row = r0; row < r1; row++) {
+        while (row >= next) {     // next plane (rbase[nw] is the total, so this ends)
+            k++;
+            S = __ldg(&conv_info[2 * k]);
+            rb = next;
+            next = __ldg(&rbase[k + 1]);
+            cbase = (size_t)__ldg(&conv_info[2 * k + 1]);
+            pb = (size_t)__ldg(&pbase[k]);
+        }
+        const int rel = row - rb;        // sub * S + y
+        const int sub = rel / S, y = rel - sub * S;
+        const size_t src = cbase + (size_t)rel * S;
+        const size_t dst = pb + (size_t)sub * S * (S + 1) + (size_t)y * (S + 1);
+        for (int x = lane; x <= S; x += 32) {
+            const float2 c = x < S ? t[src + x] : make_float2(0.f, 0.f);
+            t2[dst + x] = make_float4(c.x, c.x, c.y, c.y);
+            if (pt) pt[dst + x] = c;
+        }
     }
 }
 
@@ -1300,7 +1321,8 @@ __global__ void k_merge_delta(float2 *__restrict__ hi, float2 *__restrict__ lo, 
 struct GridPlan {
     BucketTable bt;
     int chunk;
-    int ncap;      // record capacity of per-record arrays
+    int ncap;        // record capacity of per-record arrays
+    int table_rows;  // kernel rows (S taps each) of all planes: sum of T*T*S
 };
 
 struct GridSpace {
@@ -1320,7 +1342,7 @@ struct GridSpace {
     size_t cub_bytes;
     float2 *ptab;        // row-padded copy of the table (rows of S + 1 taps)
     float4 *table2;      // padded table with each tap as {re, re, im, im} (k_grid3)
-    int *pbase;          // first padded element of every plane
+    int *pbase;          // first padded element, then first row, of every plane (k_pad_bases)
     int *moduli;         // bucket moduli of the plan (device copy)
     int *split;          // first work item of k_grid4
     int *counter4;       // k_grid4 work counter
@@ -1366,7 +1388,7 @@ static void carve_grid(Arena &A, int R, int P, int chunk, size_t table_elems, si
     s->cub = A.take<char>(s->cub_bytes);
     s->ptab = A.take<float2>(table_elems ? table_elems : 1);
     s->table2 = A.take<float4>(table_elems ? table_elems : 1);
-    s->pbase = A.take<int>(nw > 0 ? nw : 1);
+    s->pbase = A.take<int>(2 * (nw > 0 ? nw : 1) + 1);
     s->moduli = A.take<int>(kMaxBuckets);
     s->split = A.take<int>(1);
     s->counter4 = A.take<int>(1);
@@ -1421,8 +1443,11 @@ static int make_plan(const mtb_grid_params *p, const int *h_conv_info, GridPlan 
     if (tile < 4 || p->nx / tile >= 4096 || p->ny / tile >= 4096) return MTB_ERR_BAD_PARAM;
     std::memset(&g->bt, 0, sizeof(g->bt));
     g->bt.half = half;
+    const long long T = oversample_T(p->sampling);
+    long long rows = 0;
     for (int k = 0; k < p->wplanes; k++) {
         int S = h_conv_info[2 * k];
+        rows += T * T * S;
         // the direct gridders lay one support-box column per thread of a
         // 256-thread block: supports up to 255
         if (S < 1 || S % 2 == 0 || S > 255 || S >= p->nx || S >= p->ny) return MTB_ERR_KERNEL;
@@ -1432,6 +1457,8 @@ static int make_plan(const mtb_grid_params *p, const int *h_conv_info, GridPlan 
         g->bt.n = std::max(g->bt.n, b + 1);
     }
     for (int b = 0; b < kMaxBuckets; b++) g->bt.tile[b] = tile;
+    if (rows > 0x7FFFFFFFLL) return MTB_ERR_BAD_SHAPE;
+    g->table_rows = (int)rows;
     return MTB_OK;
 }
 
@@ -1576,12 +1603,14 @@ static int prepare_grid(const mtb_grid_params *p, const GridPlan &plan, const fl
     MTB_LAUNCHED();
     (void)end_bit;
     {
-        int eb = (int)std::min<size_t>((table_elems + 255) / 256, (size_t)sms * 16);
-        k_pad_table<<<eb > 0 ? eb : 1, 256, 0, st>>>(table, table_elems, conv_info, s.pbase, p->wplanes, s.ptab);
+        // compact padded rows only for the bulk-copy gridder
+        float2 *pt = p->bulk_min_support > 0 ? s.ptab : nullptr;
+        const int rows = plan.table_rows;
+        const int pb = (int)std::min<size_t>(((size_t)rows + 7) / 8, (size_t)sms * 16);
+        k_pad_expand<<<pb > 0 ? pb : 1, 256, 0, st>>>(table, conv_info, s.pbase, p->wplanes, rows, pt, s.table2);
         MTB_LAUNCHED();
-        int pb = (int)std::min<size_t>((padded + 255) / 256, (size_t)sms * 16);
-        k_expand_table<<<pb > 0 ? pb : 1, 256, 0, st>>>(s.ptab, s.table2, padded);
-        MTB_LAUNCHED();
+        (void)table_elems;
+        (void)padded;
     }
     k_set_moduli<<<1, 32, 0, st>>>(plan.bt, s.moduli);
     MTB_LAUNCHED();
