@@ -442,8 +442,12 @@ def main():
             "mtb_calibrate_fp32")
     gridder_ms = float(np.mean(gms))
     achieved = flops_per_step / (gridder_ms * 1e-3) / 1e12
+    # DRAM bytes of one gridder launch of this workload's channel, measured with
+    # ncu (profiles/k_grid3_mid4096_8h_dram.md); other workloads: not captured
+    traffic = 4.90e9 if (spec["name"] == "mid" and spec["hours"] == 8.0 and R == 29030400) else None
     roof = {"bound": "fp32", "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
-            "frac": achieved / peak.value if peak.value else None, "traffic": None,
+            "frac": achieved / peak.value if peak.value else None, "traffic": traffic,
+            "traffic_unit": "bytes per gridder launch (one channel), ncu dram__bytes_read+write",
             "kernel": "k_grid (all support buckets of one mtb_grid call, span timed by events)",
             "peak_source": "measured: mtb_calibrate_fp32 (packed f32x2 FMA chains, this GPU)"}
 
