@@ -442,8 +442,9 @@ def main():
             "mtb_calibrate_fp32")
     gridder_ms = float(np.mean(gms))
     achieved = flops_per_step / (gridder_ms * 1e-3) / 1e12
-    # DRAM bytes of one gridder launch of this workload's channel, measured with
-    # ncu (profiles/k_grid3_mid4096_8h_dram.md); other workloads: not captured
+    # DRAM bytes of one gridder launch of this workload's channel (8 h, 4096^2),
+    # measured with ncu (dram__bytes_read.sum + dram__bytes_write.sum, 1 pass);
+    # other workloads were not captured
     traffic = 4.90e9 if (spec["name"] == "mid" and spec["hours"] == 8.0 and R == 29030400) else None
     roof = {"bound": "fp32", "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
             "frac": achieved / peak.value if peak.value else None, "traffic": traffic,
