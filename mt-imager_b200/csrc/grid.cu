@@ -563,21 +563,6 @@ struct Grid2Args {
     GridJobDesc jobs[kMaxBatch];
 };
 
-typedef unsigned long long u64;
-__device__ __forceinline__ u64 pk2(float a, float b) {
-    u64 r;
-    asm("mov.b64 %0, {%1,%2};" : "=l"(r) : "f"(a), "f"(b));
-    return r;
-}
-__device__ __forceinline__ float2 upk2(u64 v) {
-    float2 r;
-    asm("mov.b64 {%0,%1}, %2;" : "=f"(r.x), "=f"(r.y) : "l"(v));
-    return r;
-}
-__device__ __forceinline__ void ffma2(u64 &acc, u64 a, u64 b) {
-    asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(acc) : "l"(a), "l"(b));
-}
-
 __device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
     unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sa), "l"(gmem) : "memory");
@@ -615,18 +600,6 @@ __device__ __forceinline__ void flush2(float *grid, double *dgrid, int cell, con
     for (int p = 0; p < P; p++) {
         v[2 * p] = acc[p].x;
         v[2 * p + 1] = acc[p].y;
-    }
-    flush_cell<P>(grid, dgrid, cell, v);
-}
-
-template <int P>
-__device__ __forceinline__ void flush2(float *grid, double *dgrid, int cell, const u64 *acc) {
-    float v[2 * P];
-#pragma unroll
-    for (int p = 0; p < P; p++) {
-        float2 f = upk2(acc[p]);
-        v[2 * p] = f.x;
-        v[2 * p + 1] = f.y;
     }
     flush_cell<P>(grid, dgrid, cell, v);
 }
@@ -1035,11 +1008,11 @@ __device__ __forceinline__ void bulk_g2s(unsigned dst, const void *src, unsigned
 }
 
 template <int P>
-__device__ __forceinline__ void flush_ab(float *grid, double *dgrid, int cell, const u64 *A, const u64 *B) {
+__device__ __forceinline__ void flush_ab(float *grid, double *dgrid, int cell, const float2 *A, const float2 *B) {
     float v[2 * P];
 #pragma unroll
     for (int p = 0; p < P; p++) {
-        const float2 fa = upk2(A[p]), fb = upk2(B[p]);
+        const float2 fa = A[p], fb = B[p];
         v[2 * p] = fa.x - fa.y;
         v[2 * p + 1] = fb.y - fb.x;
     }
@@ -1163,13 +1136,13 @@ __global__ void __launch_bounds__(kG4Threads, 1) k_grid4(Grid4Args a) {
                     int keyx = -1, keyw = -1;
                     int last[KS];
                     unsigned off[KS];
-                    u64 A[KS][P], B[KS][P];
+                    float2 A[KS][P], B[KS][P];
 #pragma unroll
                     for (int j = 0; j < KS; j++) {
                         last[j] = -1;
                         off[j] = kG4ZeroOff;
 #pragma unroll
-                        for (int p = 0; p < P; p++) A[j][p] = B[j][p] = 0ull;
+                        for (int p = 0; p < P; p++) A[j][p] = B[j][p] = make_float2(0.f, 0.f);
                     }
                     bool ok = true;
                     for (int i = i0; i < i1; i++) {
@@ -1198,27 +1171,27 @@ __global__ void __launch_bounds__(kG4Threads, 1) k_grid4(Grid4Args a) {
                                     if (last[j] >= 0) flush_ab<P>(a.grid, a.dgrid, last[j], A[j], B[j]);
                                     last[j] = cell;
 #pragma unroll
-                                    for (int p = 0; p < P; p++) A[j][p] = B[j][p] = 0ull;
+                                    for (int p = 0; p < P; p++) A[j][p] = B[j][p] = make_float2(0.f, 0.f);
                                 }
                                 off[j] = valid ? (unsigned)(cs * sregion + ((r - r0) * Sp + sx) * 8)
                                                : (unsigned)kG4ZeroOff;
                             }
                         }
-                        u64 vp[P], wp[P];
+                        float2 vp[P], wp[P];
 #pragma unroll
                         for (int p = 0; p < P; p++) {
-                            const ulonglong2 q = s_v[(size_t)i * P + p];
-                            vp[p] = q.x;
-                            wp[p] = q.y;
+                            const float4 q = ((const float4 *)s_v)[(size_t)i * P + p];
+                            vp[p] = make_float2(q.x, q.y);
+                            wp[p] = make_float2(q.z, q.w);
                         }
                         const unsigned char *sb = ring + slot * kG4Slot;
 #pragma unroll
                         for (int j = 0; j < KS; j++) {
-                            const u64 c = *(const u64 *)(sb + off[j]);
+                            const float2 c = *(const float2 *)(sb + off[j]);
 #pragma unroll
                             for (int p = 0; p < P; p++) {
-                                ffma2(A[j][p], c, vp[p]);
-                                ffma2(B[j][p], c, wp[p]);
+                                A[j][p] = __ffma2_rn(c, vp[p], A[j][p]);
+                                B[j][p] = __ffma2_rn(c, wp[p], B[j][p]);
                             }
                         }
                         mbar_arrive(empty_sa + (slot * kG4MaxStreams + cs) * 8);
