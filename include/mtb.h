@@ -208,6 +208,27 @@ typedef struct mtb_grid_job {
 /* Workspace for mtb_grid_batch over these jobs. */
 int mtb_grid_batch_workspace_size(const mtb_grid_job *jobs, int njobs, size_t *bytes);
 
+/* ---------------------------------------------------------- ingest (host) */
+/* Record order of mt-imager's visibility ingest (code/mt-imager/lib/
+ * components/VisibilityManager/SortIndex.cpp:46-87): rows whose antenna1
+ * equals antenna2 (autocorrelations) are dropped, the rest are grouped by
+ * baseline number nA*nA - antenna1*nA - antenna2 - 1 ascending, and rows of
+ * one baseline keep their original order -- consecutive records of a
+ * baseline are what make the gridder's register accumulation and duplicate
+ * compression effective.  Host memory, no GPU.
+ *   index    out int [nrows] (the first *nsorted entries are written)
+ *   nsorted  out rows kept
+ * Antenna ids outside [0, nantennas) are refused with MTB_ERR_BAD_PARAM. */
+int mtb_sort_index(const int *antenna1, const int *antenna2, int nrows, int nantennas, int *index, int *nsorted);
+
+/* Applies a record order to one host column (SortedStorage.h:205-246):
+ * out[k] = the row_bytes bytes at in + index[k]*in_stride + offset, for
+ * k < n, split over host threads (threads 0: the hardware's, at most 16).
+ * With in_stride/offset it also picks one channel out of a [row][chan][pol]
+ * column or one coordinate out of a [row][3] uvw column. */
+int mtb_gather_rows(const void *in, size_t in_stride, size_t offset, size_t row_bytes, const int *index, int n,
+                    void *out, int threads);
+
 /* Gridder knobs the autotuner chooses among (fields of mtb_grid_params). */
 typedef struct mtb_grid_tuning {
     int tile;             /* bin tile edge                                            */

@@ -34,7 +34,7 @@ EXPORTS = (
     "mtb_finalize_workspace_size", "mtb_finalize", "mtb_status_string", "mtb_version",
     "mtb_release_caches", "mtb_kernel_launch_count", "mtb_calibrate_fp32",
     "mtb_taper_kernel_build", "mtb_grid_batch_workspace_size", "mtb_grid_batch",
-    "mtb_grid_autotune_workspace_size", "mtb_grid_autotune", "mtb_fits_create", "mtb_fits_write_channel", "mtb_fits_close",
+    "mtb_grid_autotune_workspace_size", "mtb_grid_autotune", "mtb_sort_index", "mtb_gather_rows", "mtb_fits_create", "mtb_fits_write_channel", "mtb_fits_close",
     "mtb_engine_create", "mtb_engine_submit", "mtb_engine_wait", "mtb_engine_request_bytes", "mtb_engine_destroy",
 )
 
@@ -154,6 +154,8 @@ def load(path: str = LIB_PATH):
     L.mtb_calibrate_fp32.argtypes = [ctypes.POINTER(ctypes.c_double), p]
     L.mtb_grid_batch_workspace_size.argtypes = [ctypes.POINTER(GridJob), i, ctypes.POINTER(sz)]
     L.mtb_grid_batch.argtypes = [ctypes.POINTER(GridJob), i, p, sz, p]
+    L.mtb_sort_index.argtypes = [p, p, i, i, p, ctypes.POINTER(i)]
+    L.mtb_gather_rows.argtypes = [p, sz, sz, sz, p, i, p, i]
     L.mtb_grid_autotune_workspace_size.argtypes = [ctypes.POINTER(GridJob), i, ctypes.POINTER(sz)]
     L.mtb_grid_autotune.argtypes = [ctypes.POINTER(GridJob), i, p, sz, p, ctypes.POINTER(GridTuning),
                                     ctypes.POINTER(GridTuning)]

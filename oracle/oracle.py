@@ -292,6 +292,19 @@ def stats(pre):
                 gridded_points=int((pre["togrid"] * s2).sum()), compressed_points=int((pre["compress"] * s2).sum()))
 
 
+# ----------------------------------------------------------------- ingest --
+def sort_index(antenna1, antenna2, n_antennas):
+    """Baseline-major record order of the visibility ingest
+    (code/mt-imager/lib/components/VisibilityManager/SortIndex.cpp:46-87):
+    autocorrelations dropped, rows grouped by nA*nA - a1*nA - a2 - 1
+    ascending, original order kept inside a baseline (a stable sort)."""
+    a1 = np.asarray(antenna1, np.int64)
+    a2 = np.asarray(antenna2, np.int64)
+    keep = np.flatnonzero(a1 != a2)
+    key = n_antennas * n_antennas - a1[keep] * n_antennas - a2[keep] - 1
+    return keep[np.argsort(key, kind="stable")].astype(np.int32)
+
+
 # --------------------------------------------------------------- finalize --
 def _idx(fn, n):
     return np.array([fn(i, n) for i in range(n)], np.int64)
