@@ -75,6 +75,29 @@ def test_alone_equals_in_mix():
     assert mixed[-1].kernel_cache_hit or mixed[0].kernel_cache_hit
 
 
+def test_host_copy_threads_and_uvw_slices():
+    """The host copy pool's width does not change an image, and a request
+    imaging a slice of a longer uvw array (uvw_row_stride) equals one given a
+    contiguous copy; images large enough to come back in several pieces."""
+    from mtb.engine import Engine
+    c = case(46, 2048, 4, nw=4, ntimes=30, cell=10.0)[0]
+    R = c["freq"].size
+    longer = np.zeros((3, R + 1000), np.float32)
+    longer[:, 500:500 + R] = c["uvw"]
+    sliced = dict(c, uvw=longer[:, 500:500 + R])
+    assert sliced["uvw"].strides[0] == 4 * (R + 1000)
+    imgs = []
+    for threads, cc in ((1, c), (6, c), (6, sliced)):
+        with Engine(slots=1, host_threads=threads, chunk_records=700) as e:
+            r = e.wait(submit(e, cc, exact_delta=True, trial_support=33, max_support=31))
+            assert r.status == 0
+            imgs.append(r.image.copy())
+    peak = np.abs(imgs[0][0]).max()
+    assert peak > 0
+    for im in imgs[1:]:
+        assert np.abs(im - imgs[0]).max() <= MIX_TOL * peak
+
+
 def test_empty_request_and_capacity():
     from mtb.engine import Engine
     c = case(45, 64, 4, nw=4)[0]
