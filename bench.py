@@ -510,8 +510,9 @@ def main():
 def run_e2e(args, torch, dev, uvw_d, chans, imagers, images, samples_per_step, world, dist):
     """Same metric through the public API from pinned host buffers: per step
     the H2D copy of every channel's records and the D2H of every image are
-    inside the timed region.  Copies run on a side stream, double-buffered
-    against the compute of the previous channel."""
+    inside the timed region.  H2D copies run on a side stream, double-buffered
+    against the compute of the previous channel; each image's D2H runs on a
+    third stream once it is finalised."""
     host_uvw = torch.empty(uvw_d.shape, dtype=uvw_d.dtype, pin_memory=True)
     host_uvw.copy_(uvw_d)
     host = []
@@ -526,6 +527,7 @@ def run_e2e(args, torch, dev, uvw_d, chans, imagers, images, samples_per_step, w
     bufs = [[torch.empty_like(t) for t in chans[0]] for _ in range(2)]
     uvw_buf = torch.empty_like(uvw_d)
     copy = torch.cuda.Stream(device=dev)
+    back = torch.cuda.Stream(device=dev)
     comp = torch.cuda.current_stream(dev)
     h2d = host_uvw.numel() * 4 + sum(sum(t.numel() * t.element_size() for t in hc) for hc in host)
     d2h = sum(o.numel() * 4 for o in out_host)
@@ -549,7 +551,13 @@ def run_e2e(args, torch, dev, uvw_d, chans, imagers, images, samples_per_step, w
             im.grid_device(uvw_buf, *b)
             free[c % 2].record(comp)
             im.finalize(out=images[c])
-            out_host[c].copy_(images[c], non_blocking=True)
+            # the image goes back on its own stream: the next channel's
+            # gridding does not wait for the read-back
+            done = torch.cuda.Event()
+            done.record(comp)
+            back.wait_event(done)
+            with torch.cuda.stream(back):
+                out_host[c].copy_(images[c], non_blocking=True)
         torch.cuda.synchronize()
 
     step()
