@@ -22,8 +22,8 @@
 //                  record summed over its compressed duplicates
 //                  (CompressVisibilties.cu:41-74), stored in bin order together
 //                  with the record's gridder layout.
-//   k_pad_table    row-padded copy of the kernel table (rows of S + 1 taps,
-//                  16-byte aligned) and k_expand_table its {re,re,im,im} form.
+//   k_pad_expand   row-padded copy of the kernel table (rows of S + 1 taps,
+//                  16-byte aligned), every tap in {re,re,im,im} form.
 //   k_grid3        default gridder: persistent blocks take work items (up to 512
 //                  records of one bin) from a queue.  Threads own support-box
 //                  positions (Romein's assignment: cell x belongs to the slot
@@ -248,7 +248,7 @@ __global__ void k_bucket_bounds(const int4 *__restrict__ items, const int *__res
 //                   bucket modulus M, and per pol {re, im, -im, re} (direct
 //                   gridders)
 // Index of a record's sub-kernel in the row-padded table (rows of S + 1
-// taps; see k_pad_table) from its conv index in the reference layout.
+// taps; see k_pad_expand) from its conv index in the reference layout.
 __device__ __forceinline__ int padded_index(int ci, int S, const int *__restrict__ conv_info,
                                             const int *__restrict__ pbase, int nw) {
     int lo = 0, hi = nw - 1;             // last plane whose first element is <= ci
