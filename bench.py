@@ -43,6 +43,15 @@ ARCSEC = math.pi / (180.0 * 3600.0)
 
 
 # ------------------------------------------------------------ replicas ----
+def host_available_bytes():
+    """Host memory available now (bytes)."""
+    try:
+        import psutil
+        return psutil.virtual_memory().available
+    except Exception:
+        return os.sysconf("SC_AVPHYS_PAGES") * os.sysconf("SC_PAGE_SIZE")
+
+
 def max_over_ranks(ms, world, dist, torch, device):
     """The slowest rank's time, returned on every rank (an all-reduce MAX;
     every rank takes this step in the same order)."""
@@ -455,7 +464,22 @@ def main():
     # ---- end to end: host buffers, H2D per channel overlapped with compute
     e2e = None
     if not args.no_e2e:
-        e2e = run_e2e(args, torch, dev, uvw, chans, imagers, images, samples_per_step, world, dist)
+        # every rank pins a host copy of its inputs and images; with several
+        # ranks on one host that can exceed its memory: all ranks skip the leg
+        # (the same decision on every rank) when the node's share is too small
+        pinned = uvw.numel() * 4 + sum(sum(t.numel() * t.element_size() for t in ch) for ch in chans) + \
+            sum(im.numel() * 4 for im in images)
+        local_ranks = int(os.environ.get("LOCAL_WORLD_SIZE", str(world)))
+        fits = pinned * local_ranks <= 0.6 * host_available_bytes()
+        if world > 1:
+            flag = torch.tensor([1 if fits else 0], device=dev)
+            dist.all_reduce(flag, op=dist.ReduceOp.MIN)
+            fits = bool(flag.item())
+        if fits:
+            e2e = run_e2e(args, torch, dev, uvw, chans, imagers, images, samples_per_step, world, dist)
+        else:
+            e2e = {"value": None, "skipped": "pinned host copies of %d ranks (%.0f GB) exceed 60 %% of the host's "
+                                          "available memory" % (local_ranks, pinned * local_ranks / 1e9)}
 
     # ---- CPU baseline (rank 0, one GPU)
     cpu = None
