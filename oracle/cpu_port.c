@@ -27,6 +27,17 @@ int port_threads(void)
 #endif
 }
 
+/* Threads of the following parallel regions (a launcher may have set
+ * OMP_NUM_THREADS=1 for every process). */
+void port_set_threads(int n)
+{
+#ifdef _OPENMP
+    if (n > 0) omp_set_num_threads(n);
+#else
+    (void)n;
+#endif
+}
+
 /* vis, grid: float complex interleaved.  stats[4]: gridded, compressed
  * records, gridded, compressed points.  Returns 0. */
 int port_grid_chunk(int R, int P, const float *uvw, const float *freq, const float *vis,

@@ -94,6 +94,10 @@ def port():
         P = ctypes.CDLL(path)
         i, p, f = ctypes.c_int, ctypes.c_void_p, ctypes.c_float
         P.port_threads.restype = i
+        P.port_set_threads.restype = None
+        P.port_set_threads.argtypes = [i]
+        # every core this process may run on, whatever OMP_NUM_THREADS says
+        P.port_set_threads(len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count())
         P.port_grid_chunk.restype = i
         P.port_grid_chunk.argtypes = [i, i, p, p, p, p, p, i, f, p, p, p, i, i, i, f, f, p, p, p]
         _port = P
