@@ -155,6 +155,9 @@ typedef struct mtb_grid_params {
                                   (order-independent, about half the grid error, slower)   */
     int gridder_threads;       /* 0: 256; threads of a gridder block, which grids one work
                                   item at a time (256 or 512)                              */
+    int gridder;               /* 0 or 3: k_grid3 (block-wide staging of each work item);
+                                  5: k_grid5 (two item buffers refilled by one warp, no
+                                  block barriers; items of at most 256 records)           */
     int flags_u8;              /* 0: d_flags is int32 [R][P] (the reference's layout); 1: it
                                   is one byte per flag, uint8 [R][P] (0 = keep, 1 = flagged;
                                   a quarter of the bytes to move), passed cast to int *    */
@@ -235,18 +238,20 @@ typedef struct mtb_grid_tuning {
     int support_bucket;   /* odd supports per bin bucket                              */
     int max_chunk;        /* records per work item                                    */
     int gridder_threads;  /* threads per gridder block (one work item at a time)      */
+    int gridder;          /* 3: block-staged items, 5: rolling items (mtb_grid_params) */
     float ms;             /* measured time of one mtb_grid_batch call with these knobs */
 } mtb_grid_tuning;
 
 /* Autotuner.  No counterpart in the reference, whose gridder launch shapes are
  * fixed.  Grids the jobs (as mtb_grid_batch) once with every candidate of
- * tile {16, 32, 64} x support_bucket {1, 2} x max_chunk {256, 512} x
- * gridder_threads {256, 512}, times each call with CUDA events on `stream`
- * (after one untimed call), and writes the fastest to *best and to every
- * job's params.  Every job must start a fresh image (initialize_output = 1):
- * the grids, normalisers and statistics hold the result of a call with the
- * chosen knobs when it returns.  Synchronises `stream` after every call.
- * `candidates` (may be NULL) receives all 24 timings.  Workspace:
+ * tile {16, 32, 64} x support_bucket {1, 2} x five gridder shapes (gridder 3
+ * with max_chunk {256, 512} x gridder_threads {256, 512}, and gridder 5 with
+ * 256-record items and 256 threads), times each call with CUDA events on
+ * `stream` (after one untimed call), and writes the fastest to *best and to
+ * every job's params.  Every job must start a fresh image (initialize_output
+ * = 1): the grids, normalisers and statistics hold the result of a call with
+ * the chosen knobs when it returns.  Synchronises `stream` after every call.
+ * `candidates` (may be NULL) receives all 30 timings.  Workspace:
  * mtb_grid_autotune_workspace_size. */
 int mtb_grid_autotune_workspace_size(const mtb_grid_job *jobs, int njobs, size_t *bytes);
 int mtb_grid_autotune(mtb_grid_job *jobs, int njobs, void *d_workspace, size_t workspace_bytes,

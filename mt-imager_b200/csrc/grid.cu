@@ -704,13 +704,147 @@ __global__ void k_pad_expand(const float2 *__restrict__ t, const int *__restrict
     }
 }
 
-// Direct gridder with asynchronous staging.  A work item's records (already in
-// the gridder layout) are copied to shared memory with 16-byte cp.async; each
-// thread then fetches the kernel values of its slots kG3Depth records ahead
-// into its own entries of a shared-memory ring (cp.async, completion tracked
-// per thread with commit/wait groups, so no block barrier per record).  A slot
-// outside a record's support box gets zeros in its ring entry, which keeps the
-// accumulation loop free of per-slot branches.
+// The jobs of one work item for this thread (the direct gridders k_grid3 and
+// k_grid5): the item's records, visibilities and run ends are staged in
+// shared memory.  Each thread fetches the kernel values of its slots
+// kG3Depth records ahead into its own entries of a shared-memory ring
+// (cp.async, completion tracked per thread with commit/wait groups, so no
+// block barrier per record).  A slot outside a record's support box gets
+// zeros in its ring entry, which keeps the accumulation loop free of
+// per-slot branches.
+template <int P, int T>
+__device__ __forceinline__ void grid_item(const Grid2Args &a, const int4 it, const int4 *s_rec, const float4 *s_v,
+                                          const unsigned short *s_runend, ulonglong2 *ring) {
+    constexpr int KS = kG3KS, D = kG3Depth;
+    const int t = threadIdx.x;
+    const GridJobDesc &J = a.jobs[it.w];
+    const ulonglong2 *tab = (const ulonglong2 *)J.table2;
+    float *const ggrid = J.grid;
+    double *const gdelta = J.dgrid;
+    const int gnx = J.nx;
+    const int N = it.y;
+    const int M = J.M[(unsigned)it.z >> 24];
+    const int G = (M + KS - 1) / KS;
+    const int U = M * G;
+    const int ns = pick_streams(U, N, T);
+    const int njobs = ns * U;
+    for (int job = t; job < njobs; job += T) {
+        const int stream = job / U;
+        const int u = job - stream * U;
+        const int g = u / M;
+        const int col = u - g * M;
+        const int i0 = (N * stream) / ns;
+        const int i1 = (N * (stream + 1)) / ns;
+        // rows g + j*G that exist: j < nrow
+        const int nrow = (M - g + G - 1) / G;
+        if (i0 >= i1) continue;
+        // Slot geometry depends only on the record's corner and support;
+        // vbytes = 0 marks a slot outside the record's box.
+        auto geometry = [&](const int4 &rec, int *cell, int *toff, int *vbytes) {
+            const int S = rec.w;
+            int sx = col + (rec.y & 0xFFFF);
+            sx -= (sx >= M) ? M : 0;
+            int sy = g + (rec.y >> 16);
+            sy -= (sy >= M) ? M : 0;
+            const bool xok = sx < S;
+#pragma unroll
+            for (int j = 0; j < KS; j++) {
+                const bool ok = xok && (j < nrow) && (sy < S);
+                cell[j] = ok ? rec.x + sy * gnx + sx : -1;
+                toff[j] = ok ? sy * (S + 1) + sx : 0;
+                vbytes[j] = ok ? 16 : 0;
+                sy += G;
+                sy -= (sy >= M) ? M : 0;
+            }
+        };
+        // Look-ahead: the kernel values of record k go to ring slot k % D;
+        // the geometry is recomputed when k enters a new run (k == pend).
+        int pend = i0, toffL[KS], cellL[KS], vbL[KS];
+        const unsigned ring_s = (unsigned)__cvta_generic_to_shared(ring) + t * 16;
+        auto prefetch = [&](int k) {
+            if (k == pend) {
+                geometry(s_rec[k], cellL, toffL, vbL);
+                const int e = s_runend[k];
+                pend = e < i1 ? e : i1;
+            }
+            const int z = s_rec[k].z;
+            const unsigned dst = ring_s + (unsigned)(k & (D - 1)) * (KS * T * 16);
+            // slots outside the box get zeros (toff = 0 keeps the address valid)
+#pragma unroll
+            for (int j = 0; j < KS; j++) cp_async16_zfill_n(dst + j * (T * 16), tab + (z + toffL[j]), vbL[j]);
+        };
+#pragma unroll
+        for (int d = 0; d < D; d++) {
+            if (i0 + d < i1) prefetch(i0 + d);
+            cp_async_commit();
+        }
+        int last[KS];
+        float2 acc[KS][P];
+#pragma unroll
+        for (int j = 0; j < KS; j++) {
+            last[j] = -1;
+#pragma unroll
+            for (int p = 0; p < P; p++) acc[j][p] = make_float2(0.f, 0.f);
+        }
+        // Runs of records with the same corner and support: the flushes sit
+        // between runs, so the accumulators stay in place inside a run.
+        int i = i0;
+        while (i < i1) {
+            {
+                // corner or support changed: flush the slots whose cell changes
+                int cellN[KS], toffN[KS], vN[KS];
+                geometry(s_rec[i], cellN, toffN, vN);
+#pragma unroll
+                for (int j = 0; j < KS; j++) {
+                    if (cellN[j] >= 0 && cellN[j] != last[j]) {
+                        if (last[j] >= 0) flush2<P>(ggrid, gdelta, last[j], acc[j]);
+                        last[j] = cellN[j];
+#pragma unroll
+                        for (int p = 0; p < P; p++) acc[j][p] = make_float2(0.f, 0.f);
+                    }
+                }
+            }
+            const int e = s_runend[i];
+            const int re = e < i1 ? e : i1;
+            for (; i < re; ++i) {
+                // the visibilities were staged before the item started: load
+                // them ahead of the wait so their latency overlaps it
+                float2 vp[P], wp[P];
+                const float4 *vr = s_v + i * P;
+#pragma unroll
+                for (int p = 0; p < P; p++) {
+                    const float4 q = vr[p];
+                    vp[p] = make_float2(q.x, q.y);
+                    wp[p] = make_float2(q.z, q.w);
+                }
+                cp_async_wait<D - 1>();     // this thread's copies for record i have landed
+                const float4 *src = (const float4 *)(ring + ((i & (D - 1)) * KS * T + t));
+#pragma unroll
+                for (int j = 0; j < KS; j++) {
+                    const float4 c = src[j * T];
+                    const float2 cre = make_float2(c.x, c.y), cim = make_float2(c.z, c.w);
+                    // ConvolutionGridder.cu:153-181: to += vis * wt (no conjugate)
+#pragma unroll
+                    for (int p = 0; p < P; p++) {
+                        acc[j][p] = __ffma2_rn(cre, vp[p], acc[j][p]);
+                        acc[j][p] = __ffma2_rn(cim, wp[p], acc[j][p]);
+                    }
+                }
+                if (i + D < i1) prefetch(i + D);
+                cp_async_commit();
+            }
+        }
+        cp_async_wait<0>();
+#pragma unroll
+        for (int j = 0; j < KS; j++)
+            if (last[j] >= 0) flush2<P>(ggrid, gdelta, last[j], acc[j]);
+    }
+}
+
+// Direct gridder with block-wide staging: the block takes a work item from
+// the queue, copies its records (already in the gridder layout) and
+// visibilities to shared memory with 16-byte cp.async, marks the runs, and
+// every thread grids its jobs of the item.
 template <int P, int T>
 __global__ void __launch_bounds__(T, 512 / T) k_grid3(Grid2Args a) {
     extern __shared__ uint4 smem3[];
@@ -723,7 +857,6 @@ __global__ void __launch_bounds__(T, 512 / T) k_grid3(Grid2Args a) {
     const int t = threadIdx.x;
     const int lane = t & 31;
     const int nitems = a.n_items[0];
-    constexpr int KS = kG3KS, D = kG3Depth;
     for (;;) {
         __syncthreads();
         if (t == 0) s_item = atomicAdd(a.counter, 1);
@@ -732,12 +865,8 @@ __global__ void __launch_bounds__(T, 512 / T) k_grid3(Grid2Args a) {
         if (v >= nitems) break;
         const int4 it = a.items[v];
         const GridJobDesc &J = a.jobs[it.w];
-        const ulonglong2 *tab = (const ulonglong2 *)J.table2;
         const int4 *grec = J.wpos;
         const float4 *gvis = J.wvis4;
-        float *const ggrid = J.grid;
-        double *const gdelta = J.dgrid;
-        const int gnx = J.nx;
         const int N = it.y;
         // stage the item's records (gridder layout, 16-byte pieces)
         for (int k = t; k < N; k += T) cp_async16(&s_rec[k], &grec[it.x + k]);
@@ -767,122 +896,7 @@ __global__ void __launch_bounds__(T, 512 / T) k_grid3(Grid2Args a) {
             s_runend[k] = (unsigned short)(m == 0 ? N : (w << 5) + __ffs(m) - 1);
         }
         __syncthreads();
-        const int M = J.M[(unsigned)it.z >> 24];
-        const int G = (M + KS - 1) / KS;
-        const int U = M * G;
-        const int ns = pick_streams(U, N, T);
-        const int njobs = ns * U;
-        for (int job = t; job < njobs; job += T) {
-            const int stream = job / U;
-            const int u = job - stream * U;
-            const int g = u / M;
-            const int col = u - g * M;
-            const int i0 = (N * stream) / ns;
-            const int i1 = (N * (stream + 1)) / ns;
-            // rows g + j*G that exist: j < nrow
-            const int nrow = (M - g + G - 1) / G;
-            if (i0 >= i1) continue;
-            // Slot geometry depends only on the record's corner and support;
-            // vbytes = 0 marks a slot outside the record's box.
-            auto geometry = [&](const int4 &rec, int *cell, int *toff, int *vbytes) {
-                const int S = rec.w;
-                int sx = col + (rec.y & 0xFFFF);
-                sx -= (sx >= M) ? M : 0;
-                int sy = g + (rec.y >> 16);
-                sy -= (sy >= M) ? M : 0;
-                const bool xok = sx < S;
-#pragma unroll
-                for (int j = 0; j < KS; j++) {
-                    const bool ok = xok && (j < nrow) && (sy < S);
-                    cell[j] = ok ? rec.x + sy * gnx + sx : -1;
-                    toff[j] = ok ? sy * (S + 1) + sx : 0;
-                    vbytes[j] = ok ? 16 : 0;
-                    sy += G;
-                    sy -= (sy >= M) ? M : 0;
-                }
-            };
-            // Look-ahead: the kernel values of record k go to ring slot k % D;
-            // the geometry is recomputed when k enters a new run (k == pend).
-            int pend = i0, toffL[KS], cellL[KS], vbL[KS];
-            const unsigned ring_s = (unsigned)__cvta_generic_to_shared(ring) + t * 16;
-            auto prefetch = [&](int k) {
-                if (k == pend) {
-                    geometry(s_rec[k], cellL, toffL, vbL);
-                    const int e = s_runend[k];
-                    pend = e < i1 ? e : i1;
-                }
-                const int z = s_rec[k].z;
-                const unsigned dst = ring_s + (unsigned)(k & (D - 1)) * (KS * T * 16);
-                // slots outside the box get zeros (toff = 0 keeps the address valid)
-#pragma unroll
-                for (int j = 0; j < KS; j++) cp_async16_zfill_n(dst + j * (T * 16), tab + (z + toffL[j]), vbL[j]);
-            };
-#pragma unroll
-            for (int d = 0; d < D; d++) {
-                if (i0 + d < i1) prefetch(i0 + d);
-                cp_async_commit();
-            }
-            int last[KS];
-            float2 acc[KS][P];
-#pragma unroll
-            for (int j = 0; j < KS; j++) {
-                last[j] = -1;
-#pragma unroll
-                for (int p = 0; p < P; p++) acc[j][p] = make_float2(0.f, 0.f);
-            }
-            // Runs of records with the same corner and support: the flushes sit
-            // between runs, so the accumulators stay in place inside a run.
-            int i = i0;
-            while (i < i1) {
-                {
-                    // corner or support changed: flush the slots whose cell changes
-                    int cellN[KS], toffN[KS], vN[KS];
-                    geometry(s_rec[i], cellN, toffN, vN);
-#pragma unroll
-                    for (int j = 0; j < KS; j++) {
-                        if (cellN[j] >= 0 && cellN[j] != last[j]) {
-                            if (last[j] >= 0) flush2<P>(ggrid, gdelta, last[j], acc[j]);
-                            last[j] = cellN[j];
-#pragma unroll
-                            for (int p = 0; p < P; p++) acc[j][p] = make_float2(0.f, 0.f);
-                        }
-                    }
-                }
-                const int e = s_runend[i];
-                const int re = e < i1 ? e : i1;
-                for (; i < re; ++i) {
-                    // the visibilities were staged before the item started: load
-                    // them ahead of the wait so their latency overlaps it
-                    float2 vp[P], wp[P];
-                    const float4 *vr = s_v + i * P;
-#pragma unroll
-                    for (int p = 0; p < P; p++) {
-                        const float4 q = vr[p];
-                        vp[p] = make_float2(q.x, q.y);
-                        wp[p] = make_float2(q.z, q.w);
-                    }
-                    cp_async_wait<D - 1>();     // this thread's copies for record i have landed
-                    const float4 *src = (const float4 *)(ring + ((i & (D - 1)) * KS * T + t));
-#pragma unroll
-                    for (int j = 0; j < KS; j++) {
-                        const float4 c = src[j * T];
-                        const float2 cre = make_float2(c.x, c.y), cim = make_float2(c.z, c.w);
-                        // ConvolutionGridder.cu:153-181: to += vis * wt (no conjugate)
-#pragma unroll
-                        for (int p = 0; p < P; p++) {
-                            acc[j][p] = __ffma2_rn(cre, vp[p], acc[j][p]);
-                            acc[j][p] = __ffma2_rn(cim, wp[p], acc[j][p]);
-                        }
-                    }
-                    if (i + D < i1) prefetch(i + D);
-                    cp_async_commit();
-                }
-            }
-            cp_async_wait<0>();
-#pragma unroll
-            for (int j = 0; j < KS; j++)
-                if (last[j] >= 0) flush2<P>(ggrid, gdelta, last[j], acc[j]);
-        }
+        grid_item<P, T>(a, it, s_rec, s_v, s_runend, ring);
     }
 }
 
@@ -1210,6 +1224,147 @@ __global__ void __launch_bounds__(kG4Threads, 1) k_grid4(Grid4Args a) {
     }
 }
 
+// Rolling-items gridder: the jobs of k_grid3 without block barriers.  Two
+// item buffers in shared memory; warp 0 refills a buffer with the item two
+// ahead once every thread has left it ("empty" mbarrier, one arrival per
+// thread) and publishes it ("full" mbarrier, one arrival per lane of warp 0),
+// so a thread that finishes its jobs of one item starts on the next at once
+// instead of waiting for the slowest thread at a block barrier.  Every wait
+// is bounded by a clock deadline; a wait that runs out sets *err and the
+// kernel returns.
+static const int kG5Chunk = 256;   // records of one work item (one buffer)
+
+template <int P>
+struct G5Layout {   // one item buffer, byte offsets
+    static constexpr size_t rec = 0;                                        // int4 [kG5Chunk]
+    static constexpr size_t vis = rec + (size_t)kG5Chunk * 16;              // float4 [kG5Chunk][P]
+    static constexpr size_t runend = vis + (size_t)kG5Chunk * P * 16;       // ushort [kG5Chunk]
+    static constexpr size_t start = runend + (size_t)kG5Chunk * 2;          // unsigned [kG5Chunk / 32]
+    static constexpr size_t item = start + (size_t)kG5Chunk / 8;            // int4 (y < 0: no more items)
+    static constexpr size_t bytes = (item + 16 + 15) & ~(size_t)15;
+};
+
+template <int P>
+__global__ void __launch_bounds__(kG3Threads, 2) k_grid5(Grid2Args a, int *err) {
+    constexpr int T = kG3Threads;
+    using LY = G5Layout<P>;
+    extern __shared__ uint4 smem5[];
+    unsigned char *const base = (unsigned char *)smem5;
+    ulonglong2 *const ring = (ulonglong2 *)(base + 2 * LY::bytes);      // [kG3Depth][kG3KS][T]
+    __shared__ __align__(8) unsigned long long s_bars[4];                // full[2], empty[2]
+    __shared__ volatile int s_abort;
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const int nitems = a.n_items[0];
+    const unsigned full0 = smem_u32(&s_bars[0]), empty0 = smem_u32(&s_bars[2]);
+    if (t == 0) {
+        mbar_init(full0, 32);
+        mbar_init(full0 + 8, 32);
+        mbar_init(empty0, T);
+        mbar_init(empty0 + 8, T);
+        s_abort = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+
+    // warp 0: the next item of the queue (or the end mark) into buffer b
+    auto stage = [&](int b) {
+        unsigned char *B = base + b * LY::bytes;
+        int4 *s_rec = (int4 *)(B + LY::rec);
+        float4 *s_v = (float4 *)(B + LY::vis);
+        unsigned short *s_runend = (unsigned short *)(B + LY::runend);
+        unsigned *s_start = (unsigned *)(B + LY::start);
+        int v = 0;
+        if (lane == 0) v = atomicAdd(a.counter, 1);
+        v = __shfl_sync(0xFFFFFFFFu, v, 0);
+        int4 it = make_int4(0, -1, 0, 0);
+        if (v < nitems) it = a.items[v];
+        if (it.y > kG5Chunk) {   // the plan caps items at kG5Chunk records
+            if (lane == 0) atomicExch(err, 2);
+            it.y = -1;
+        }
+        if (it.y >= 0) {
+            const GridJobDesc &J = a.jobs[it.w];
+            const int4 *grec = J.wpos;
+            const float4 *gvis = J.wvis4;
+            const int N = it.y;
+            for (int k = lane; k < N; k += 32) cp_async16(&s_rec[k], &grec[it.x + k]);
+            for (int k = lane; k < N * P; k += 32) cp_async16(&s_v[k], &gvis[(size_t)it.x * P + k]);
+            cp_async_commit();
+            cp_async_wait<0>();
+            __syncwarp();
+            for (int k0 = 0; k0 < N; k0 += 32) {      // run starts
+                const int k = k0 + lane;
+                bool st = false;
+                if (k < N) {
+                    const int4 r = s_rec[k];
+                    st = (k == 0) || r.x != s_rec[k - 1].x || r.w != s_rec[k - 1].w;
+                }
+                const unsigned m = __ballot_sync(0xFFFFFFFFu, st);
+                if (lane == 0) s_start[k0 >> 5] = m;
+            }
+            __syncwarp();
+            const int nw = (N + 31) >> 5;
+            for (int k = lane; k < N; k += 32) {      // run ends
+                int w = k >> 5;
+                unsigned m = (k & 31) == 31 ? 0u : s_start[w] & (0xFFFFFFFFu << ((k & 31) + 1));
+                while (m == 0 && ++w < nw) m = s_start[w];
+                s_runend[k] = (unsigned short)(m == 0 ? N : (w << 5) + __ffs(m) - 1);
+            }
+        }
+        if (lane == 0) *(int4 *)(B + LY::item) = it;
+        __syncwarp();
+        mbar_arrive(full0 + 8 * b);                    // every lane: its copies and stores are done
+    };
+    auto fail = [&]() {
+        s_abort = 1;
+        atomicExch(err, 1);
+    };
+
+    if (warp == 0) {
+        stage(0);
+        stage(1);
+    }
+    for (int k = 0;; k++) {
+        const int b = k & 1;
+        const unsigned ph = (unsigned)(k >> 1) & 1u;
+        if (!mbar_wait(full0 + 8 * b, ph, &s_abort)) {
+            fail();
+            break;
+        }
+        const unsigned char *B = base + b * LY::bytes;
+        const int4 it = *(const int4 *)(B + LY::item);
+        if (it.y < 0) break;
+        grid_item<P, T>(a, it, (const int4 *)(B + LY::rec), (const float4 *)(B + LY::vis),
+                        (const unsigned short *)(B + LY::runend), ring);
+        mbar_arrive(empty0 + 8 * b);
+        if (warp == 0) {
+            if (!mbar_wait(empty0 + 8 * b, ph, &s_abort)) {
+                fail();
+                break;
+            }
+            stage(b);                                  // item k + 2
+        }
+    }
+}
+
+template <int P>
+static size_t grid5_smem() {
+    return 2 * G5Layout<P>::bytes + (size_t)kG3Depth * kG3KS * kG3Threads * 16;
+}
+
+template <int P>
+static int launch_grid5(const Grid2Args &a, int *err, cudaStream_t st) {
+    auto kern = k_grid5<P>;
+    const size_t smem = grid5_smem<P>();
+    MTB_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    MTB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kG3Threads, smem));
+    if (per_sm < 1) return MTB_ERR_BAD_SHAPE;
+    kern<<<per_sm * sm_count(), kG3Threads, smem, st>>>(a, err);
+    MTB_LAUNCHED();
+    return MTB_OK;
+}
+
 template <int P>
 static size_t grid4_smem() {
     return (size_t)kG3Chunk * 16 * (1 + P) + (size_t)kG4Depth * kG4Slot + 2 * kG4Depth * kG4MaxStreams * 8;
@@ -1393,6 +1548,7 @@ static size_t padded_elems_of(const mtb_grid_params *p, const int *h_conv_info) 
 static int effective_chunk(const mtb_grid_params *p) {
     int c = p->max_chunk > 0 ? p->max_chunk : kDefaultChunk;
     if (p->merge != 1 && c > kG3Chunk) c = kG3Chunk;
+    if (p->merge != 1 && p->gridder == 5 && c > kG5Chunk) c = kG5Chunk;
     return c;
 }
 
@@ -1406,6 +1562,8 @@ static int check_params(const mtb_grid_params *p) {
     if (p->merge < 0 || p->merge > 2) return MTB_ERR_BAD_PARAM;
     if (p->bulk_min_support < 0) return MTB_ERR_BAD_PARAM;
     if (p->gridder_threads != 0 && p->gridder_threads != 256 && p->gridder_threads != 512) return MTB_ERR_BAD_PARAM;
+    if (p->gridder != 0 && p->gridder != 3 && p->gridder != 5) return MTB_ERR_BAD_PARAM;
+    if (p->gridder == 5 && p->gridder_threads == 512) return MTB_ERR_BAD_PARAM;
     return MTB_OK;
 }
 
@@ -1697,7 +1855,9 @@ static int run_grid(const mtb_grid_params *p, const GridPlan &plan, const float2
     g2.counter = s.counters;
     g2.njobs = 1;
     g2.jobs[0] = job_desc<P>(p, grid, grid_lo != nullptr, s);
-    MTB_TRY(launch_grid3<P>(g2, p->gridder_threads, st));
+    const bool rolling = p->gridder == 5;
+    if (rolling) MTB_TRY(launch_grid5<P>(g2, s.err, st));
+    else MTB_TRY(launch_grid3<P>(g2, p->gridder_threads, st));
     Grid4Args g4;
     g4.items = s.items;
     g4.first = s.split;
@@ -1712,7 +1872,7 @@ static int run_grid(const mtb_grid_params *p, const GridPlan &plan, const float2
     g4.bt = plan.bt;
     g4.err = s.err;
     if (bulk) MTB_TRY(launch_grid4<P>(g4, st));
-    if (bulk && check_gridder()) {
+    if ((bulk || rolling) && check_gridder()) {
         int e = 0;
         MTB_CUDA_TRY(cudaMemcpyAsync(&e, s.err, sizeof(int), cudaMemcpyDeviceToHost, st));
         MTB_CUDA_TRY(cudaStreamSynchronize(st));
@@ -1835,6 +1995,7 @@ static int check_batch(const mtb_grid_job *jobs, int njobs) {
         MTB_TRY(check_params(&jobs[j].params));
         if (jobs[j].params.npol != jobs[0].params.npol) return MTB_ERR_BAD_SHAPE;
         if (jobs[j].params.gridder_threads != jobs[0].params.gridder_threads) return MTB_ERR_BAD_PARAM;
+        if (jobs[j].params.gridder != jobs[0].params.gridder) return MTB_ERR_BAD_PARAM;
         if (jobs[j].nrecords < 0) return MTB_ERR_BAD_SHAPE;
         if (!jobs[j].h_conv_info) return MTB_ERR_NULL;
     }
@@ -1908,7 +2069,18 @@ static int run_batch(const mtb_grid_job *jobs, int njobs, const GridPlan *plans,
     g2.items = items;
     g2.n_items = n_total;
     g2.counter = counter;
-    MTB_TRY(launch_grid3<P>(g2, jobs[0].params.gridder_threads, st));
+    if (p0.gridder == 5) {
+        MTB_CUDA_TRY(cudaMemsetAsync(spaces[0].err, 0, sizeof(int), st));
+        MTB_TRY(launch_grid5<P>(g2, spaces[0].err, st));
+        if (check_gridder()) {
+            int e = 0;
+            MTB_CUDA_TRY(cudaMemcpyAsync(&e, spaces[0].err, sizeof(int), cudaMemcpyDeviceToHost, st));
+            MTB_CUDA_TRY(cudaStreamSynchronize(st));
+            if (e) return MTB_ERR_KERNEL;
+        }
+    } else {
+        MTB_TRY(launch_grid3<P>(g2, jobs[0].params.gridder_threads, st));
+    }
     if (p0.gridder_end_event) MTB_CUDA_TRY(cudaEventRecord((cudaEvent_t)p0.gridder_end_event, st));
     for (int j = 0; j < njobs; j++) {
         const mtb_grid_job &J = jobs[j];

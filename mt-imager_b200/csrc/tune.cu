@@ -13,16 +13,21 @@ namespace {
 
 const int kTiles[] = {16, 32, 64};
 const int kBuckets[] = {1, 2};
-const int kChunks[] = {256, 512};
-const int kThreads[] = {256, 512};
-const int kCandidates = 3 * 2 * 2 * 2;
+// (gridder, records per work item, block size): the block-staged gridder at
+// two item lengths and two block sizes, the rolling-items gridder (items of at
+// most 256 records, 256 threads)
+const int kShapes[][3] = {{3, 256, 256}, {3, 256, 512}, {3, 512, 256}, {3, 512, 512}, {5, 256, 256}};
+const int kNShapes = 5;
+const int kCandidates = 3 * 2 * kNShapes;
 
 mtb_grid_tuning candidate(int c) {
     mtb_grid_tuning t;
-    t.tile = kTiles[c / 8];
-    t.support_bucket = kBuckets[(c / 4) % 2];
-    t.max_chunk = kChunks[(c / 2) % 2];
-    t.gridder_threads = kThreads[c % 2];
+    const int *sh = kShapes[c % kNShapes];
+    t.tile = kTiles[c / (2 * kNShapes)];
+    t.support_bucket = kBuckets[(c / kNShapes) % 2];
+    t.gridder = sh[0];
+    t.max_chunk = sh[1];
+    t.gridder_threads = sh[2];
     t.ms = 0.f;
     return t;
 }
@@ -33,6 +38,7 @@ void apply(const mtb_grid_tuning &t, mtb_grid_job *jobs, int njobs) {
         jobs[j].params.support_bucket = t.support_bucket;
         jobs[j].params.max_chunk = t.max_chunk;
         jobs[j].params.gridder_threads = t.gridder_threads;
+        jobs[j].params.gridder = t.gridder;
     }
 }
 

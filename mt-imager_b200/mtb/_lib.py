@@ -67,7 +67,7 @@ class GridParams(ctypes.Structure):
                 ("support_bucket", ctypes.c_int), ("max_chunk", ctypes.c_int), ("merge", ctypes.c_int),
                 ("gridder_start_event", ctypes.c_void_p), ("gridder_end_event", ctypes.c_void_p),
                 ("bulk_min_support", ctypes.c_int), ("psf", ctypes.c_int), ("exact_delta", ctypes.c_int),
-                ("gridder_threads", ctypes.c_int), ("flags_u8", ctypes.c_int)]
+                ("gridder_threads", ctypes.c_int), ("gridder", ctypes.c_int), ("flags_u8", ctypes.c_int)]
 
 
 class GridStats(ctypes.Structure):
@@ -97,7 +97,7 @@ class FitsHeader(ctypes.Structure):
 
 class GridTuning(ctypes.Structure):
     _fields_ = [("tile", ctypes.c_int), ("support_bucket", ctypes.c_int), ("max_chunk", ctypes.c_int),
-                ("gridder_threads", ctypes.c_int), ("ms", ctypes.c_float)]
+                ("gridder_threads", ctypes.c_int), ("gridder", ctypes.c_int), ("ms", ctypes.c_float)]
 
 
 class EngineConfig(ctypes.Structure):

@@ -128,7 +128,7 @@ class WProjectionImager:
                  trial_support=0, max_support=0, w_max=0.0, pol_type=L.MTB_POL_LINEAR, compensated=True,
                  tile=0, support_bucket=0, max_chunk=0, merge=0, bulk_min_support=0, device="cuda",
                  kernels: KernelTable | None = None, psf=False, mode="wproj", taper_support=7,
-                 exact_delta=False, gridder_threads=0):
+                 exact_delta=False, gridder_threads=0, gridder=0):
         """mode "wproj" (W-projection kernels) or "normal" (taper-only kernel of
         support taper_support at oversampling `sampling`, one plane); psf
         grids every visibility as 1 + 0i (mt-imager's psf=true)."""
@@ -148,7 +148,7 @@ class WProjectionImager:
         self.compensated = compensated
         self.pol_type = pol_type
         self.tuning = dict(tile=tile, support_bucket=support_bucket, max_chunk=max_chunk, merge=merge,
-                           bulk_min_support=bulk_min_support, gridder_threads=gridder_threads)
+                           bulk_min_support=bulk_min_support, gridder_threads=gridder_threads, gridder=gridder)
         self.grid = torch.zeros((ny, nx, npol), dtype=torch.complex64, device=self.device)
         self.grid_lo = torch.zeros_like(self.grid) if compensated else None
         self.normalizer = torch.zeros(npol, dtype=torch.float32, device=self.device)
@@ -181,6 +181,7 @@ class WProjectionImager:
         gp.psf = int(self.psf)
         gp.exact_delta = int(self.exact_delta)
         gp.gridder_threads = self.tuning["gridder_threads"]
+        gp.gridder = self.tuning["gridder"]
         if self.gridder_events is not None:
             gp.gridder_start_event = self.gridder_events[0].cuda_event
             gp.gridder_end_event = self.gridder_events[1].cuda_event
@@ -302,12 +303,13 @@ def grid_batch(entries, workspace=None, stream=None):
     return workspace
 
 
-TUNING_KEYS = ("tile", "support_bucket", "max_chunk", "gridder_threads")
+TUNING_KEYS = ("tile", "support_bucket", "max_chunk", "gridder_threads", "gridder")
+N_CANDIDATES = 30
 
 
 def autotune(entries, workspace=None, stream=None):
     """Choose the gridder knobs (tile, support_bucket, max_chunk,
-    gridder_threads) for a batch by timing every candidate on this chunk
+    gridder_threads, gridder) for a batch by timing every candidate on this chunk
     (mtb_grid_autotune).  entries as for grid_batch; every imager must start a
     fresh image.  The chosen knobs are set on every imager (later chunks use
     them) and its grid holds this chunk gridded with them.  Returns (best,
@@ -324,7 +326,7 @@ def autotune(entries, workspace=None, stream=None):
     if workspace is None or workspace.numel() < need.value:
         workspace = torch.empty(max(1, need.value), dtype=torch.uint8, device=entries[0][0].device)
     best = L.GridTuning()
-    cands = (L.GridTuning * 24)()
+    cands = (L.GridTuning * N_CANDIDATES)()
     L.check(lib.mtb_grid_autotune(jobs, len(entries), _ptr(workspace), need.value, _stream(stream),
                                   ctypes.byref(best), cands), "mtb_grid_autotune")
     as_dict = lambda t: dict({k: getattr(t, k) for k in TUNING_KEYS}, ms=t.ms)  # noqa: E731

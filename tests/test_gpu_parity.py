@@ -164,7 +164,8 @@ def test_chunked_equals_single(cfg1):
                                     dict(max_chunk=37, exact_delta=True),
                                     dict(merge=1), dict(merge=2), dict(merge=1, tile=16),
                                     dict(bulk_min_support=17), dict(bulk_min_support=25), dict(exact_delta=True),
-                                    dict(gridder_threads=512), dict(gridder_threads=512, tile=16, max_chunk=256)])
+                                    dict(gridder_threads=512), dict(gridder_threads=512, tile=16, max_chunk=256),
+                                    dict(gridder=5), dict(gridder=5, tile=64)])
 def test_tuning_does_not_change_result(cfg1, tuning):
     obs, setup, geo, kern, img_o, grid_o, norm_o = cfg1
     im, img = run_gpu(obs, setup, **tuning)
@@ -173,21 +174,22 @@ def test_tuning_does_not_change_result(cfg1, tuning):
     assert rel_rms(img[0], img_o[0]) <= IMAGE_RMS_TOL
 
 
-@pytest.mark.parametrize("kw", [dict(), dict(tile=64), dict(nx=320, s=3), dict(merge=1),
+@pytest.mark.parametrize("kw", [dict(), dict(tile=64), dict(nx=320, s=3), dict(merge=1), dict(gridder=5),
                                 dict(bulk_min_support=17), dict(nx=320, s=3, bulk_min_support=17)])
 def test_large_supports(oracle, kw):
-    """Supports up to 55 (and 105 with odd sampling): the per-thread and the
-    bulk-copy direct gridders (one and several passes, one and several record
+    """Supports up to 55 (and 105 with odd sampling): the direct gridders
+    (block-staged, rolling-items and bulk-copy; one and several record
     streams), the shared-memory window variant, and support bands split across
     blocks."""
     tile = kw.pop("tile", 0)
     merge = kw.pop("merge", 0)
     bulk = kw.pop("bulk_min_support", 0)
+    gridder = kw.pop("gridder", 0)
     obs, setup = wide_case(**kw)
     geo = oracle.geometry_for(setup)
     kern = oracle.wkernels(geo)
     img_o, grid_o, norm_o = oracle.image_channel(obs, 0, setup, kern, geo)
-    im, img = run_gpu(obs, setup, tile=tile, merge=merge, bulk_min_support=bulk)
+    im, img = run_gpu(obs, setup, tile=tile, merge=merge, bulk_min_support=bulk, gridder=gridder)
     assert np.array_equal(im.kernels.conv_info, kern["conv_info"])
     assert np.abs(im.kernels.table.cpu().numpy() - kern["table"]).max() <= KERNEL_TOL
     g = im.grid_sum().cpu().numpy()
