@@ -534,8 +534,7 @@ __global__ void __launch_bounds__(KMAX >= 8 ? 576 : 1024) k_grid(GridArgs a) {
 // and no two slots of a unit share a cell).  Each slot accumulates V * C for
 // all polarisations in registers with packed f32x2 FMAs and merges into the
 // grid (vector reductions) only when its cell changes and at the end of a job.
-static const int kG2Threads = 256;
-static const int kG3Threads = kG2Threads;   // default block size (threads per work item)
+static const int kG3Threads = 256;          // default block size (threads per work item)
 static const int kG3Chunk = 512;            // records of one work item, staged at once
 static const int kG3Depth = 4;              // records of kernel values fetched ahead
 static const int kG3KS = 4;                 // support-box slots per thread
