@@ -1910,6 +1910,8 @@ extern "C" int mtb_grid_workspace_size(const mtb_grid_params *p, const int *h_co
     if (!bytes || !h_conv_info) return MTB_ERR_NULL;
     MTB_TRY(check_params(p));
     if (nrecords < 0) return MTB_ERR_BAD_SHAPE;
+    GridPlan plan;   // refuses supports and tiles the gridders cannot take, as mtb_grid does
+    MTB_TRY(make_plan(p, h_conv_info, &plan));
     int chunk = effective_chunk(p);
     Arena A;
     GridSpace s;

@@ -89,3 +89,22 @@ def test_status_codes_match_header():
     assert len(codes) == 10
     for name, v in codes.items():
         assert getattr(L, name) == v, name
+
+
+@pytest.mark.parametrize("support,tile,status", [(255, 0, L.MTB_OK), (257, 0, L.MTB_ERR_KERNEL),
+                                                 (16, 0, L.MTB_ERR_KERNEL), (7, 2, L.MTB_ERR_BAD_PARAM)])
+def test_plan_limits(mtblib, support, tile, status):
+    """The direct gridders lay one support-box column per thread of a block:
+    supports are odd and at most 255; tiles at least 4 cells.  Refused on the
+    host, before any device work."""
+    p = L.GridParams()
+    p.nx = p.ny = 1024
+    p.npol, p.sampling, p.wplanes = 4, 4, 1
+    p.u_increment = p.v_increment = p.w_sq_increment = 1.0
+    p.tile = tile
+    info = (ctypes.c_int * 2)(support, 0)
+    n = ctypes.c_size_t(0)
+    rc = mtblib.mtb_grid_workspace_size(ctypes.byref(p), ctypes.cast(info, ctypes.c_void_p), 1000, ctypes.byref(n))
+    if status == L.MTB_OK and rc != L.MTB_OK:
+        pytest.skip("workspace query needs the device on this host (status %d)" % rc)
+    assert rc == status
