@@ -284,7 +284,7 @@ def main():
     ap.add_argument("--config", default="mid", choices=["mid", "small", "serve", "cube"])
     ap.add_argument("--channels", type=int, default=16)
     ap.add_argument("--hours", type=float, default=8.0)
-    ap.add_argument("--e2e-steps", type=int, default=1)
+    ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-records", type=int, default=0, help="records for the CPU baseline sample")
     ap.add_argument("--ref-baselines", type=int, default=560)
     ap.add_argument("--tile", type=int, default=0)
@@ -542,10 +542,12 @@ def main():
 
 def run_e2e(args, torch, dev, uvw_d, chans, imagers, images, samples_per_step, world, dist):
     """Same metric through the public API from pinned host buffers: per step
-    the H2D copy of every channel's records and the D2H of every image are
-    inside the timed region.  H2D copies run on a side stream, double-buffered
-    against the compute of the previous channel; each image's D2H runs on a
-    third stream once it is finalised."""
+    the H2D copy of every channel's records (and of uvw) and the D2H of every
+    image are inside the timed region.  H2D copies run on a side stream,
+    double-buffered against the compute of the previous channel; each image's
+    D2H runs on a third stream once it is finalised.  Steps follow each other
+    without a device drain (a streaming imager): events guard every buffer
+    reuse, and the timed region ends after the last image is on the host."""
     host_uvw = torch.empty(uvw_d.shape, dtype=uvw_d.dtype, pin_memory=True)
     host_uvw.copy_(uvw_d)
     host = []
@@ -558,49 +560,62 @@ def run_e2e(args, torch, dev, uvw_d, chans, imagers, images, samples_per_step, w
         host.append(hc)
     out_host = [torch.empty(im.shape, dtype=im.dtype, pin_memory=True) for im in images]
     bufs = [[torch.empty_like(t) for t in chans[0]] for _ in range(2)]
-    uvw_buf = torch.empty_like(uvw_d)
+    uvw_bufs = [torch.empty_like(uvw_d) for _ in range(2)]
     copy = torch.cuda.Stream(device=dev)
     back = torch.cuda.Stream(device=dev)
     comp = torch.cuda.current_stream(dev)
     h2d = host_uvw.numel() * 4 + sum(sum(t.numel() * t.element_size() for t in hc) for hc in host)
     d2h = sum(o.numel() * 4 for o in out_host)
+    # events: buffer pair free (last gridding that read it done), uvw buffer
+    # free, image c read back
+    state = dict(seq=0, free=[None, None], uvw_free=[None, None], back=[None] * len(host))
 
-    def step():
-        ready = [torch.cuda.Event() for _ in host]
-        free = [torch.cuda.Event() for _ in range(2)]
+    def record(stream):
+        e = torch.cuda.Event()
+        e.record(stream)
+        return e
+
+    def step(n):
+        ub = uvw_bufs[n % 2]
         with torch.cuda.stream(copy):
-            uvw_buf.copy_(host_uvw, non_blocking=True)
+            if state["uvw_free"][n % 2] is not None:
+                copy.wait_event(state["uvw_free"][n % 2])
+            ub.copy_(host_uvw, non_blocking=True)
         for c, hc in enumerate(host):
-            b = bufs[c % 2]
+            k = state["seq"] % 2
+            state["seq"] += 1
+            b = bufs[k]
             with torch.cuda.stream(copy):
-                if c >= 2:
-                    copy.wait_event(free[c % 2])
+                if state["free"][k] is not None:
+                    copy.wait_event(state["free"][k])
                 for dst, src in zip(b, hc):
                     dst.copy_(src, non_blocking=True)
-                ready[c].record(copy)
-            comp.wait_event(ready[c])
+                ready = record(copy)
+            comp.wait_event(ready)
             im = imagers[c]
             im.reset()
-            im.grid_device(uvw_buf, *b)
-            free[c % 2].record(comp)
+            im.grid_device(ub, *b)
+            state["free"][k] = record(comp)
+            if state["back"][c] is not None:
+                comp.wait_event(state["back"][c])      # images[c] of the last step is on the host
             im.finalize(out=images[c])
-            # the image goes back on its own stream: the next channel's
-            # gridding does not wait for the read-back
-            done = torch.cuda.Event()
-            done.record(comp)
-            back.wait_event(done)
+            back.wait_event(record(comp))
             with torch.cuda.stream(back):
                 out_host[c].copy_(images[c], non_blocking=True)
-        torch.cuda.synchronize()
+                state["back"][c] = record(back)
+        state["uvw_free"][n % 2] = record(comp)
 
-    step()
+    step(0)
+    torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     a.record()
-    for _ in range(args.e2e_steps):
-        step()
+    for n in range(1, args.e2e_steps + 1):
+        step(n)
+    for e in state["back"]:
+        comp.wait_event(e)
     b.record()
     torch.cuda.synchronize()
     ms = max_over_ranks(a.elapsed_time(b) / args.e2e_steps, world, dist, torch, dev)
