@@ -566,6 +566,7 @@ def run_e2e(args, torch, dev, uvw_d, chans, imagers, images, samples_per_step, w
     comp = torch.cuda.current_stream(dev)
     h2d = host_uvw.numel() * 4 + sum(sum(t.numel() * t.element_size() for t in hc) for hc in host)
     d2h = sum(o.numel() * 4 for o in out_host)
+    ref_image = images[-1].clone()          # the device path's image of the last channel
     # events: buffer pair free (last gridding that read it done), uvw buffer
     # free, image c read back
     state = dict(seq=0, free=[None, None], uvw_free=[None, None], back=[None] * len(host))
@@ -619,8 +620,15 @@ def run_e2e(args, torch, dev, uvw_d, chans, imagers, images, samples_per_step, w
     b.record()
     torch.cuda.synchronize()
     ms = max_over_ranks(a.elapsed_time(b) / args.e2e_steps, world, dist, torch, dev)
+    # the image that came back to the host equals the device path's (to the
+    # rounding of the FP32 reductions)
+    ref = ref_image.cpu().numpy()
+    got = out_host[-1].numpy()
+    check = float(np.sqrt(np.mean((got - ref) ** 2)) / max(float(np.abs(ref[0]).max()), 1e-30))
+    if not check <= 1e-5:
+        raise RuntimeError("e2e image differs from the device path: rms/peak %g" % check)
     return {"value": job_throughput(samples_per_step, world, ms), "unit": "samples/s", "h2d_bytes_per_step": int(h2d),
-            "d2h_bytes_per_step": int(d2h), "ms_per_step": ms}
+            "d2h_bytes_per_step": int(d2h), "ms_per_step": ms, "image_check_rms": check}
 
 
 # ---------------------------------------------------------------- serving --
