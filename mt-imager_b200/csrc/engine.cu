@@ -229,17 +229,19 @@ namespace {
 
 // Admission estimate: the request's grid, compensation and delta grids, image,
 // and an mtb_grid workspace for its largest chunk with every plane at the
-// support cap (an upper bound before the kernel table exists).
+// largest support the gridders take (an upper bound before the kernel table
+// exists).
 int request_bytes(const mtb_engine_config &cfg, const mtb_image_request *r, size_t *out) {
     mtb_wkernel_info info;
     int s = mtb_wkernel_query(&r->geometry, &info);
     if (s != MTB_OK) return s;
     const size_t cells = (size_t)r->geometry.nx * r->geometry.ny * r->npol;
-    std::vector<int> ci((size_t)r->geometry.wplanes * 2);
-    for (int k = 0; k < r->geometry.wplanes; k++) {
-        ci[2 * k] = info.support_cap;
-        ci[2 * k + 1] = k * info.T * info.T * info.support_cap * info.support_cap;
-    }
+    // every plane at the largest support the gridders take (odd, at most 255)
+    int S = std::min(info.support_cap, 255);
+    if (S % 2 == 0) S--;
+    if (S < 1) S = 1;
+    std::vector<int> ci((size_t)r->geometry.wplanes * 2, 0);   // table offsets do not size the workspace
+    for (int k = 0; k < r->geometry.wplanes; k++) ci[2 * k] = S;
     mtb_grid_params gp;
     std::memset(&gp, 0, sizeof(gp));
     gp.nx = r->geometry.nx;
