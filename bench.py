@@ -285,6 +285,7 @@ def main():
     ap.add_argument("--channels", type=int, default=16)
     ap.add_argument("--hours", type=float, default=8.0)
     ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--streams", type=int, default=1, help="CUDA streams the channels of a step alternate over")
     ap.add_argument("--cpu-records", type=int, default=0, help="records for the CPU baseline sample")
     ap.add_argument("--ref-baselines", type=int, default=560)
     ap.add_argument("--tile", type=int, default=0)
@@ -408,15 +409,30 @@ def main():
     torch.cuda.synchronize()
     lat_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in freqs]
 
+    # the channels of a step alternate over args.streams CUDA streams, so one
+    # channel's finalisation overlaps the next channel's binning
+    main_stream = torch.cuda.current_stream(dev)
+    streams = [main_stream] + [torch.cuda.Stream(device=dev) for _ in range(max(1, args.streams) - 1)]
+
     def step(record_latency=True):
+        begin = torch.cuda.Event()
+        begin.record(main_stream)
+        for st in streams[1:]:
+            st.wait_event(begin)
         for c, (im, (freq, vis, weights, flags)) in enumerate(zip(imagers, chans)):
-            if record_latency:
-                lat_ev[c][0].record()
-            im.reset()
-            im.grid_device(uvw, freq, vis, weights, flags)
-            im.finalize(out=images[c])
-            if record_latency:
-                lat_ev[c][1].record()
+            st = streams[c % len(streams)]
+            with torch.cuda.stream(st):
+                if record_latency:
+                    lat_ev[c][0].record(st)
+                im.reset()
+                im.grid_device(uvw, freq, vis, weights, flags)
+                im.finalize(out=images[c])
+                if record_latency:
+                    lat_ev[c][1].record(st)
+        for st in streams[1:]:
+            done = torch.cuda.Event()
+            done.record(st)
+            main_stream.wait_event(done)
 
     for _ in range(max(3, args.warmup)):
         step()
@@ -520,7 +536,7 @@ def main():
                        "image": n, "cell_arcsec": dl / ARCSEC, "wplanes": spec["wplanes"],
                        "sampling": spec["sampling"], "supports": [int(sup.min()), int(sup.max())],
                        "samples_per_step": samples_per_step, "l2": "inputs larger than L2 (1.6 GB per channel)",
-                       "flags": "uint8 [R][4] (flags_u8)",
+                       "flags": "uint8 [R][4] (flags_u8)", "streams": args.streams,
                        "parallelism": "replicas" if world > 1 else "single GPU"},
             "images_per_s": len(freqs) * world / (ms_per_step * 1e-3),
             "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
