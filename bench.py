@@ -377,11 +377,14 @@ def main():
     freqs = channel_freqs(spec)
     gen = torch.Generator(device=dev).manual_seed(7 + rank)
     chans = []
+    # one weights array for every channel: mt-imager reads the MS WEIGHT column
+    # (per row and polarisation) and hands the same array to each channel
+    # (MSVisibilityDataSetAsync.cpp:262-271)
+    weights = torch.ones((R, 4), dtype=torch.float32, device=dev)
     for c, f in enumerate(freqs):
         vis = make_vis(uvw, f, srcs, torch, gen)
         # one byte per flag (mtb_grid_params.flags_u8): a quarter of the int32 layout's bytes to move
         flags = (torch.rand(R, device=dev, generator=gen) < spec["flag"]).to(torch.uint8)[:, None].repeat(1, 4).contiguous()
-        weights = torch.ones((R, 4), dtype=torch.float32, device=dev)
         freq = torch.full((R,), f / C_LIGHT, dtype=torch.float32, device=dev)
         chans.append((freq, vis, weights, flags))
     torch.cuda.synchronize()
@@ -492,7 +495,8 @@ def main():
         # every rank pins a host copy of its inputs and images; with several
         # ranks on one host that can exceed its memory: all ranks skip the leg
         # (the same decision on every rank) when the node's share is too small
-        pinned = uvw.numel() * 4 + sum(sum(t.numel() * t.element_size() for t in ch) for ch in chans) + \
+        unique = {id(t): t for ch in chans for t in ch}       # the shared weights count once
+        pinned = uvw.numel() * 4 + sum(t.numel() * t.element_size() for t in unique.values()) + \
             sum(im.numel() * 4 for im in images)
         local_ranks = int(os.environ.get("LOCAL_WORLD_SIZE", str(world)))
         fits = pinned * local_ranks <= 0.6 * host_available_bytes()
@@ -531,7 +535,8 @@ def main():
             "metric": METRIC, "value": value, "unit": "samples/s", "n_gpus": world, "steps": args.steps,
             "warmup": max(3, args.warmup), "ms_per_step": ms_per_step, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32 (FP64 coordinates and w-phase)",
-            "data": "synthetic (seeded earth-rotation tracks, point-source sky)",
+            "data": "synthetic (seeded earth-rotation tracks, point-source sky; one weights array shared by the "
+                    "channels, as the MS WEIGHT column)",
             "config": {"workload": workload_name(spec), "records_per_channel": R, "channels": len(freqs),
                        "image": n, "cell_arcsec": dl / ARCSEC, "wplanes": spec["wplanes"],
                        "sampling": spec["sampling"], "supports": [int(sup.min()), int(sup.max())],
@@ -558,29 +563,32 @@ def main():
 
 def run_e2e(args, torch, dev, uvw_d, chans, imagers, images, samples_per_step, world, dist):
     """Same metric through the public API from pinned host buffers: per step
-    the H2D copy of every channel's records (and of uvw) and the D2H of every
-    image are inside the timed region.  H2D copies run on a side stream,
+    the H2D copy of every channel's records (and of the arrays the channels
+    share: uvw and the weights) and the D2H of every image are inside the
+    timed region.  H2D copies run on a side stream,
     double-buffered against the compute of the previous channel; each image's
     D2H runs on a third stream once it is finalised.  Steps follow each other
     without a device drain (a streaming imager): events guard every buffer
     reuse, and the timed region ends after the last image is on the host."""
-    host_uvw = torch.empty(uvw_d.shape, dtype=uvw_d.dtype, pin_memory=True)
-    host_uvw.copy_(uvw_d)
-    host = []
-    for (freq, vis, weights, flags) in chans:
-        hc = []
-        for t in (freq, vis, weights, flags):
-            h = torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
-            h.copy_(t)
-            hc.append(h)
-        host.append(hc)
+    def pinned(t):
+        h = torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
+        h.copy_(t)
+        return h
+
+    shared_w = all(ch[2] is chans[0][2] for ch in chans)
+    host_uvw = pinned(uvw_d)
+    host_w = pinned(chans[0][2]) if shared_w else None
+    # per channel: freq, vis, flags (and weights when the channels do not share them)
+    host = [[pinned(t) for t in ((f, v, fl) if shared_w else (f, v, w, fl))] for (f, v, w, fl) in chans]
     out_host = [torch.empty(im.shape, dtype=im.dtype, pin_memory=True) for im in images]
-    bufs = [[torch.empty_like(t) for t in chans[0]] for _ in range(2)]
+    bufs = [[torch.empty_like(t) for t in host[0]] for _ in range(2)]
     uvw_bufs = [torch.empty_like(uvw_d) for _ in range(2)]
+    w_bufs = [torch.empty_like(chans[0][2]) for _ in range(2)] if shared_w else None
     copy = torch.cuda.Stream(device=dev)
     back = torch.cuda.Stream(device=dev)
     comp = torch.cuda.current_stream(dev)
-    h2d = host_uvw.numel() * 4 + sum(sum(t.numel() * t.element_size() for t in hc) for hc in host)
+    h2d = host_uvw.numel() * 4 + (host_w.numel() * 4 if shared_w else 0) + \
+        sum(sum(t.numel() * t.element_size() for t in hc) for hc in host)
     d2h = sum(o.numel() * 4 for o in out_host)
     ref_image = images[-1].clone()          # the device path's image of the last channel
     # events: buffer pair free (last gridding that read it done), uvw buffer
@@ -594,10 +602,13 @@ def run_e2e(args, torch, dev, uvw_d, chans, imagers, images, samples_per_step, w
 
     def step(n):
         ub = uvw_bufs[n % 2]
+        wb = w_bufs[n % 2] if shared_w else None
         with torch.cuda.stream(copy):
             if state["uvw_free"][n % 2] is not None:
                 copy.wait_event(state["uvw_free"][n % 2])
             ub.copy_(host_uvw, non_blocking=True)
+            if shared_w:
+                wb.copy_(host_w, non_blocking=True)
         for c, hc in enumerate(host):
             k = state["seq"] % 2
             state["seq"] += 1
@@ -611,7 +622,10 @@ def run_e2e(args, torch, dev, uvw_d, chans, imagers, images, samples_per_step, w
             comp.wait_event(ready)
             im = imagers[c]
             im.reset()
-            im.grid_device(ub, *b)
+            if shared_w:
+                im.grid_device(ub, b[0], b[1], wb, b[2])
+            else:
+                im.grid_device(ub, *b)
             state["free"][k] = record(comp)
             if state["back"][c] is not None:
                 comp.wait_event(state["back"][c])      # images[c] of the last step is on the host
