@@ -581,7 +581,7 @@ def run_e2e(args, torch, dev, uvw_d, chans, imagers, images, samples_per_step, w
     # per channel: freq, vis, flags (and weights when the channels do not share them)
     host = [[pinned(t) for t in ((f, v, fl) if shared_w else (f, v, w, fl))] for (f, v, w, fl) in chans]
     out_host = [torch.empty(im.shape, dtype=im.dtype, pin_memory=True) for im in images]
-    bufs = [[torch.empty_like(t) for t in host[0]] for _ in range(2)]
+    bufs = [[torch.empty(t.shape, dtype=t.dtype, device=dev) for t in host[0]] for _ in range(2)]
     uvw_bufs = [torch.empty_like(uvw_d) for _ in range(2)]
     w_bufs = [torch.empty_like(chans[0][2]) for _ in range(2)] if shared_w else None
     copy = torch.cuda.Stream(device=dev)

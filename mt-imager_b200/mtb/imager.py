@@ -32,6 +32,16 @@ def _dev(x, dtype, device):
     return torch.from_numpy(np.ascontiguousarray(x)).to(device=device, dtype=dtype)
 
 
+def _on_device(t, device):
+    """t lives on `device` (a device without an index means the current one)."""
+    if t.device.type != device.type:
+        return False
+    if device.type != "cuda":
+        return True
+    want = device.index if device.index is not None else torch.cuda.current_device()
+    return t.device.index == want
+
+
 def _is_byte_flags(flags):
     dt = getattr(flags, "dtype", None)
     return dt in (np.uint8, np.bool_, torch.uint8, torch.bool)
@@ -219,6 +229,11 @@ class WProjectionImager:
         return self.grid_device(uvw, freq, vis, weights, flags, stream)
 
     def grid_device(self, uvw, freq, vis, weights, flags, stream=None):
+        """One chunk from tensors already on the imager's device (layouts of
+        grid_chunk); anything else is refused before a kernel sees it."""
+        for name, t in (("uvw", uvw), ("freq", freq), ("vis", vis), ("weights", weights), ("flags", flags)):
+            if not (isinstance(t, torch.Tensor) and _on_device(t, self.device) and t.is_contiguous()):
+                raise ValueError("%s must be a contiguous tensor on %s" % (name, self.device))
         k = self.build_kernels()
         R = int(freq.numel())
         gp = self.grid_params(self._fresh)
@@ -263,6 +278,9 @@ def _batch_jobs(entries):
     jobs = (L.GridJob * len(entries))()
     keep = []
     for j, (im, uvw, freq, vis, weights, flags) in enumerate(entries):
+        for name, t in (("uvw", uvw), ("freq", freq), ("vis", vis), ("weights", weights), ("flags", flags)):
+            if not (isinstance(t, torch.Tensor) and _on_device(t, im.device) and t.is_contiguous()):
+                raise ValueError("image %d: %s must be a contiguous tensor on %s" % (j, name, im.device))
         k = im.build_kernels()
         gp = im.grid_params(im._fresh)
         J = jobs[j]
