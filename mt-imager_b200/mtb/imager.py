@@ -144,6 +144,8 @@ class WProjectionImager:
         grids every visibility as 1 + 0i (mt-imager's psf=true)."""
         self.lib = L.load()
         self.device = torch.device(device)
+        if self.device.type != "cuda":
+            raise ValueError("the imager runs on a CUDA device (no CPU fallback); got %s" % self.device)
         self.nx, self.ny, self.npol = nx, ny, npol
         m_increment = l_increment if m_increment is None else m_increment
         if mode not in ("wproj", "normal"):

@@ -108,3 +108,9 @@ def test_plan_limits(mtblib, support, tile, status):
     if status == L.MTB_OK and rc != L.MTB_OK:
         pytest.skip("workspace query needs the device on this host (status %d)" % rc)
     assert rc == status
+
+
+def test_imager_refuses_a_cpu_device():
+    from mtb.imager import WProjectionImager
+    with pytest.raises(ValueError):
+        WProjectionImager(64, 64, 1e-4, device="cpu")
