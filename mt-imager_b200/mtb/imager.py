@@ -32,6 +32,11 @@ def _dev(x, dtype, device):
     return torch.from_numpy(np.ascontiguousarray(x)).to(device=device, dtype=dtype)
 
 
+def _require_cuda(device):
+    if torch.device(device).type != "cuda":
+        raise ValueError("the library runs on a CUDA device (no CPU fallback); got %s" % device)
+
+
 def _on_device(t, device):
     """t lives on `device` (a device without an index means the current one)."""
     if t.device.type != device.type:
@@ -82,6 +87,7 @@ def build_taper_kernels(nx, ny, l_increment, m_increment, support=7, sampling=8,
                         stream=None) -> KernelTable:
     """mode=normal: the taper-only kernel table (one plane, no w-term) of
     OnlyTaperConvFunction.cpp:29-99 through mtb_taper_kernel_build."""
+    _require_cuda(device)
     lib = L.load()
     T = sampling if sampling % 2 else sampling + 1
     n = T * T * support * support
@@ -113,6 +119,7 @@ def query_wkernels(params: L.WKernelParams) -> L.WKernelInfo:
 
 
 def build_wkernels(params: L.WKernelParams, device="cuda", stream=None) -> KernelTable:
+    _require_cuda(device)
     lib = L.load()
     info = query_wkernels(params)
     ws = torch.empty(max(1, info.workspace_bytes), dtype=torch.uint8, device=device)
@@ -144,8 +151,7 @@ class WProjectionImager:
         grids every visibility as 1 + 0i (mt-imager's psf=true)."""
         self.lib = L.load()
         self.device = torch.device(device)
-        if self.device.type != "cuda":
-            raise ValueError("the imager runs on a CUDA device (no CPU fallback); got %s" % self.device)
+        _require_cuda(self.device)
         self.nx, self.ny, self.npol = nx, ny, npol
         m_increment = l_increment if m_increment is None else m_increment
         if mode not in ("wproj", "normal"):

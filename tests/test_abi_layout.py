@@ -114,3 +114,11 @@ def test_imager_refuses_a_cpu_device():
     from mtb.imager import WProjectionImager
     with pytest.raises(ValueError):
         WProjectionImager(64, 64, 1e-4, device="cpu")
+
+
+def test_kernel_builders_refuse_a_cpu_device():
+    from mtb.imager import build_taper_kernels, build_wkernels, wkernel_params
+    with pytest.raises(ValueError):
+        build_wkernels(wkernel_params(64, 64, 1e-4, 1e-4, 4, 4), device="cpu")
+    with pytest.raises(ValueError):
+        build_taper_kernels(64, 64, 1e-4, 1e-4, device="cpu")
