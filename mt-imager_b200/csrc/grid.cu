@@ -550,7 +550,7 @@ struct GridJobDesc {
     double *dgrid;         // compensated mode: FP64 delta grid of this call, else null
     const int *M;          // [kMaxBuckets] bucket moduli (device)
     int nx;
-    int pad_;
+    int uniform;           // 1: every record's support equals its bucket's modulus
 };
 static const int kMaxBatch = 64;   // images one batched launch grids
 
@@ -711,7 +711,9 @@ __global__ void k_pad_expand(const float2 *__restrict__ t, const int *__restrict
 // block barrier per record).  A slot outside a record's support box gets
 // zeros in its ring entry, which keeps the accumulation loop free of
 // per-slot branches.
-template <int P, int T>
+// UNIFORM: every record's support equals the modulus M (one support per
+// bucket), so no slot of a record's box falls outside it.
+template <int P, int T, bool UNIFORM>
 __device__ __forceinline__ void grid_item(const Grid2Args &a, const int4 it, const int4 *s_rec, const float4 *s_v,
                                           const unsigned short *s_runend, ulonglong2 *ring) {
     constexpr int KS = kG3KS, D = kG3Depth;
@@ -745,10 +747,10 @@ __device__ __forceinline__ void grid_item(const Grid2Args &a, const int4 it, con
             sx -= (sx >= M) ? M : 0;
             int sy = g + (rec.y >> 16);
             sy -= (sy >= M) ? M : 0;
-            const bool xok = sx < S;
+            const bool xok = UNIFORM || sx < S;
 #pragma unroll
             for (int j = 0; j < KS; j++) {
-                const bool ok = xok && (j < nrow) && (sy < S);
+                const bool ok = xok && (j < nrow) && (UNIFORM || sy < S);
                 cell[j] = ok ? rec.x + sy * gnx + sx : -1;
                 toff[j] = ok ? sy * (S + 1) + sx : 0;
                 vbytes[j] = ok ? 16 : 0;
@@ -895,7 +897,8 @@ __global__ void __launch_bounds__(T, 512 / T) k_grid3(Grid2Args a) {
             s_runend[k] = (unsigned short)(m == 0 ? N : (w << 5) + __ffs(m) - 1);
         }
         __syncthreads();
-        grid_item<P, T>(a, it, s_rec, s_v, s_runend, ring);
+        if (J.uniform) grid_item<P, T, true>(a, it, s_rec, s_v, s_runend, ring);
+        else grid_item<P, T, false>(a, it, s_rec, s_v, s_runend, ring);
     }
 }
 
@@ -1333,8 +1336,12 @@ __global__ void __launch_bounds__(kG3Threads, 2) k_grid5(Grid2Args a, int *err) 
         const unsigned char *B = base + b * LY::bytes;
         const int4 it = *(const int4 *)(B + LY::item);
         if (it.y < 0) break;
-        grid_item<P, T>(a, it, (const int4 *)(B + LY::rec), (const float4 *)(B + LY::vis),
-                        (const unsigned short *)(B + LY::runend), ring);
+        if (a.jobs[it.w].uniform)
+            grid_item<P, T, true>(a, it, (const int4 *)(B + LY::rec), (const float4 *)(B + LY::vis),
+                                  (const unsigned short *)(B + LY::runend), ring);
+        else
+            grid_item<P, T, false>(a, it, (const int4 *)(B + LY::rec), (const float4 *)(B + LY::vis),
+                                   (const unsigned short *)(B + LY::runend), ring);
         mbar_arrive(empty0 + 8 * b);
         if (warp == 0) {
             if (!mbar_wait(empty0 + 8 * b, ph, &s_abort)) {
@@ -1768,7 +1775,8 @@ static GridJobDesc job_desc(const mtb_grid_params *p, float *grid, bool compensa
     d.dgrid = (compensated && p->exact_delta) ? s.delta : nullptr;
     d.M = s.moduli;
     d.nx = p->nx;
-    d.pad_ = 0;
+    // one odd support per bucket: every record's support is its bucket's modulus
+    d.uniform = p->support_bucket <= 1 ? 1 : 0;
     return d;
 }
 
