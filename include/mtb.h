@@ -155,9 +155,11 @@ typedef struct mtb_grid_params {
                                   (order-independent, about half the grid error, slower)   */
     int gridder_threads;       /* 0: 256; threads of a gridder block, which grids one work
                                   item at a time (256 or 512)                              */
-    int gridder;               /* 0 or 3: k_grid3 (block-wide staging of each work item);
+    int gridder;               /* 0: default (5, or 3 with gridder_threads 512);
+                                  3: k_grid3 (block-wide staging of each work item);
                                   5: k_grid5 (two item buffers refilled by one warp, no
-                                  block barriers; items of at most 256 records)           */
+                                  block barriers; items of at most 256 records).  A gridder
+                                  that could not complete sets the normaliser to NaN      */
     int flags_u8;              /* 0: d_flags is int32 [R][P] (the reference's layout); 1: it
                                   is one byte per flag, uint8 [R][P] (0 = keep, 1 = flagged;
                                   a quarter of the bytes to move), passed cast to int *    */

@@ -306,10 +306,14 @@ __global__ void k_gather(int R, const unsigned *__restrict__ skeys, const int *_
     }
 }
 
+// err (may be null): the gridder's error flag; when set, the normaliser
+// becomes NaN so the image of a gridding that did not complete cannot pass
+// for a valid one.
 __global__ void k_finish(int P, const double *__restrict__ norm_acc, float *__restrict__ normalizer,
-                         const unsigned long long *__restrict__ st, mtb_grid_stats *__restrict__ out) {
+                         const unsigned long long *__restrict__ st, mtb_grid_stats *__restrict__ out,
+                         const int *__restrict__ err) {
     int t = threadIdx.x;
-    if (t < P) normalizer[t] += (float)norm_acc[t];
+    if (t < P) normalizer[t] = (err && *err) ? __int_as_float(0x7fc00000) : normalizer[t] + (float)norm_acc[t];
     if (out && t == 0) {
         out->gridded_records += st[0];
         out->compressed_records += st[1];
@@ -1551,10 +1555,24 @@ static size_t padded_elems_of(const mtb_grid_params *p, const int *h_conv_info) 
 }
 
 // records per work item: the direct gridder stages a whole item in shared memory
+// The direct gridder a call uses: gridder 0 selects the default, the
+// rolling-items k_grid5, unless 512-thread blocks are asked for (k_grid3 only).
+// A stream under CUDA-graph capture cannot be synchronised: the debug
+// read-back of the gridder's error flag is skipped there.
+static bool capturing(cudaStream_t st) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    return cudaStreamIsCapturing(st, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone;
+}
+
+static int gridder_of(const mtb_grid_params *p) {
+    if (p->gridder != 0) return p->gridder;
+    return p->gridder_threads == 512 ? 3 : 5;
+}
+
 static int effective_chunk(const mtb_grid_params *p) {
     int c = p->max_chunk > 0 ? p->max_chunk : kDefaultChunk;
     if (p->merge != 1 && c > kG3Chunk) c = kG3Chunk;
-    if (p->merge != 1 && p->gridder == 5 && c > kG5Chunk) c = kG5Chunk;
+    if (p->merge != 1 && gridder_of(p) == 5 && c > kG5Chunk) c = kG5Chunk;
     return c;
 }
 
@@ -1784,7 +1802,7 @@ static GridJobDesc job_desc(const mtb_grid_params *p, float *grid, bool compensa
 // add the call's normaliser sums and statistics.
 template <int P>
 static int finish_grid(const mtb_grid_params *p, float *grid, float *grid_lo, float *normalizer,
-                       mtb_grid_stats *stats, GridSpace &s, cudaStream_t st) {
+                       mtb_grid_stats *stats, GridSpace &s, const int *err, cudaStream_t st) {
     const int sms = sm_count();
     if (grid_lo) {
         const size_t n2 = (size_t)p->nx * p->ny * P;     // complex values
@@ -1806,7 +1824,7 @@ static int finish_grid(const mtb_grid_params *p, float *grid, float *grid_lo, fl
             }
         }
     }
-    k_finish<<<1, 32, 0, st>>>(P, s.norm_acc, normalizer, s.stats, stats);
+    k_finish<<<1, 32, 0, st>>>(P, s.norm_acc, normalizer, s.stats, stats, err);
     MTB_LAUNCHED();
     return MTB_OK;
 }
@@ -1844,7 +1862,7 @@ static int run_grid(const mtb_grid_params *p, const GridPlan &plan, const float2
             MTB_TRY(launch_bucket<P>(a, L, st));
         }
         if (p->gridder_end_event) MTB_CUDA_TRY(cudaEventRecord((cudaEvent_t)p->gridder_end_event, st));
-        k_finish<<<1, 32, 0, st>>>(P, s.norm_acc, normalizer, s.stats, stats);
+        k_finish<<<1, 32, 0, st>>>(P, s.norm_acc, normalizer, s.stats, stats, nullptr);
         MTB_LAUNCHED();
         return MTB_OK;
     }
@@ -1862,7 +1880,7 @@ static int run_grid(const mtb_grid_params *p, const GridPlan &plan, const float2
     g2.counter = s.counters;
     g2.njobs = 1;
     g2.jobs[0] = job_desc<P>(p, grid, grid_lo != nullptr, s);
-    const bool rolling = p->gridder == 5;
+    const bool rolling = gridder_of(p) == 5;
     if (rolling) MTB_TRY(launch_grid5<P>(g2, s.err, st));
     else MTB_TRY(launch_grid3<P>(g2, p->gridder_threads, st));
     Grid4Args g4;
@@ -1879,14 +1897,14 @@ static int run_grid(const mtb_grid_params *p, const GridPlan &plan, const float2
     g4.bt = plan.bt;
     g4.err = s.err;
     if (bulk) MTB_TRY(launch_grid4<P>(g4, st));
-    if ((bulk || rolling) && check_gridder()) {
+    if ((bulk || rolling) && check_gridder() && !capturing(st)) {
         int e = 0;
         MTB_CUDA_TRY(cudaMemcpyAsync(&e, s.err, sizeof(int), cudaMemcpyDeviceToHost, st));
         MTB_CUDA_TRY(cudaStreamSynchronize(st));
         if (e) return MTB_ERR_KERNEL;
     }
     if (p->gridder_end_event) MTB_CUDA_TRY(cudaEventRecord((cudaEvent_t)p->gridder_end_event, st));
-    return finish_grid<P>(p, grid, grid_lo, normalizer, stats, s, st);
+    return finish_grid<P>(p, grid, grid_lo, normalizer, stats, s, s.err, st);
 }
 
 // PreProcessUVW's seven outputs in the reference's layout
@@ -2078,10 +2096,11 @@ static int run_batch(const mtb_grid_job *jobs, int njobs, const GridPlan *plans,
     g2.items = items;
     g2.n_items = n_total;
     g2.counter = counter;
-    if (p0.gridder == 5) {
-        MTB_CUDA_TRY(cudaMemsetAsync(spaces[0].err, 0, sizeof(int), st));
+    // the batch's gridder error flag (read by every image's k_finish)
+    MTB_CUDA_TRY(cudaMemsetAsync(spaces[0].err, 0, sizeof(int), st));
+    if (gridder_of(&p0) == 5) {
         MTB_TRY(launch_grid5<P>(g2, spaces[0].err, st));
-        if (check_gridder()) {
+        if (check_gridder() && !capturing(st)) {
             int e = 0;
             MTB_CUDA_TRY(cudaMemcpyAsync(&e, spaces[0].err, sizeof(int), cudaMemcpyDeviceToHost, st));
             MTB_CUDA_TRY(cudaStreamSynchronize(st));
@@ -2095,7 +2114,7 @@ static int run_batch(const mtb_grid_job *jobs, int njobs, const GridPlan *plans,
         const mtb_grid_job &J = jobs[j];
         if (J.nrecords == 0) continue;
         MTB_TRY(finish_grid<P>(&J.params, (float *)J.d_grid, (float *)J.d_grid_lo, J.d_normalizer, J.d_stats,
-                               spaces[j], st));
+                               spaces[j], spaces[0].err, st));
     }
     return MTB_OK;
 }
