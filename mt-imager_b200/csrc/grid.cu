@@ -24,8 +24,13 @@
 //                  with the record's gridder layout.
 //   k_pad_expand   row-padded copy of the kernel table (rows of S + 1 taps,
 //                  16-byte aligned), every tap in {re,re,im,im} form.
-//   k_grid3        default gridder: persistent blocks take work items (up to 512
-//                  records of one bin) from a queue.  Threads own support-box
+//   k_grid5        default gridder: persistent blocks take work items (up to 256
+//                  records of one bin) from a queue; one warp stages the item
+//                  two ahead into the second of two shared-memory buffers
+//                  (mbarrier hand-offs), so threads never wait at a block
+//                  barrier.  The jobs of an item are those of k_grid3.
+//   k_grid3        the same jobs with block-wide staging of one item at a time
+//                  (items of up to 512 records; gridder = 3).  Threads own support-box
 //                  positions (Romein's assignment: cell x belongs to the slot
 //                  with a == x mod M), accumulate V * C in registers with packed
 //                  f32x2 FMAs while their cell is unchanged, and flush a cell
