@@ -165,6 +165,30 @@ def test_chunk_invariance(oracle):
     assert np.abs(a - b).max() <= 1e-9 * np.abs(a).max()
 
 
+def test_hermitian_mirror_grids_identically(oracle):
+    """A visibility measured on (u, v, w) equals the conjugate of the one on
+    (-u, -v, -w).  PreProcessUVW folds every w<0 record onto -uvw with its
+    imaginary part negated (WProjPreProcessUVW.cu:160-175), so a chunk and
+    its mirror (uvw negated, visibilities conjugated) must give the same
+    decisions, the same grid and the same normaliser, bit for bit."""
+    obs, setup = synth.small_config(seed=11, n_ant=8, ntimes=40, nx=64, wplanes=4, flag_frac=0.2)
+    keep = obs.uvw[2] != 0                     # w = 0 exactly is not folded (w < 0 is false for -0)
+    uvw = np.ascontiguousarray(obs.uvw[:, keep])
+    f = obs.freq_over_c(0)[keep]
+    vis, wts, flg = obs.vis[0][keep], obs.weights[0][keep], obs.flags[0][keep]
+    geo = oracle.geometry_for(setup)
+    kern = oracle.wkernels(geo)
+    g1, n1, p1 = oracle.grid_chunk(uvw, f, vis, wts, flg, geo, kern)
+    g2, n2, p2 = oracle.grid_chunk(-uvw, f, np.conj(vis), wts, flg, geo, kern)
+    assert p1["togrid"].sum() > 0 and (p1["imgmult"] == -1).any() and (p1["imgmult"] == 1).any()
+    for key in ("loc", "convidx", "togrid", "compress", "support", "plane", "offx", "offy"):
+        assert np.array_equal(p1[key], p2[key]), key
+    used = (p1["togrid"] | p1["compress"]) == 1      # a rejected record's multiplier is not used
+    assert np.array_equal(p1["imgmult"][used], -p2["imgmult"][used])
+    assert np.array_equal(n1, n2)
+    assert np.array_equal(g1, g2)
+
+
 def test_odd_and_even_sampling_layout(oracle):
     for s in (3, 5, 4):
         geo = small_geo(oracle, s=s, nw=2)
