@@ -50,11 +50,30 @@ def _compile(src, out, extra=()):
     return out
 
 
+def _port_path():
+    """The CPU port is built with -march=native, so its file name carries a
+    digest of this host's CPU model and flags: a copy built on another CPU
+    (whose instructions this one may lack) is never loaded; it is rebuilt."""
+    import hashlib
+    key = ""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith(("model name", "flags")):
+                    key += line
+                if line.startswith("flags"):
+                    break
+    except OSError:
+        pass
+    tag = hashlib.sha1(key.encode()).hexdigest()[:12] if key else "generic"
+    return os.path.join(BUILD, "libcpu_port-%s.so" % tag)
+
+
 def build():
     """Compile the oracle (and the FP32 CPU port) shared libraries."""
     _compile(SRC, os.path.join(BUILD, "liboracle_wproj.so"))
     if os.path.exists(PORT_SRC):
-        _compile(PORT_SRC, os.path.join(BUILD, "libcpu_port.so"), extra=("-O3", "-march=native"))
+        _compile(PORT_SRC, _port_path(), extra=("-O3", "-march=native"))
 
 
 def lib():
@@ -90,7 +109,7 @@ def port():
     the CPU baseline bench.py times."""
     global _port
     if _port is None:
-        path = _compile(PORT_SRC, os.path.join(BUILD, "libcpu_port.so"), extra=("-O3", "-march=native"))
+        path = _compile(PORT_SRC, _port_path(), extra=("-O3", "-march=native"))
         P = ctypes.CDLL(path)
         i, p, f = ctypes.c_int, ctypes.c_void_p, ctypes.c_float
         P.port_threads.restype = i
