@@ -122,3 +122,24 @@ def test_kernel_builders_refuse_a_cpu_device():
         build_wkernels(wkernel_params(64, 64, 1e-4, 1e-4, 4, 4), device="cpu")
     with pytest.raises(ValueError):
         build_taper_kernels(64, 64, 1e-4, 1e-4, device="cpu")
+
+
+def test_entry_points_report_a_missing_device():
+    """Without a CUDA device the entry points that need one return
+    MTB_ERR_CUDA (no host fallback, no crash), and the engine calls refuse
+    null handles before touching the device."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a CUDA device is present")
+    lib = L.load()
+    h = ctypes.c_void_p(123)
+    assert lib.mtb_engine_create(None, ctypes.byref(h)) == L.MTB_ERR_CUDA
+    assert h.value is None                      # no engine handed out on failure
+    t = ctypes.c_double(-1.0)
+    assert lib.mtb_calibrate_fp32(ctypes.byref(t), None) == L.MTB_ERR_CUDA
+    assert lib.mtb_status_string(L.MTB_ERR_CUDA)
+    ticket = ctypes.c_longlong()
+    req = L.ImageRequest()
+    assert lib.mtb_engine_submit(None, ctypes.byref(req), ctypes.byref(ticket)) == L.MTB_ERR_NULL
+    assert lib.mtb_engine_wait(None, 1, ctypes.byref(L.ImageResult())) == L.MTB_ERR_NULL
+    assert lib.mtb_engine_destroy(None) == L.MTB_ERR_NULL
