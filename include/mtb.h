@@ -95,8 +95,12 @@ typedef struct mtb_wkernel_info {
     size_t workspace_bytes;  /* workspace mtb_wkernel_build needs                      */
 } mtb_wkernel_info;
 
-/* Host-only: derived scalars and buffer sizes.  Replaces the parameter logic
- * of WProjectionConvFunction's constructor (WProjectionConvFunction.cpp:90-160). */
+/* Derived scalars and buffer sizes; launches nothing and enqueues no stream
+ * work, but needs the current device: the workspace size includes the work
+ * area of the batched cuFFT plan, which is created here (and cached for
+ * mtb_wkernel_build).  Without a device it returns MTB_ERR_CUDA.  Replaces the
+ * parameter logic of WProjectionConvFunction's constructor
+ * (WProjectionConvFunction.cpp:90-160). */
 int mtb_wkernel_query(const mtb_wkernel_params *p, mtb_wkernel_info *info);
 
 /* Builds every w-plane kernel in one pass (all planes batched through cuFFT Z2Z,

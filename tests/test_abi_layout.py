@@ -137,6 +137,9 @@ def test_entry_points_report_a_missing_device():
     assert h.value is None                      # no engine handed out on failure
     t = ctypes.c_double(-1.0)
     assert lib.mtb_calibrate_fp32(ctypes.byref(t), None) == L.MTB_ERR_CUDA
+    # the w-kernel query sizes the cuFFT work area, which needs the device
+    p = L.WKernelParams(nx=256, ny=256, l_increment=1e-5, m_increment=1e-5, wplanes=32, sampling=8)
+    assert lib.mtb_wkernel_query(ctypes.byref(p), ctypes.byref(L.WKernelInfo())) == L.MTB_ERR_CUDA
     assert lib.mtb_status_string(L.MTB_ERR_CUDA)
     ticket = ctypes.c_longlong()
     req = L.ImageRequest()
