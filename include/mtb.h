@@ -181,9 +181,12 @@ typedef struct mtb_grid_stats {
 int mtb_grid_workspace_size(const mtb_grid_params *p, const int *h_conv_info, int nrecords, size_t *bytes);
 
 /* Grids one chunk of records into the accumulating grid: one WImager::calculate
- * (WImager.cpp:271-290).  FP64 coordinates; FP32 tile accumulation in shared
- * memory; each tile merged into the grid once.  With d_grid_lo non-NULL the merge
- * is compensated: d_grid + d_grid_lo carries the running sum to about twice
+ * (WImager.cpp:271-290).  FP64 coordinates and oversampling offsets; records
+ * binned by (support bucket, uv tile); FP32 sums in registers, each flushed
+ * when its grid cell changes (merge = 0, the default), or into a shared-memory
+ * tile window merged once per work item (merge = 1).  With d_grid_lo non-NULL
+ * the call's flushes go to a delta grid that one pass merges into
+ * d_grid + d_grid_lo with a TwoSum, carrying the running sum to about twice
  * FP32 precision (pass the same d_grid_lo to mtb_finalize).  d_stats (device
  * memory, may be NULL) accumulates the four record statistics.
  *   h_conv_info   host int [wplanes][2] as returned by mtb_wkernel_build */
