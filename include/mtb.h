@@ -271,8 +271,9 @@ int mtb_grid_autotune(mtb_grid_job *jobs, int njobs, void *d_workspace, size_t w
  * by a work queue over (image, support bucket, tile) bins.  Every image is
  * preprocessed and binned as by mtb_grid, its work items are concatenated into
  * one queue, and the gridder takes each item's image from it.  The result for
- * every image equals mtb_grid's.  All work is enqueued on `stream`; the call
- * can be captured into a CUDA graph. */
+ * every image equals mtb_grid's to the rounding of the FP32 reductions (bit
+ * for bit with exact_delta).  All work is enqueued on `stream`; the call can
+ * be captured into a CUDA graph. */
 int mtb_grid_batch(const mtb_grid_job *jobs, int njobs, void *d_workspace, size_t workspace_bytes,
                    mtb_stream_t stream);
 
