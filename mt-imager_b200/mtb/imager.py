@@ -310,7 +310,7 @@ def grid_batch(entries, workspace=None, stream=None):
     """Grid one chunk into each of several images with one persistent gridder
     launch (mtb_grid_batch).  entries: (WProjectionImager, uvw, freq, vis,
     weights, flags) with device tensors in the layouts of grid_device; every
-    imager must have the same npol and gridder_threads.  Returns the workspace
+    imager must have the same npol, gridder_threads and gridder.  Returns the workspace
     tensor so a caller can pass it back (or keep it alive across a CUDA graph
     replay)."""
     if not entries:
