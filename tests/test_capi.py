@@ -48,3 +48,26 @@ def test_python_binding_matches_header():
     # struct layouts the binding passes by pointer
     assert ctypes.sizeof(_lib.WKernelParams) == 48
     assert ctypes.sizeof(_lib.GridStats) == 32
+
+
+def test_cmake_target_matches_build_script(tmp_path):
+    """mt-imager_b200/CMakeLists.txt (the target a CMake host project adds)
+    configures, compiles every csrc/*.cu that build.py compiles, and targets
+    sm_100a only.  Configure step only: no compilation."""
+    import shutil
+    import subprocess
+    import pytest
+    cmake = shutil.which("cmake")
+    nvcc = os.path.join(os.environ.get("CUDA_HOME", "/usr/local/cuda"), "bin", "nvcc")
+    if cmake is None or not os.path.exists(nvcc):
+        pytest.skip("cmake or nvcc not available")
+    r = subprocess.run([cmake, "-S", os.path.join(ROOT, "mt-imager_b200"), "-B", str(tmp_path),
+                        "-DCMAKE_CUDA_COMPILER=" + nvcc], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    flags = open(tmp_path / "CMakeFiles" / "mtb.dir" / "flags.make").read()
+    assert "arch=compute_100a,code=[sm_100a]" in flags
+    assert not re.search(r"sm_(?!100a)\d+", flags)
+    build_make = open(tmp_path / "CMakeFiles" / "mtb.dir" / "build.make").read()
+    compiled = set(re.findall(r"csrc/(\w+)\.cu\.o:", build_make))
+    sources = {os.path.basename(s)[:-3] for s in glob.glob(os.path.join(ROOT, "mt-imager_b200", "csrc", "*.cu"))}
+    assert compiled == sources
