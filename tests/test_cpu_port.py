@@ -38,10 +38,13 @@ def _port_chunk(O, obs, geo, kern, npol, threads=None):
     return grid, norm, st
 
 
-@pytest.mark.parametrize("npol,sampling,wplanes,seed", [(4, 4, 8, 4), (4, 3, 4, 6), (2, 8, 8, 8), (1, 4, 2, 9)])
-def test_port_matches_oracle(oracle, npol, sampling, wplanes, seed):
+@pytest.mark.parametrize("npol,sampling,wplanes,seed,ny", [(4, 4, 8, 4, 128), (4, 3, 4, 6, 128), (2, 8, 8, 8, 128),
+                                                         (1, 4, 2, 9, 128), (4, 4, 8, 10, 96)])
+def test_port_matches_oracle(oracle, npol, sampling, wplanes, seed, ny):
+    import dataclasses
     obs, setup = synth.small_config(seed=seed, n_ant=10, ntimes=60, nx=128, cell_arcsec=20, wplanes=wplanes,
                                     sampling=sampling, flag_frac=0.2)
+    setup = dataclasses.replace(setup, ny=ny)
     geo = oracle.geometry_for(setup)
     kern = oracle.wkernels(geo)
     g, n, pre = oracle.grid_chunk(obs.uvw, obs.freq_over_c(0), obs.vis[0][:, :npol], obs.weights[0][:, :npol],

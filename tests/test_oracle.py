@@ -202,3 +202,25 @@ def test_odd_and_even_sampling_layout(oracle):
         assert np.all(pre["offx"][g] < T) and np.all(pre["offy"][g] < T) and np.all(pre["offx"][g] >= 0)
         end = pre["convidx"][g] + pre["support"][g] ** 2
         assert np.all(end <= k["table"].size)
+
+
+@pytest.mark.parametrize("ny", [96, 160])
+def test_rectangular_image_places_source(oracle, ny):
+    """image.nx and image.ny are independent (ConfigurationManager.cpp:170-202):
+    Δv = 1/(Δm·ny), the taper correction of each axis uses its own size and
+    the Stokes rows are flipped over ny.  An off-centre point source lands on
+    the pixel the FP64 DFT puts it on."""
+    import dataclasses
+    obs, setup = synth.small_config(seed=3, n_ant=10, ntimes=60, nx=128, cell_arcsec=20, flag_frac=0.0)
+    setup = dataclasses.replace(setup, ny=ny)
+    dl = setup.dl
+    src = np.array([[12 * dl, -7 * dl, 1.0, 0.0, 0.0, 0.0]])
+    obs.vis[0] = synth.predict_vis(obs.uvw.astype(np.float64), obs.freqs_hz[0], src).astype(np.complex64)
+    img, _, _ = oracle.image_channel(obs, 0, setup)
+    d = oracle.dft_image(obs, 0, setup)
+    assert img.shape == d.shape == (4, ny, 128)
+    pk = (ny - 1 - (ny // 2 - 7), 64 + 12)
+    assert np.unravel_index(np.argmax(d[0]), d[0].shape) == pk
+    assert np.unravel_index(np.argmax(img[0]), img[0].shape) == pk
+    assert abs(img[0][pk] - d[0][pk]) < 0.05        # method error of the reference's kernels
+    assert np.sqrt(np.mean((img[0] - d[0]) ** 2)) < 0.02
