@@ -71,3 +71,13 @@ def test_cmake_target_matches_build_script(tmp_path):
     compiled = set(re.findall(r"csrc/(\w+)\.cu\.o:", build_make))
     sources = {os.path.basename(s)[:-3] for s in glob.glob(os.path.join(ROOT, "mt-imager_b200", "csrc", "*.cu"))}
     assert compiled == sources
+
+
+def test_missing_library_fails_loudly(tmp_path, monkeypatch):
+    """No CPU fallback: without libmtb.so the binding raises instead of
+    returning a stand-in."""
+    import pytest
+    from mtb import _lib
+    monkeypatch.setattr(_lib, "_lib", None)
+    with pytest.raises(RuntimeError, match="libmtb.so not found"):
+        _lib.load(str(tmp_path / "libmtb.so"))
