@@ -146,3 +146,51 @@ def test_entry_points_report_a_missing_device():
     assert lib.mtb_engine_submit(None, ctypes.byref(req), ctypes.byref(ticket)) == L.MTB_ERR_NULL
     assert lib.mtb_engine_wait(None, 1, ctypes.byref(L.ImageResult())) == L.MTB_ERR_NULL
     assert lib.mtb_engine_destroy(None) == L.MTB_ERR_NULL
+
+
+def _valid_grid_params():
+    p = L.GridParams()
+    p.nx = p.ny = 1024
+    p.npol, p.sampling, p.wplanes = 4, 4, 1
+    p.u_increment = p.v_increment = p.w_sq_increment = 1.0
+    return p
+
+
+@pytest.mark.parametrize("field,value,status", [
+    ("nx", 65536, L.MTB_ERR_BAD_SHAPE),        # with ny = 65536: 2^32 cells, above the 2^31-cell limit
+    ("npol", 3, L.MTB_ERR_BAD_SHAPE),
+    ("nx", 1, L.MTB_ERR_BAD_PARAM),
+    ("sampling", 0, L.MTB_ERR_BAD_PARAM),
+    ("wplanes", 0, L.MTB_ERR_BAD_PARAM),
+    ("u_increment", 0.0, L.MTB_ERR_BAD_PARAM),
+    ("w_sq_increment", float("nan"), L.MTB_ERR_BAD_PARAM),
+    ("merge", 3, L.MTB_ERR_BAD_PARAM),
+    ("gridder_threads", 384, L.MTB_ERR_BAD_PARAM),
+    ("gridder", 4, L.MTB_ERR_BAD_PARAM),
+    ("max_chunk", -1, L.MTB_ERR_BAD_PARAM),
+])
+def test_grid_parameter_refusals(mtblib, field, value, status):
+    """Out-of-range gridding parameters are refused on the host with the
+    status the reference's ValidationException cases map to, before any
+    device work (so without a GPU too)."""
+    p = _valid_grid_params()
+    if field == "nx" and value == 65536:
+        p.ny = 65536                            # 2^32 cells
+    setattr(p, field, value)
+    info = (ctypes.c_int * 2)(7, 0)
+    n = ctypes.c_size_t(0)
+    rc = mtblib.mtb_grid_workspace_size(ctypes.byref(p), ctypes.cast(info, ctypes.c_void_p), 1000, ctypes.byref(n))
+    assert rc == status
+
+
+def test_grid_refuses_negative_records_and_rolling_512(mtblib):
+    info = (ctypes.c_int * 2)(7, 0)
+    n = ctypes.c_size_t(0)
+    p = _valid_grid_params()
+    assert mtblib.mtb_grid_workspace_size(ctypes.byref(p), ctypes.cast(info, ctypes.c_void_p), -1,
+                                          ctypes.byref(n)) == L.MTB_ERR_BAD_SHAPE
+    p.gridder, p.gridder_threads = 5, 512     # the rolling-items gridder runs 256-thread blocks only
+    assert mtblib.mtb_grid_workspace_size(ctypes.byref(p), ctypes.cast(info, ctypes.c_void_p), 10,
+                                          ctypes.byref(n)) == L.MTB_ERR_BAD_PARAM
+    assert mtblib.mtb_grid_workspace_size(None, ctypes.cast(info, ctypes.c_void_p), 10,
+                                          ctypes.byref(n)) == L.MTB_ERR_NULL
