@@ -194,3 +194,17 @@ def test_grid_refuses_negative_records_and_rolling_512(mtblib):
                                           ctypes.byref(n)) == L.MTB_ERR_BAD_PARAM
     assert mtblib.mtb_grid_workspace_size(None, ctypes.cast(info, ctypes.c_void_p), 10,
                                           ctypes.byref(n)) == L.MTB_ERR_NULL
+
+
+@pytest.mark.parametrize("nx,ny,npol,s,pol,status", [
+    (1024, 1024, 3, 8, 0, L.MTB_ERR_BAD_SHAPE),
+    (1, 1024, 4, 8, 0, L.MTB_ERR_BAD_PARAM),
+    (1024, 1024, 4, 0, 0, L.MTB_ERR_BAD_PARAM),
+    (1024, 1024, 4, 8, 2, L.MTB_ERR_BAD_PARAM),      # neither linear nor circular feeds
+    (65536, 65536, 4, 8, 0, L.MTB_ERR_BAD_SHAPE),    # 2^32 cells
+])
+def test_finalize_parameter_refusals(mtblib, nx, ny, npol, s, pol, status):
+    p = L.FinalizeParams(nx=nx, ny=ny, npol=npol, sampling=s, pol_type=pol)
+    n = ctypes.c_size_t(0)
+    assert mtblib.mtb_finalize_workspace_size(ctypes.byref(p), ctypes.byref(n)) == status
+    assert mtblib.mtb_finalize(ctypes.byref(p), None, None, None, None, None, 0, None) == status
