@@ -208,3 +208,20 @@ def test_finalize_parameter_refusals(mtblib, nx, ny, npol, s, pol, status):
     n = ctypes.c_size_t(0)
     assert mtblib.mtb_finalize_workspace_size(ctypes.byref(p), ctypes.byref(n)) == status
     assert mtblib.mtb_finalize(ctypes.byref(p), None, None, None, None, None, 0, None) == status
+
+
+@pytest.mark.parametrize("kw,status", [
+    (dict(trial_support=32), L.MTB_ERR_BAD_PARAM),            # supports are odd (WProjPreFFTconvFunc.cpp:77)
+    (dict(nx=1), L.MTB_ERR_BAD_PARAM),
+    (dict(l_increment=0.0), L.MTB_ERR_BAD_PARAM),
+    (dict(wplanes=0), L.MTB_ERR_BAD_PARAM),
+    (dict(nx=4, ny=4), L.MTB_ERR_BAD_PARAM),                  # trial support 4/8 -> 1: no kernel
+    (dict(trial_support=6001), L.MTB_ERR_BAD_SHAPE),          # (S_t * s)^2 screen above 2^31 elements
+])
+def test_wkernel_parameter_refusals(mtblib, kw, status):
+    """The w-kernel parameters are checked on the host before the cuFFT plan
+    (and so before any device is needed)."""
+    base = dict(nx=256, ny=256, l_increment=1e-5, m_increment=1e-5, wplanes=32, sampling=8)
+    base.update(kw)
+    p = L.WKernelParams(**base)
+    assert mtblib.mtb_wkernel_query(ctypes.byref(p), ctypes.byref(L.WKernelInfo())) == status
