@@ -224,3 +224,30 @@ def test_rectangular_image_places_source(oracle, ny):
     assert np.unravel_index(np.argmax(img[0]), img[0].shape) == pk
     assert abs(img[0][pk] - d[0][pk]) < 0.05        # method error of the reference's kernels
     assert np.sqrt(np.mean((img[0] - d[0]) ** 2)) < 0.02
+
+
+@pytest.mark.parametrize("nx,cell,nw,s,st,ms", [(4096, 2.4, 128, 8, 67, 65), (512, 6.0, 16, 3, 0, 0)])
+def test_kernel_table_symmetries(oracle, nx, cell, nw, s, st, ms):
+    """Size-independent properties of the kernel tables, the first case at the
+    mid-size geometry (4096^2, 128 w-planes, oversampling 8, trial support 67).
+    The taper x w-screen depends on l^2 + m^2 only (WProjPreFFTconvFunc.cu:
+    34-105), so every plane's oversampled kernel is unchanged by uv -> -uv and
+    by u <-> v; supports are odd, within the cap and grow with |w|; the w = 0
+    plane has DC 1; ConvSums are the sub-kernels' real sums."""
+    dl = cell * synth.ARCSEC
+    geo = oracle.kernel_geometry(nx, nx, dl, dl, nw, s, st, ms)
+    k = oracle.wkernels(geo)
+    T = geo["T"]
+    sup = k["supports"]
+    assert np.all(sup % 2 == 1) and np.all(sup <= geo["support_cap"]) and np.all(np.diff(sup) >= 0)
+    assert sup[-1] > sup[0]
+    for pl in range(nw):
+        S, o = int(sup[pl]), int(k["conv_info"][pl, 1])
+        c = k["table"][o:o + T * T * S * S].reshape(T, T, S, S)
+        pk = np.abs(c).max()
+        assert np.abs(c - c[::-1, ::-1, ::-1, ::-1]).max() <= 1e-13 * pk
+        assert np.abs(c - c.transpose(1, 0, 3, 2)).max() <= 1e-13 * pk
+        assert np.allclose(k["conv_sums"][pl], c.real.reshape(T * T, -1).sum(axis=1), rtol=0, atol=1e-12)
+    S0 = int(sup[0])
+    c0 = k["table"][:T * T * S0 * S0].reshape(T, T, S0, S0)
+    assert abs(c0[s // 2, s // 2, S0 // 2, S0 // 2] - 1.0) < 1e-12
