@@ -251,3 +251,39 @@ def test_kernel_table_symmetries(oracle, nx, cell, nw, s, st, ms):
     S0 = int(sup[0])
     c0 = k["table"][:T * T * S0 * S0].reshape(T, T, S0, S0)
     assert abs(c0[s // 2, s // 2, S0 // 2, S0 // 2] - 1.0) < 1e-12
+
+
+def test_w_negative_cross_hands_are_not_exchanged(oracle):
+    """The reference conjugates a w<0 record polarisation by polarisation
+    (imaginary part x -1, common.hcu:80-104, after WProjPreProcessUVW.cu:
+    170-175) without exchanging XY and YX.  For a real sky conj(XY(u)) is
+    YX(-u), so such a record adds its Stokes V with the opposite sign (I, Q
+    and U are symmetric in the cross hands).  The oracle, and the path it
+    pins, keep this: V at a polarised source is V * (N+ - N-) / N of the
+    gridded records, and it is recovered in full when every record has w >= 0."""
+    obs, setup = synth.small_config(seed=3, n_ant=10, ntimes=60, nx=128, cell_arcsec=20, flag_frac=0.0)
+    dl = setup.dl
+    I, Q, U, V = 1.0, 0.3, -0.2, 0.1
+    src = np.array([[12 * dl, -7 * dl, I, Q, U, V]])
+    obs.vis[0] = synth.predict_vis(obs.uvw.astype(np.float64), obs.freqs_hz[0], src).astype(np.complex64)
+    geo = oracle.geometry_for(setup)
+    kern = oracle.wkernels(geo)
+    pk = (127 - (64 - 7), 64 + 12)
+    img, _, _ = oracle.image_channel(obs, 0, setup, kern, geo)
+    d = oracle.dft_image(obs, 0, setup, geo, kern)
+    for p, want in enumerate((I, Q, U)):
+        assert abs(d[p][pk] - want) < 2e-3
+        assert abs(img[p][pk] - want * img[0][pk] / I) < 2e-3
+    pre = oracle.preprocess(obs.uvw, obs.freq_over_c(0), obs.weights[0], obs.flags[0], geo, kern)
+    w = obs.uvw[2][(pre["togrid"] | pre["compress"]) == 1]
+    frac = ((w >= 0).sum() - (w < 0).sum()) / w.size
+    assert 0.0 < frac < 0.5
+    assert abs(d[3][pk] - V * frac * d[0][pk]) < 1e-4
+    assert abs(img[3][pk] - V * frac * img[0][pk]) < 1e-4
+    # the same source seen by the records with w >= 0 only: V in full
+    keep = obs.uvw[2] >= 0
+    obs.uvw = np.ascontiguousarray(obs.uvw[:, keep])
+    for name in ("vis", "weights", "flags"):
+        getattr(obs, name)[0] = np.ascontiguousarray(getattr(obs, name)[0][keep])
+    d = oracle.dft_image(obs, 0, setup, geo, kern)
+    assert abs(d[3][pk] - V * d[0][pk]) < 2e-3
