@@ -86,3 +86,18 @@ def test_psf_image_matches_oracle(oracle):
     c = (setup.ny - 1 - setup.ny // 2, setup.nx // 2)
     assert abs(img[0][c] - 1.0) < 1e-3                 # normalised PSF peaks at 1 in the centre
     assert np.sqrt(np.mean((img[0] - img_o[0]) ** 2)) <= IMAGE_RMS_TOL * np.abs(img_o[0]).max()
+
+
+def test_oracle_psf_known_answer(oracle):
+    """psf=true grids every visibility as 1 + 0i (VisibilityForPSFStorageManager.cpp:
+    65-77): the normalised PSF peaks at 1 at the phase centre, and the FP64 DFT
+    of the same records agrees with it (CPU)."""
+    obs, setup = synth.small_config(seed=52, n_ant=12, ntimes=60, nx=128, cell_arcsec=20, flag_frac=0.1)
+    obs_psf = synth.Observation(**{**obs.__dict__, "vis": [np.ones_like(obs.vis[0])]})
+    img, _, _ = oracle.image_channel(obs_psf, 0, setup)
+    d = oracle.dft_image(obs_psf, 0, setup)
+    c = (setup.ny - 1 - setup.ny // 2, setup.nx // 2)
+    assert abs(d[0][c] - 1.0) < 1e-12
+    assert abs(img[0][c] - 1.0) < 1e-3
+    assert np.unravel_index(np.argmax(img[0]), img[0].shape) == c
+    assert np.sqrt(np.mean((img[0] - d[0]) ** 2)) < 0.02
