@@ -75,3 +75,17 @@ def test_port_result_does_not_depend_on_threads(oracle):
     assert np.array_equal(s1, s3)
     assert np.array_equal(g1, g3)
     assert np.allclose(n1, n3, rtol=1e-6)
+
+
+def test_port_empty_and_fully_flagged_chunks(oracle):
+    obs, setup = synth.small_config(seed=13, n_ant=6, ntimes=20, nx=64, wplanes=4, sampling=4, flag_frac=0.0)
+    geo = oracle.geometry_for(setup)
+    kern = oracle.wkernels(geo)
+    obs.flags[0][:] = 1
+    grid, norm, st = _port_chunk(oracle, obs, geo, kern, 4)
+    assert not st.any() and not grid.any() and not norm.any()
+    empty = synth.Observation(**{**obs.__dict__, "uvw": np.zeros((3, 0), np.float32),
+                                 "vis": [obs.vis[0][:0]], "weights": [obs.weights[0][:0]],
+                                 "flags": [obs.flags[0][:0]]})
+    grid, norm, st = _port_chunk(oracle, empty, geo, kern, 4)
+    assert not st.any() and not grid.any() and not norm.any()
