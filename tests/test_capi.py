@@ -81,3 +81,25 @@ def test_missing_library_fails_loudly(tmp_path, monkeypatch):
     monkeypatch.setattr(_lib, "_lib", None)
     with pytest.raises(RuntimeError, match="libmtb.so not found"):
         _lib.load(str(tmp_path / "libmtb.so"))
+
+
+def test_c_program_uses_the_abi(tmp_path, mtblib):
+    """tests/cpp/host_abi.c, plain C99 built with gcc against include/ and
+    libmtb.so, calls the host-side entry points (ingest order, column gather,
+    status strings, parameter refusals) without Python or a GPU."""
+    import shutil
+    import subprocess
+    import pytest
+    cc = os.environ.get("CC", "gcc")
+    if shutil.which(cc) is None:
+        pytest.skip("no C compiler")
+    lib = os.path.join(ROOT, "mt-imager_b200")
+    cuda = os.environ.get("CUDA_HOME", "/usr/local/cuda")
+    exe = tmp_path / "host_abi"
+    subprocess.run([cc, "-std=c99", "-Wall", "-Wextra", "-Werror", "-O2",
+                    os.path.join(ROOT, "tests", "cpp", "host_abi.c"), "-o", str(exe),
+                    "-I", os.path.join(ROOT, "include"), "-L", lib, "-lmtb", "-Wl,-rpath," + lib,
+                    "-Wl,-rpath," + os.path.join(cuda, "lib64")], check=True)
+    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 0, r.stderr
+    assert r.stdout.strip() == "ok"
