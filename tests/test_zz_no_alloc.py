@@ -1,6 +1,13 @@
 """mtb_preprocess_uvw_noalloc (fixed device scratch, no workspace) against
 mtb_preprocess_uvw (caller workspace) on the same inputs.
 
+The entry point serves callers that must not allocate device memory: code
+running inside an allocator or memory-pool callback (where cudaMalloc would
+re-enter the allocator), a framework that partitions the device up front and
+hands plugins only the buffers it owns, a plugin whose host forbids
+allocation.  Its scratch is a fixed array in the library's device image, so
+it allocates nothing and refuses chunks above its stated capacity.
+
 The file name sorts last so the fixed scratch is exercised after every other
 test has used the library; two different chunks run back to back so a value
 left in the scratch by the first call would show up in the second.
