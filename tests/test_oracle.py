@@ -251,6 +251,8 @@ def test_kernel_table_symmetries(oracle, nx, cell, nw, s, st, ms):
     S0 = int(sup[0])
     c0 = k["table"][:T * T * S0 * S0].reshape(T, T, S0, S0)
     assert abs(c0[s // 2, s // 2, S0 // 2, S0 // 2] - 1.0) < 1e-12
+    # w = 0: the transform of a real, even taper is real
+    assert np.abs(c0.imag).max() <= 1e-12 * np.abs(c0).max()
 
 
 def test_w_negative_cross_hands_are_not_exchanged(oracle):
