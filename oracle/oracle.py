@@ -393,7 +393,7 @@ def stokes_and_corrections(sh, norm, geo, pol_type="linear"):
 
 
 # -------------------------------------------------------------- pipelines --
-def image_channel(obs, chan, setup, kern=None, geo=None, chunk=None):
+def image_channel(obs, chan, setup, kern=None, geo=None, chunk=None, pol_type="linear"):
     """Full W-projection image of one channel (optionally in record chunks)."""
     geo = geo or geometry_for(setup)
     kern = kern or wkernels(geo)
@@ -405,13 +405,14 @@ def image_channel(obs, chan, setup, kern=None, geo=None, chunk=None):
         b = min(R, a + chunk)
         g, n, _ = grid_chunk(obs.uvw[:, a:b], freq[a:b], obs.vis[chan][a:b], obs.weights[chan][a:b],
                              obs.flags[chan][a:b], geo, kern, g, n)
-    return finalize(g, n, geo), g, n
+    return finalize(g, n, geo, pol_type), g, n
 
 
-def dft_image(obs, chan, setup, geo=None, kern=None):
+def dft_image(obs, chan, setup, geo=None, kern=None, pol_type="linear"):
     """FP64 direct-DFT Stokes image of exactly the records the W-projection
     path grids, normalised by the gridded weight sum and flipped like the
-    reference's Stokes output (no taper or sinc correction applies)."""
+    reference's Stokes output (no taper or sinc correction applies).
+    pol_type "linear" or "circular" (PostIFFTStokesConverter.cu:42-90)."""
     geo = geo or geometry_for(setup)
     kern = kern or wkernels(geo)
     freq = obs.freq_over_c(chan)
@@ -427,11 +428,16 @@ def dft_image(obs, chan, setup, geo=None, kern=None):
     wsum = wts[gridded].sum(axis=0)
     re, im = out.real / wsum[:, None, None], out.imag / wsum[:, None, None]
     st = np.empty((P, geo["ny"], geo["nx"]))
-    if P == 4:
+    if P == 4 and pol_type == "linear":
         st[0] = (re[0] + re[3]) * 0.5
         st[1] = (re[0] - re[3]) * 0.5
         st[2] = (re[1] + re[2]) * 0.5
         st[3] = (im[1] - im[2]) * 0.5
+    elif P == 4:
+        st[0] = (re[0] + re[3]) * 0.5
+        st[1] = (re[1] + re[2]) * 0.5
+        st[2] = (im[2] - im[1]) * 0.5
+        st[3] = (re[0] - re[3]) * 0.5
     else:
         st[:] = re
     return st[:, ::-1, :]

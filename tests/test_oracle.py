@@ -289,3 +289,35 @@ def test_w_negative_cross_hands_are_not_exchanged(oracle):
         getattr(obs, name)[0] = np.ascontiguousarray(getattr(obs, name)[0][keep])
     d = oracle.dft_image(obs, 0, setup, geo, kern)
     assert abs(d[3][pk] - V * d[0][pk]) < 2e-3
+
+
+def test_circular_feeds_against_the_dft(oracle):
+    """Circular feeds (StokesConverter, PostIFFTStokesConverter.cu:72-90):
+    RR = I + V, LL = I - V, RL = Q - iU, LR = Q + iU, the convention under which
+    the converter's U = (Im LR - Im RL) / 2 is +U.  I, Q and V of a polarised
+    source come out in full; U, carried by the cross hands, is scaled by
+    (N+ - N-) / N like V with linear feeds (w<0 records are conjugated without
+    exchanging RL and LR)."""
+    obs, setup = synth.small_config(seed=3, n_ant=10, ntimes=60, nx=128, cell_arcsec=20, flag_frac=0.0)
+    dl = setup.dl
+    I, Q, U, V = 1.0, 0.3, -0.2, 0.1
+    l, m = 12 * dl, -7 * dl
+    f = obs.freqs_hz[0] / synth.C_LIGHT
+    u, v, w = obs.uvw.astype(np.float64) * f
+    ph = np.exp(-2j * np.pi * (u * l + v * m + w * (math.sqrt(1 - l * l - m * m) - 1.0)))
+    obs.vis[0] = np.stack([(I + V) * ph, (Q - 1j * U) * ph, (Q + 1j * U) * ph, (I - V) * ph], axis=1).astype(np.complex64)
+    geo = oracle.geometry_for(setup)
+    kern = oracle.wkernels(geo)
+    pk = (127 - (64 - 7), 64 + 12)
+    img, _, _ = oracle.image_channel(obs, 0, setup, kern, geo, pol_type="circular")
+    d = oracle.dft_image(obs, 0, setup, geo, kern, pol_type="circular")
+    pre = oracle.preprocess(obs.uvw, obs.freq_over_c(0), obs.weights[0], obs.flags[0], geo, kern)
+    ws = obs.uvw[2][(pre["togrid"] | pre["compress"]) == 1]
+    frac = ((ws >= 0).sum() - (ws < 0).sum()) / ws.size
+    for p, want in ((0, I), (1, Q), (3, V)):
+        assert abs(d[p][pk] - want) < 2e-3
+        assert abs(img[p][pk] - want * img[0][pk] / I) < 2e-3
+    assert abs(d[2][pk] - U * frac * d[0][pk]) < 1e-4
+    assert abs(img[2][pk] - U * frac * img[0][pk]) < 1e-4
+    for p in range(4):
+        assert np.sqrt(np.mean((img[p] - d[p]) ** 2)) < 0.02
