@@ -321,3 +321,23 @@ def test_circular_feeds_against_the_dft(oracle):
     assert abs(img[2][pk] - U * frac * img[0][pk]) < 1e-4
     for p in range(4):
         assert np.sqrt(np.mean((img[p] - d[p]) ** 2)) < 0.02
+
+
+def test_image_is_invariant_to_a_weight_scale(oracle):
+    """The grid and the normaliser (sum of ConvSums x weight, WImager.cpp:
+    196-197) both scale with the weights, so multiplying every weight by a
+    constant leaves the normalised image unchanged; per-record weights do
+    change it."""
+    obs, setup = synth.small_config(seed=17, n_ant=8, ntimes=40, nx=64, flag_frac=0.1)
+    a, ga, na = oracle.image_channel(obs, 0, setup)
+    obs2 = synth.Observation(**{**obs.__dict__, "weights": [obs.weights[0] * np.float32(2.5)]})
+    b, gb, nb = oracle.image_channel(obs2, 0, setup)
+    assert np.allclose(nb, 2.5 * na, rtol=1e-12)
+    assert np.abs(gb - 2.5 * ga).max() <= 1e-12 * np.abs(gb).max()
+    assert np.abs(b - a).max() <= 1e-10 * np.abs(a).max()     # FP64 rounding through the FFT and corrections
+    rng = np.random.default_rng(0)
+    obs3 = synth.Observation(**{**obs.__dict__, "weights": [(obs.weights[0] *
+                                                            rng.uniform(0.5, 2.0, obs.weights[0].shape)
+                                                            ).astype(np.float32)]})
+    c, _, _ = oracle.image_channel(obs3, 0, setup)
+    assert np.abs(c - a).max() > 1e-6 * np.abs(a).max()
