@@ -293,6 +293,7 @@ def main():
     ap.add_argument("--support-bucket", type=int, default=0)
     ap.add_argument("--max-chunk", type=int, default=0)
     ap.add_argument("--merge", type=int, default=0)
+    ap.add_argument("--gridder", type=int, default=0, help="mtb_grid_params.gridder (0: the library default)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-serve", action="store_true", help="skip the request-stream measurement")
@@ -403,7 +404,7 @@ def main():
     imagers = [WProjectionImager(n, n, dl, wplanes=spec["wplanes"], sampling=spec["sampling"],
                                  trial_support=spec["trial_support"], max_support=spec["max_support"],
                                  kernels=kern, device=dev, tile=args.tile, support_bucket=args.support_bucket,
-                                 max_chunk=args.max_chunk, merge=args.merge) for _ in freqs]
+                                 max_chunk=args.max_chunk, merge=args.merge, gridder=args.gridder) for _ in freqs]
     images = [torch.empty((4, n, n), dtype=torch.float32, device=dev) for _ in freqs]
     gev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in freqs]
     for im, ev in zip(imagers, gev):

@@ -162,7 +162,10 @@ typedef struct mtb_grid_params {
     int gridder;               /* 0: default (5, or 3 with gridder_threads 512);
                                   3: k_grid3 (block-wide staging of each work item);
                                   5: k_grid5 (two item buffers refilled by one warp, no
-                                  block barriers; items of at most 256 records).  A gridder
+                                  block barriers; items of at most 256 records);
+                                  7: k_grid7 (every warp streams its own jobs -- one work
+                                  item against 128 slots of its support box -- with no
+                                  block barriers; items of at most 512 records).  A gridder
                                   that could not complete sets the normaliser to NaN      */
     int flags_u8;              /* 0: d_flags is int32 [R][P] (the reference's layout); 1: it
                                   is one byte per flag, uint8 [R][P] (0 = keep, 1 = flagged;

@@ -554,7 +554,7 @@ static const int kG3KS = 4;                 // support-box slots per thread
 struct GridJobDesc {
     const int4 *wpos;
     const float4 *wvis4;
-    const float4 *table2;
+    const float4 *table2;  // padded table, taps as {re, re, im, im}
     float *grid;
     double *dgrid;         // compensated mode: FP64 delta grid of this call, else null
     const int *M;          // [kMaxBuckets] bucket moduli (device)
@@ -706,7 +706,7 @@ __global__ void k_pad_expand(const float2 *__restrict__ t, const int *__restrict
         const size_t dst = pb + (size_t)sub * S * (S + 1) + (size_t)y * (S + 1);
         for (int x = lane; x <= S; x += 32) {
             const float2 c = x < S ? t[src + x] : make_float2(0.f, 0.f);
-            t2[dst + x] = make_float4(c.x, c.x, c.y, c.y);
+            if (t2) t2[dst + x] = make_float4(c.x, c.x, c.y, c.y);
             if (pt) pt[dst + x] = c;
         }
     }
@@ -1245,15 +1245,74 @@ __global__ void __launch_bounds__(kG4Threads, 1) k_grid4(Grid4Args a) {
 // kernel returns.
 static const int kG5Chunk = 256;   // records of one work item (one buffer)
 
-template <int P>
-struct G5Layout {   // one item buffer, byte offsets
-    static constexpr size_t rec = 0;                                        // int4 [kG5Chunk]
-    static constexpr size_t vis = rec + (size_t)kG5Chunk * 16;              // float4 [kG5Chunk][P]
-    static constexpr size_t runend = vis + (size_t)kG5Chunk * P * 16;       // ushort [kG5Chunk]
-    static constexpr size_t start = runend + (size_t)kG5Chunk * 2;          // unsigned [kG5Chunk / 32]
-    static constexpr size_t item = start + (size_t)kG5Chunk / 8;            // int4 (y < 0: no more items)
-    static constexpr size_t bytes = (item + 16 + 15) & ~(size_t)15;
+template <int P, int CHUNK = kG5Chunk>
+struct G5Layout {   // one item buffer of CHUNK records, byte offsets
+    static constexpr int chunk = CHUNK;
+    static constexpr size_t rec = 0;                                        // int4 [CHUNK]
+    static constexpr size_t vis = rec + (size_t)CHUNK * 16;                 // float4 [CHUNK][P]
+    static constexpr size_t runend = vis + (size_t)CHUNK * P * 16;          // ushort [CHUNK]
+    static constexpr size_t start = runend + (size_t)CHUNK * 2;             // unsigned [CHUNK / 32]
+    static constexpr size_t item = (start + (size_t)CHUNK / 8 + 15) & ~(size_t)15;   // int4 (y < 0: no more items)
+    static constexpr size_t bytes = item + 16;
+    static_assert(CHUNK % 32 == 0, "run starts are kept as 32-bit words");
+    static_assert(rec % 16 == 0 && vis % 16 == 0 && item % 16 == 0 && bytes % 16 == 0,
+                  "16-byte fields (cp.async targets, int4 loads) must stay 16-byte aligned");
 };
+
+// Warp 0 of a rolling-items block: the next item of the queue (or the end
+// mark, item.y < 0) into item buffer B with its records, visibilities and run
+// ends, then one arrival per lane on the buffer's "full" mbarrier.
+template <int P, int CHUNK>
+__device__ __forceinline__ void stage_item(const Grid2Args &a, unsigned char *B, unsigned full_bar, int nitems,
+                                           int *err) {
+    using LY = G5Layout<P, CHUNK>;
+    const int lane = threadIdx.x & 31;
+    int4 *s_rec = (int4 *)(B + LY::rec);
+    float4 *s_v = (float4 *)(B + LY::vis);
+    unsigned short *s_runend = (unsigned short *)(B + LY::runend);
+    unsigned *s_start = (unsigned *)(B + LY::start);
+    int v = 0;
+    if (lane == 0) v = atomicAdd(a.counter, 1);
+    v = __shfl_sync(0xFFFFFFFFu, v, 0);
+    int4 it = make_int4(0, -1, 0, 0);
+    if (v < nitems) it = a.items[v];
+    if (it.y > CHUNK) {      // the plan caps items at CHUNK records
+        if (lane == 0) atomicExch(err, 2);
+        it.y = -1;
+    }
+    if (it.y >= 0) {
+        const GridJobDesc &J = a.jobs[it.w];
+        const int4 *grec = J.wpos;
+        const float4 *gvis = J.wvis4;
+        const int N = it.y;
+        for (int k = lane; k < N; k += 32) cp_async16(&s_rec[k], &grec[it.x + k]);
+        for (int k = lane; k < N * P; k += 32) cp_async16(&s_v[k], &gvis[(size_t)it.x * P + k]);
+        cp_async_commit();
+        cp_async_wait<0>();
+        __syncwarp();
+        for (int k0 = 0; k0 < N; k0 += 32) {      // run starts
+            const int k = k0 + lane;
+            bool st = false;
+            if (k < N) {
+                const int4 r = s_rec[k];
+                st = (k == 0) || r.x != s_rec[k - 1].x || r.w != s_rec[k - 1].w;
+            }
+            const unsigned m = __ballot_sync(0xFFFFFFFFu, st);
+            if (lane == 0) s_start[k0 >> 5] = m;
+        }
+        __syncwarp();
+        const int nw = (N + 31) >> 5;
+        for (int k = lane; k < N; k += 32) {      // run ends
+            int w = k >> 5;
+            unsigned m = (k & 31) == 31 ? 0u : s_start[w] & (0xFFFFFFFFu << ((k & 31) + 1));
+            while (m == 0 && ++w < nw) m = s_start[w];
+            s_runend[k] = (unsigned short)(m == 0 ? N : (w << 5) + __ffs(m) - 1);
+        }
+    }
+    if (lane == 0) *(int4 *)(B + LY::item) = it;
+    __syncwarp();
+    mbar_arrive(full_bar);                    // every lane: its copies and stores are done
+}
 
 template <int P>
 __global__ void __launch_bounds__(kG3Threads, 2) k_grid5(Grid2Args a, int *err) {
@@ -1264,7 +1323,7 @@ __global__ void __launch_bounds__(kG3Threads, 2) k_grid5(Grid2Args a, int *err) 
     ulonglong2 *const ring = (ulonglong2 *)(base + 2 * LY::bytes);      // [kG3Depth][kG3KS][T]
     __shared__ __align__(8) unsigned long long s_bars[4];                // full[2], empty[2]
     __shared__ volatile int s_abort;
-    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const int t = threadIdx.x, warp = t >> 5;
     const int nitems = a.n_items[0];
     const unsigned full0 = smem_u32(&s_bars[0]), empty0 = smem_u32(&s_bars[2]);
     if (t == 0) {
@@ -1276,64 +1335,14 @@ __global__ void __launch_bounds__(kG3Threads, 2) k_grid5(Grid2Args a, int *err) 
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
-
-    // warp 0: the next item of the queue (or the end mark) into buffer b
-    auto stage = [&](int b) {
-        unsigned char *B = base + b * LY::bytes;
-        int4 *s_rec = (int4 *)(B + LY::rec);
-        float4 *s_v = (float4 *)(B + LY::vis);
-        unsigned short *s_runend = (unsigned short *)(B + LY::runend);
-        unsigned *s_start = (unsigned *)(B + LY::start);
-        int v = 0;
-        if (lane == 0) v = atomicAdd(a.counter, 1);
-        v = __shfl_sync(0xFFFFFFFFu, v, 0);
-        int4 it = make_int4(0, -1, 0, 0);
-        if (v < nitems) it = a.items[v];
-        if (it.y > kG5Chunk) {   // the plan caps items at kG5Chunk records
-            if (lane == 0) atomicExch(err, 2);
-            it.y = -1;
-        }
-        if (it.y >= 0) {
-            const GridJobDesc &J = a.jobs[it.w];
-            const int4 *grec = J.wpos;
-            const float4 *gvis = J.wvis4;
-            const int N = it.y;
-            for (int k = lane; k < N; k += 32) cp_async16(&s_rec[k], &grec[it.x + k]);
-            for (int k = lane; k < N * P; k += 32) cp_async16(&s_v[k], &gvis[(size_t)it.x * P + k]);
-            cp_async_commit();
-            cp_async_wait<0>();
-            __syncwarp();
-            for (int k0 = 0; k0 < N; k0 += 32) {      // run starts
-                const int k = k0 + lane;
-                bool st = false;
-                if (k < N) {
-                    const int4 r = s_rec[k];
-                    st = (k == 0) || r.x != s_rec[k - 1].x || r.w != s_rec[k - 1].w;
-                }
-                const unsigned m = __ballot_sync(0xFFFFFFFFu, st);
-                if (lane == 0) s_start[k0 >> 5] = m;
-            }
-            __syncwarp();
-            const int nw = (N + 31) >> 5;
-            for (int k = lane; k < N; k += 32) {      // run ends
-                int w = k >> 5;
-                unsigned m = (k & 31) == 31 ? 0u : s_start[w] & (0xFFFFFFFFu << ((k & 31) + 1));
-                while (m == 0 && ++w < nw) m = s_start[w];
-                s_runend[k] = (unsigned short)(m == 0 ? N : (w << 5) + __ffs(m) - 1);
-            }
-        }
-        if (lane == 0) *(int4 *)(B + LY::item) = it;
-        __syncwarp();
-        mbar_arrive(full0 + 8 * b);                    // every lane: its copies and stores are done
-    };
     auto fail = [&]() {
         s_abort = 1;
         atomicExch(err, 1);
     };
 
     if (warp == 0) {
-        stage(0);
-        stage(1);
+        stage_item<P, LY::chunk>(a, base, full0, nitems, err);
+        stage_item<P, LY::chunk>(a, base + LY::bytes, full0 + 8, nitems, err);
     }
     for (int k = 0;; k++) {
         const int b = k & 1;
@@ -1357,9 +1366,408 @@ __global__ void __launch_bounds__(kG3Threads, 2) k_grid5(Grid2Args a, int *err) 
                 fail();
                 break;
             }
-            stage(b);                                  // item k + 2
+            stage_item<P, LY::chunk>(a, base + b * LY::bytes, full0 + 8 * b, nitems, err);   // item k + 2
         }
     }
+}
+
+// ---------------------------------------------------------------------------
+// Per-warp streaming gridder (k_grid7).
+//
+// Every warp works on its own: it takes a job from one ticket counter, grids
+// it and takes the next, with no barrier and no wait on another warp.  A job
+// is one (work item, part) pair: the item's records (one bin: one support
+// bucket of modulus M, at most kG7Chunk records) against one part of the
+// item's M x M support box, 128 slots (4 per lane).  Lane l of part w owns
+// the slots q = 128 w + 32 j + l (j < 4, q < M^2) at box position
+// (a, b) = (q mod M, q / M); for a record with corner (cx, cy) slot (a, b)
+// touches cell (cx + (a - cx) mod M, cy + (b - cy) mod M) (Romein's
+// assignment), so a slot keeps its cell while the record moves by less than a
+// cell and accumulates in registers until the cell changes.  The 32 lanes walk
+// the same records in the same order, so every branch on records and runs is
+// uniform across the warp.
+//
+// Pipeline of a job (distances in records; one cp.async group per record):
+//   record i + 2D: lanes 0..P copy the record and its visibilities from
+//                  global memory into the warp's record ring;
+//   record i + D:  every lane copies its slots' taps (each {re, re, im, im},
+//                  16 bytes: one shared-memory load feeds both packed FMAs of
+//                  a tap and polarisation) into its entries of the tap ring
+//                  (zero-fill for a slot outside the record's box);
+//   record i:      two packed FMAs per tap and polarisation.
+// A slot's cell and table offset change only between runs of records with
+// the same corner and support (k_gather flags the first record of a run):
+// the look-ahead computes the offsets when it reaches a run's first record and
+// leaves the run's cells in a per-lane FIFO, where the accumulation side picks
+// them up at the same record and flushes the slots whose cell changes.
+//
+// Jobs are ordered by segment (image, support bucket), largest support
+// first, so the longest jobs are handed out first.
+static const int kG7Warps = 8;
+static const int kG7Threads = 32 * kG7Warps;
+static const int kG7KS = 4;                        // slots per lane
+static const int kG7Depth = 4;                     // taps fetched this many records ahead
+static const int kG7RecRing = 16;                  // record-ring entries (records fetched 2 * kG7Depth ahead)
+static const int kG7PartSlots = 32 * kG7KS;        // slots of one job
+static const int kG7Chunk = 512;                   // records of one work item
+static const int kG7TapStride = kG7Depth * kG7KS * 32;   // tap-ring / FIFO entries per warp
+static_assert(kG7RecRing >= 2 * kG7Depth + 1, "the record ring holds every record in flight");
+
+// Jobs [job0, next.job0) are items [item0, item0 + n) x wu parts of modulus m.
+struct G7Segment {
+    int job0, item0, wu, m;
+};
+
+struct Grid7Args {
+    const int4 *items;        // work items; item.w selects the image
+    const G7Segment *segs;    // n_segs + 1 entries, the last holding the total job count
+    const int *n_segs;
+    int *counter;             // job tickets
+    GridJobDesc jobs[kMaxBatch];
+};
+
+// Where the segments of a launch come from: per image, its bucket item ranges
+// (k_bucket_bounds), its item count and its bucket moduli.
+struct G7SegSrc {
+    const int *bounds[kMaxBatch];
+    const int *n_items[kMaxBatch];   // null: the image has no records
+    const int *M[kMaxBatch];
+};
+
+// One block of kMaxBuckets threads: the segments of every image in image
+// order (the order of the concatenated item list), buckets by descending
+// modulus within an image.
+__global__ void k_g7_segments(G7SegSrc src, int nimages, G7Segment *__restrict__ segs, int *__restrict__ n_segs) {
+    using Scan = cub::BlockScan<int, kMaxBuckets>;
+    __shared__ typename Scan::TempStorage tmp;
+    __shared__ int s_nseg, s_job0, s_base;
+    const int t = threadIdx.x;
+    const int bb = kMaxBuckets - 1 - t;       // this thread's bucket
+    if (t == 0) s_nseg = s_job0 = s_base = 0;
+    __syncthreads();
+    for (int j = 0; j < nimages; j++) {
+        const int ni = src.n_items[j] ? *src.n_items[j] : 0;
+        int cnt = 0, m = 0, lo = 0;
+        if (ni > 0) {
+            lo = src.bounds[j][2 * bb];
+            cnt = src.bounds[j][2 * bb + 1] - lo;
+            m = src.M[j][bb];
+            if (m <= 0 || cnt <= 0) cnt = 0;
+        }
+        const int wu = cnt ? (m * m + kG7PartSlots - 1) / kG7PartSlots : 0;
+        int idx, njob, aggr_seg, aggr_job;
+        Scan(tmp).ExclusiveSum(cnt ? 1 : 0, idx, aggr_seg);
+        __syncthreads();
+        Scan(tmp).ExclusiveSum(cnt * wu, njob, aggr_job);
+        if (cnt) {
+            G7Segment g;
+            g.job0 = s_job0 + njob;
+            g.item0 = s_base + lo;
+            g.wu = wu;
+            g.m = m;
+            segs[s_nseg + idx] = g;
+        }
+        __syncthreads();
+        if (t == 0) {
+            s_nseg += aggr_seg;
+            s_job0 += aggr_job;
+            s_base += ni;
+        }
+        __syncthreads();
+    }
+    if (t == 0) {
+        G7Segment g;
+        g.job0 = s_job0;
+        g.item0 = s_base;
+        g.wu = 1;
+        g.m = 0;
+        segs[s_nseg] = g;
+        *n_segs = s_nseg;
+    }
+}
+
+__device__ __forceinline__ void cp_async16_s(unsigned smem_addr, const void *gmem) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_addr), "l"(gmem) : "memory");
+}
+
+// Runs of the direct layout within each work item: the first record of every
+// run (a record whose corner or support differs from the previous record of
+// the item, and the item's first record) gets the run's length in bits 16-31
+// of wpos.w (bits 0-15 hold the support).  One warp per item; items hold at
+// most kG7Chunk records.
+__global__ void k_mark_runs(const int4 *__restrict__ items, const int *__restrict__ n_items, int4 *__restrict__ wpos) {
+    const int lane = threadIdx.x & 31;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    const int nit = *n_items;
+    for (int v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < nit; v += nwarps) {
+        const int4 it = items[v];
+        int4 *const w = wpos + it.x;
+        const int N = it.y;
+        int next = N;                              // first run start after the current group
+        for (int g = ((N - 1) >> 5) << 5; g >= 0; g -= 32) {
+            const int k = g + lane;
+            bool st = false;
+            int4 r = make_int4(0, 0, 0, 0);
+            if (k < N) {
+                r = w[k];
+                st = k == 0;
+                if (!st) {
+                    const int4 q = w[k - 1];
+                    st = q.x != r.x || (q.w & 0xFFFF) != (r.w & 0xFFFF);
+                }
+            }
+            const unsigned m = __ballot_sync(0xFFFFFFFFu, st);
+            const unsigned above = lane == 31 ? 0u : m & (0xFFFFFFFFu << (lane + 1));
+            const int nxt = above ? g + __ffs(above) - 1 : next;
+            __syncwarp();                          // every lane has read w[k - 1] before it is rewritten
+            if (k < N) w[k].w = (r.w & 0xFFFF) | (st ? (nxt - k) << 16 : 0);
+            if (m) next = g + __ffs(m) - 1;
+        }
+    }
+}
+
+// One job of this warp.  tring / fifo: this lane's first tap-ring and FIFO
+// entry (entry (d, j) is (d * KS + j) * 32 entries further on); rring: the
+// warp's record ring (entry e: the record, then its P visibilities).
+// UNIFORM: every record's support equals the modulus M (one support per
+// bucket), so a slot inside the box is inside every record's box.
+// EXACT: flushes go to the FP64 delta grid, otherwise to the FP32 grid.
+//
+// The record loop is cut at run starts of both pipeline sides: the first
+// record of a run on the accumulation side (flush the slots whose cell
+// changes) and the record whose fetch opens a run on the look-ahead side (new
+// table offsets).  Between those points the loop holds no branch and no
+// conditional update of the accumulators.
+template <int P, bool UNIFORM, bool EXACT>
+__device__ __forceinline__ void grid_job7(const GridJobDesc &J, const int first, const int N, const int M,
+                                          const int part, float4 *tring, int *fifo, float4 *rring) {
+    constexpr int KS = kG7KS, D = kG7Depth, RR = kG7RecRing, E = 1 + P;
+    const int lane = threadIdx.x & 31;
+    const float4 *const tab = J.table2;
+    float *const ggrid = EXACT ? nullptr : J.grid;
+    double *const gdelta = EXACT ? J.dgrid : nullptr;
+    const int gnx = J.nx;
+    const int MM = M * M;
+    // box position (qa, qb) of every slot of this lane; qb = -1: no slot
+    int qa[KS], qb[KS];
+    int nb[KS];                  // copy size of each slot's tap: 16, or 0 outside the box
+#pragma unroll
+    for (int j = 0; j < KS; j++) {
+        const int q = part * kG7PartSlots + j * 32 + lane;
+        const int b = q / M;
+        qa[j] = q - b * M;
+        qb[j] = q < MM ? b : -1;
+        nb[j] = q < MM ? 16 : 0;
+    }
+    // record ring: lane 0 copies the record, lanes 1..P its visibilities
+    const int rflag = lane <= P ? 1 : 0;
+    const char *const rsrc = lane == 0 ? (const char *)(J.wpos + first)
+                                       : (const char *)(J.wvis4 + (size_t)first * P + (lane <= P ? lane - 1 : 0));
+    const int rstride = lane == 0 ? 16 : 16 * P;
+    const unsigned rdst = (unsigned)__cvta_generic_to_shared(rring) + (unsigned)lane * 16;
+    auto rfetch = [&](int r) {
+        asm volatile("{\n .reg .pred p;\n setp.ne.b32 p, %2, 0;\n @p cp.async.cg.shared.global [%0], [%1], 16;\n}" ::"r"(
+                         rdst + (unsigned)((r & (RR - 1)) * E) * 16),
+                     "l"(rsrc + (size_t)r * rstride), "r"(rflag)
+                     : "memory");
+    };
+    auto rec = [&](int k) { return *(const int4 *)(rring + (k & (RR - 1)) * E); };
+    // look-ahead: row base of every slot for the run being fetched
+    const float4 *src[KS];
+    auto pgeom = [&](int k, const int4 r) {   // record k opens a run: geometry of its slots
+        const int rxm = r.y & 0xFFFF, rym = r.y >> 16, S = r.w & 0xFFFF;
+        int *const f = fifo + (k & (D - 1)) * KS * 32;
+#pragma unroll
+        for (int j = 0; j < KS; j++) {
+            int sx = qa[j] + rxm;
+            sx -= (sx >= M) ? M : 0;
+            int sy = qb[j] + rym;
+            sy -= (sy >= M) ? M : 0;
+            const bool ok = qb[j] >= 0 && (UNIFORM || (sx < S && sy < S));
+            src[j] = tab + (ok ? sy * (S + 1) + sx : 0);
+            if (!UNIFORM) nb[j] = ok ? 16 : 0;
+            f[j * 32] = ok ? r.x + sy * gnx + sx : -1;
+        }
+    };
+    const unsigned tdst = (unsigned)__cvta_generic_to_shared(tring);
+    auto tfetch = [&](int k, int z) {
+        const unsigned d = tdst + (unsigned)((k & (D - 1)) * KS * 32) * 16;
+#pragma unroll
+        for (int j = 0; j < KS; j++) cp_async16_zfill_n(d + j * 32 * 16, src[j] + z, nb[j]);
+    };
+    // prologue: records 0 .. 2D-1, then the taps of records 0 .. D-1
+#pragma unroll 1
+    for (int r = 0; r < 2 * D; r++) {
+        if (r < N) rfetch(r);
+        cp_async_commit();
+    }
+    cp_async_wait<D>();        // records 0 .. D-1 have landed (this lane's copies)
+    __syncwarp();              // ... and every lane's
+    int pend = 0;              // next record whose fetch opens a run
+#pragma unroll 1
+    for (int k = 0; k < D; k++) {
+        if (k < N) {
+            const int4 r = rec(k);
+            if (k == pend) {
+                pgeom(k, r);
+                pend = k + max(1, r.w >> 16);
+            }
+            tfetch(k, r.z);
+        }
+        cp_async_commit();
+    }
+    int last[KS];
+    float2 acc[KS][P];
+#pragma unroll
+    for (int j = 0; j < KS; j++) {
+        last[j] = -1;
+#pragma unroll
+        for (int p = 0; p < P; p++) acc[j][p] = make_float2(0.f, 0.f);
+    }
+    // One record: accumulate record i (two packed FMAs per tap and
+    // polarisation; ConvolutionGridder.cu:153-181: to += vis * wt, no
+    // conjugate); TAP: fetch the taps of record i + D; REC: refill the record
+    // ring with record i + 2D.
+    auto step = [&](const int i, auto TAP, auto REC) {
+        cp_async_wait<D - 1>();     // taps of record i and record i + D have landed (this lane's copies)
+        __syncwarp();               // ... and every lane's
+        const float4 *ent = rring + (i & (RR - 1)) * E;
+        float2 vp[P], wp[P];
+#pragma unroll
+        for (int p = 0; p < P; p++) {
+            const float4 q = ent[1 + p];
+            vp[p] = make_float2(q.x, q.y);
+            wp[p] = make_float2(q.z, q.w);
+        }
+        const float4 *c4 = tring + (i & (D - 1)) * KS * 32;
+#pragma unroll
+        for (int j = 0; j < KS; j++) {
+            const float4 c = c4[j * 32];
+            const float2 cre = make_float2(c.x, c.y), cim = make_float2(c.z, c.w);
+#pragma unroll
+            for (int p = 0; p < P; p++) {
+                acc[j][p] = __ffma2_rn(cre, vp[p], acc[j][p]);
+                acc[j][p] = __ffma2_rn(cim, wp[p], acc[j][p]);
+            }
+        }
+        if (decltype(TAP)::value) tfetch(i + D, rec(i + D).z);
+        if (decltype(REC)::value) rfetch(i + 2 * D);
+        cp_async_commit();
+    };
+    using T_ = std::true_type;
+    using F_ = std::false_type;
+    int i = 0, cend = 0;
+    while (i < N) {
+        cp_async_wait<D - 1>();     // taps of record i and record i + D have landed
+        __syncwarp();
+        if (i == cend) {
+            // record i opens a run: flush the slots whose cell changes
+            const int *f = fifo + (i & (D - 1)) * KS * 32;
+            int cell[KS];
+            bool chg = false;
+#pragma unroll
+            for (int j = 0; j < KS; j++) {
+                cell[j] = f[j * 32];
+                chg |= cell[j] >= 0 && cell[j] != last[j];
+            }
+            if (chg) {
+#pragma unroll
+                for (int j = 0; j < KS; j++)
+                    if (cell[j] >= 0 && cell[j] != last[j] && last[j] >= 0) flush2<P>(ggrid, gdelta, last[j], acc[j]);
+            }
+            // Reset of the flushed slots by a packed multiply with 0 (1 keeps
+            // the sum): branch-free, so the accumulators keep their registers
+            // through the loop (an assignment under the branch above made the
+            // compiler copy every accumulator once per record).  It differs
+            // from an assignment only for a non-finite sum, which has already
+            // gone to the grid, where the inverse FFT spreads it over the whole
+            // image either way.
+#pragma unroll
+            for (int j = 0; j < KS; j++) {
+                const bool c = cell[j] >= 0 && cell[j] != last[j];
+                const float kf = c ? 0.f : 1.f;
+#pragma unroll
+                for (int p = 0; p < P; p++) acc[j][p] = __fmul2_rn(acc[j][p], make_float2(kf, kf));
+                last[j] = c ? cell[j] : last[j];
+            }
+            cend = i + max(1, rec(i).w >> 16);
+        }
+        if (i + D < N) {
+            if (i + D == pend) {
+                const int4 r = rec(i + D);
+                pgeom(i + D, r);
+                pend = i + D + max(1, r.w >> 16);
+            }
+            // records whose accumulation and look-ahead meet no run start
+            int stop = cend < pend - D ? cend : pend - D;
+            if (i + 2 * D < N) {
+                stop = stop < N - 2 * D ? stop : N - 2 * D;
+                #pragma unroll 1
+                for (; i < stop; ++i) step(i, T_{}, T_{});
+            } else {
+                stop = stop < N - D ? stop : N - D;
+                #pragma unroll 1
+                for (; i < stop; ++i) step(i, T_{}, F_{});
+            }
+        } else {
+            #pragma unroll 1
+            for (; i < cend; ++i) step(i, F_{}, F_{});
+        }
+    }
+    cp_async_wait<0>();
+    __syncwarp();              // the rings are reused by the next job
+#pragma unroll
+    for (int j = 0; j < KS; j++)
+        if (last[j] >= 0) flush2<P>(ggrid, gdelta, last[j], acc[j]);
+}
+
+template <int P, bool UNIFORM, bool EXACT>
+__global__ void __launch_bounds__(kG7Threads, 2) k_grid7(Grid7Args a) {
+    constexpr int E = 1 + P;
+    extern __shared__ float4 smem7[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    float4 *const tring = smem7 + warp * kG7TapStride + lane;                                  // [warp][D][KS][32]
+    int *const fifo = (int *)(smem7 + kG7Warps * kG7TapStride) + warp * kG7TapStride + lane;    // [warp][D][KS][32]
+    float4 *const rring = smem7 + kG7Warps * kG7TapStride + kG7Warps * kG7TapStride / 4 +
+                          warp * kG7RecRing * E;                                                // [warp][RR][E]
+    const int nsegs = *a.n_segs;
+    const int total = a.segs[nsegs].job0;
+    int seg = 0;
+    for (;;) {
+        int t = 0;
+        if (lane == 0) t = atomicAdd(a.counter, 1);
+        t = __shfl_sync(0xFFFFFFFFu, t, 0);
+        if (t >= total) break;
+        while (a.segs[seg + 1].job0 <= t) seg++;      // a warp's tickets only grow
+        const G7Segment g = a.segs[seg];
+        const int rel = t - g.job0;
+        const int k = rel / g.wu;
+        const int4 it = a.items[g.item0 + k];
+        grid_job7<P, UNIFORM, EXACT>(a.jobs[it.w], it.x, it.y, g.m, rel - k * g.wu, tring, fifo, rring);
+    }
+}
+
+template <int P>
+static size_t grid7_smem() {
+    return (size_t)kG7Warps * (kG7TapStride * (sizeof(float4) + sizeof(int)) + kG7RecRing * (1 + P) * sizeof(float4));
+}
+
+// UNIFORM kernel when every image of the launch has one support per bucket
+template <int P>
+static int launch_grid7(const Grid7Args &a, cudaStream_t st) {
+    bool uniform = true;
+    for (int j = 0; j < kMaxBatch && a.jobs[j].wpos; j++) uniform = uniform && a.jobs[j].uniform;
+    const bool exact = a.jobs[0].dgrid != nullptr;
+    auto kern = uniform ? (exact ? k_grid7<P, true, true> : k_grid7<P, true, false>)
+                        : (exact ? k_grid7<P, false, true> : k_grid7<P, false, false>);
+    const size_t smem = grid7_smem<P>();
+    MTB_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    MTB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kG7Threads, smem));
+    if (per_sm < 1) return MTB_ERR_BAD_SHAPE;
+    kern<<<per_sm * sm_count(), kG7Threads, smem, st>>>(a);
+    MTB_LAUNCHED();
+    return MTB_OK;
 }
 
 template <int P>
@@ -1491,6 +1899,9 @@ struct GridSpace {
     int *counter4;       // k_grid4 work counter
     int *err;            // gridder pipeline error flag
     double *delta;       // this call's grid contribution (compensated mode; FP64 or FP32)
+    G7Segment *segs;     // k_grid7 job segments (kMaxBuckets + 1)
+    int *n_segs;
+    int *counter7;       // k_grid7 job tickets
 };
 
 static size_t cub_bytes(int n) {
@@ -1537,6 +1948,9 @@ static void carve_grid(Arena &A, int R, int P, int chunk, size_t table_elems, si
     s->counter4 = A.take<int>(1);
     s->err = A.take<int>(1);
     s->delta = A.take<double>(grid_cells ? grid_cells * 2 * P : 1);
+    s->segs = A.take<G7Segment>(kMaxBuckets + 1);
+    s->n_segs = A.take<int>(1);
+    s->counter7 = A.take<int>(1);
 }
 
 // float2 elements of the kernel table described by conv_info
@@ -1571,13 +1985,19 @@ static bool capturing(cudaStream_t st) {
 
 static int gridder_of(const mtb_grid_params *p) {
     if (p->gridder != 0) return p->gridder;
-    return p->gridder_threads == 512 ? 3 : 5;
+    if (p->gridder_threads == 512) return 3;
+    return p->bulk_min_support > 0 ? 5 : 7;
 }
+
+// the gridders that read the {re, re, im, im} table and the compact one
+static bool wants_expanded(const mtb_grid_params *) { return true; }
+static bool wants_compact(const mtb_grid_params *p) { return p->bulk_min_support > 0; }
 
 static int effective_chunk(const mtb_grid_params *p) {
     int c = p->max_chunk > 0 ? p->max_chunk : kDefaultChunk;
     if (p->merge != 1 && c > kG3Chunk) c = kG3Chunk;
     if (p->merge != 1 && gridder_of(p) == 5 && c > kG5Chunk) c = kG5Chunk;
+    if (p->merge != 1 && gridder_of(p) == 7 && c > kG7Chunk) c = kG7Chunk;
     return c;
 }
 
@@ -1591,8 +2011,9 @@ static int check_params(const mtb_grid_params *p) {
     if (p->merge < 0 || p->merge > 2) return MTB_ERR_BAD_PARAM;
     if (p->bulk_min_support < 0) return MTB_ERR_BAD_PARAM;
     if (p->gridder_threads != 0 && p->gridder_threads != 256 && p->gridder_threads != 512) return MTB_ERR_BAD_PARAM;
-    if (p->gridder != 0 && p->gridder != 3 && p->gridder != 5) return MTB_ERR_BAD_PARAM;
-    if (p->gridder == 5 && p->gridder_threads == 512) return MTB_ERR_BAD_PARAM;
+    if (p->gridder != 0 && p->gridder != 3 && p->gridder != 5 && p->gridder != 7) return MTB_ERR_BAD_PARAM;
+    if ((p->gridder == 5 || p->gridder == 7) && p->gridder_threads == 512) return MTB_ERR_BAD_PARAM;
+    if (p->gridder == 7 && p->bulk_min_support > 0) return MTB_ERR_BAD_PARAM;
     return MTB_OK;
 }
 
@@ -1761,13 +2182,22 @@ static int prepare_grid(const mtb_grid_params *p, const GridPlan &plan, const fl
     MTB_LAUNCHED();
     launch_gather<P, true>(p, blocks, st, R, s, vis, weights, flags, plan, conv_info, s.pbase, p->wplanes);
     MTB_LAUNCHED();
+    if (gridder_of(p) == 7) {
+        // one warp per work item; the item count is on the device: cover the
+        // largest count this chunk can have and let the kernel read the rest
+        const int wb = std::min((R / 8 + 7) / 8 + 1, sms * 16);
+        k_mark_runs<<<wb, 256, 0, st>>>(s.items, s.n_items, s.wpos);
+        MTB_LAUNCHED();
+    }
     (void)end_bit;
     {
-        // compact padded rows only for the bulk-copy gridder
-        float2 *pt = p->bulk_min_support > 0 ? s.ptab : nullptr;
+        // compact padded rows for the bulk-copy gridder, the expanded copy
+        // for the others
+        float2 *pt = wants_compact(p) ? s.ptab : nullptr;
+        float4 *t2 = wants_expanded(p) ? s.table2 : nullptr;
         const int rows = plan.table_rows;
         const int pb = (int)std::min<size_t>(((size_t)rows + 7) / 8, (size_t)sms * 16);
-        k_pad_expand<<<pb > 0 ? pb : 1, 256, 0, st>>>(table, conv_info, s.pbase, p->wplanes, rows, pt, s.table2);
+        k_pad_expand<<<pb > 0 ? pb : 1, 256, 0, st>>>(table, conv_info, s.pbase, p->wplanes, rows, pt, t2);
         MTB_LAUNCHED();
         (void)table_elems;
         (void)padded;
@@ -1885,9 +2315,30 @@ static int run_grid(const mtb_grid_params *p, const GridPlan &plan, const float2
     g2.counter = s.counters;
     g2.njobs = 1;
     g2.jobs[0] = job_desc<P>(p, grid, grid_lo != nullptr, s);
-    const bool rolling = gridder_of(p) == 5;
-    if (rolling) MTB_TRY(launch_grid5<P>(g2, s.err, st));
-    else MTB_TRY(launch_grid3<P>(g2, p->gridder_threads, st));
+    const int which = gridder_of(p);
+    const bool rolling = which == 5;
+    if (which == 7) {
+        G7SegSrc src;
+        std::memset(&src, 0, sizeof(src));
+        src.bounds[0] = s.bounds;
+        src.n_items[0] = s.n_items;
+        src.M[0] = s.moduli;
+        k_g7_segments<<<1, kMaxBuckets, 0, st>>>(src, 1, s.segs, s.n_segs);
+        MTB_LAUNCHED();
+        MTB_CUDA_TRY(cudaMemsetAsync(s.counter7, 0, sizeof(int), st));
+        Grid7Args g7;
+        std::memset(&g7, 0, sizeof(g7));
+        g7.items = s.items;
+        g7.segs = s.segs;
+        g7.n_segs = s.n_segs;
+        g7.counter = s.counter7;
+        g7.jobs[0] = g2.jobs[0];
+        MTB_TRY(launch_grid7<P>(g7, st));
+    } else if (which == 5) {
+        MTB_TRY(launch_grid5<P>(g2, s.err, st));
+    } else {
+        MTB_TRY(launch_grid3<P>(g2, p->gridder_threads, st));
+    }
     Grid4Args g4;
     g4.items = s.items;
     g4.first = s.split;
@@ -2045,7 +2496,7 @@ static int batch_plans(const mtb_grid_job *jobs, int njobs, GridPlan *plans) {
 
 // every job's space, then the batch queue, its length and its counter
 static void carve_batch(Arena &A, const mtb_grid_job *jobs, int njobs, const GridPlan *plans, GridSpace *spaces,
-                        int4 **items, int **n_total, int **counter) {
+                        int4 **items, int **n_total, int **counter, G7Segment **segs) {
     size_t cap = 0;
     for (int j = 0; j < njobs; j++) {
         const mtb_grid_params *p = &jobs[j].params;
@@ -2057,6 +2508,7 @@ static void carve_batch(Arena &A, const mtb_grid_job *jobs, int njobs, const Gri
     *items = A.take<int4>(cap);
     *n_total = A.take<int>(1);
     *counter = A.take<int>(1);
+    *segs = A.take<G7Segment>((size_t)njobs * kMaxBuckets + 1);
 }
 
 extern "C" int mtb_grid_batch_workspace_size(const mtb_grid_job *jobs, int njobs, size_t *bytes) {
@@ -2068,14 +2520,15 @@ extern "C" int mtb_grid_batch_workspace_size(const mtb_grid_job *jobs, int njobs
     GridSpace spaces[kMaxBatch];
     int4 *items;
     int *n_total, *counter;
-    carve_batch(A, jobs, njobs, plans, spaces, &items, &n_total, &counter);
+    G7Segment *segs;
+    carve_batch(A, jobs, njobs, plans, spaces, &items, &n_total, &counter, &segs);
     *bytes = A.used;
     return MTB_OK;
 }
 
 template <int P>
 static int run_batch(const mtb_grid_job *jobs, int njobs, const GridPlan *plans, GridSpace *spaces, int4 *items,
-                     int *n_total, int *counter, cudaStream_t st) {
+                     int *n_total, int *counter, G7Segment *segs, cudaStream_t st) {
     BatchQueues q;
     Grid2Args g2;
     g2.njobs = njobs;
@@ -2103,7 +2556,26 @@ static int run_batch(const mtb_grid_job *jobs, int njobs, const GridPlan *plans,
     g2.counter = counter;
     // the batch's gridder error flag (read by every image's k_finish)
     MTB_CUDA_TRY(cudaMemsetAsync(spaces[0].err, 0, sizeof(int), st));
-    if (gridder_of(&p0) == 5) {
+    if (gridder_of(&p0) == 7) {
+        G7SegSrc src;
+        std::memset(&src, 0, sizeof(src));
+        for (int j = 0; j < njobs; j++) {
+            src.bounds[j] = spaces[j].bounds;
+            src.n_items[j] = jobs[j].nrecords > 0 ? spaces[j].n_items : nullptr;
+            src.M[j] = spaces[j].moduli;
+        }
+        k_g7_segments<<<1, kMaxBuckets, 0, st>>>(src, njobs, segs, spaces[0].n_segs);
+        MTB_LAUNCHED();
+        MTB_CUDA_TRY(cudaMemsetAsync(spaces[0].counter7, 0, sizeof(int), st));
+        Grid7Args g7;
+        std::memset(&g7, 0, sizeof(g7));
+        g7.items = items;
+        g7.segs = segs;
+        g7.n_segs = spaces[0].n_segs;
+        g7.counter = spaces[0].counter7;
+        for (int j = 0; j < njobs; j++) g7.jobs[j] = g2.jobs[j];
+        MTB_TRY(launch_grid7<P>(g7, st));
+    } else if (gridder_of(&p0) == 5) {
         MTB_TRY(launch_grid5<P>(g2, spaces[0].err, st));
         if (check_gridder() && !capturing(st)) {
             int e = 0;
@@ -2142,7 +2614,8 @@ extern "C" int mtb_grid_batch(const mtb_grid_job *jobs, int njobs, void *d_works
     GridSpace spaces[kMaxBatch];
     int4 *items;
     int *n_total, *counter;
-    carve_batch(A, jobs, njobs, plans, spaces, &items, &n_total, &counter);
+    G7Segment *segs;
+    carve_batch(A, jobs, njobs, plans, spaces, &items, &n_total, &counter, &segs);
     if (!A.ok()) return MTB_ERR_WORKSPACE;
     for (int j = 0; j < njobs; j++) {
         const mtb_grid_job &J = jobs[j];
@@ -2155,9 +2628,9 @@ extern "C" int mtb_grid_batch(const mtb_grid_job *jobs, int njobs, void *d_works
         if (J.d_stats) MTB_CUDA_TRY(cudaMemsetAsync(J.d_stats, 0, sizeof(mtb_grid_stats), st));
     }
     const int P = jobs[0].params.npol;
-    if (P == 1) return run_batch<1>(jobs, njobs, plans, spaces, items, n_total, counter, st);
-    if (P == 2) return run_batch<2>(jobs, njobs, plans, spaces, items, n_total, counter, st);
-    return run_batch<4>(jobs, njobs, plans, spaces, items, n_total, counter, st);
+    if (P == 1) return run_batch<1>(jobs, njobs, plans, spaces, items, n_total, counter, segs, st);
+    if (P == 2) return run_batch<2>(jobs, njobs, plans, spaces, items, n_total, counter, segs, st);
+    return run_batch<4>(jobs, njobs, plans, spaces, items, n_total, counter, segs, st);
 }
 
 extern "C" int mtb_preprocess_uvw(const mtb_grid_params *p, const int *d_conv_info, const int *h_conv_info,

@@ -165,7 +165,10 @@ def test_chunked_equals_single(cfg1):
                                     dict(merge=1), dict(merge=2), dict(merge=1, tile=16),
                                     dict(bulk_min_support=17), dict(bulk_min_support=25), dict(exact_delta=True),
                                     dict(gridder_threads=512), dict(gridder_threads=512, tile=16, max_chunk=256),
-                                    dict(gridder=5), dict(gridder=5, tile=64)])
+                                    dict(gridder=5), dict(gridder=5, tile=64),
+                                    dict(gridder=7), dict(gridder=7, tile=64), dict(gridder=7, tile=16),
+                                    dict(gridder=7, support_bucket=3), dict(gridder=7, exact_delta=True),
+                                    dict(gridder=7, max_chunk=37, exact_delta=True)])
 def test_tuning_does_not_change_result(cfg1, tuning):
     obs, setup, geo, kern, img_o, grid_o, norm_o = cfg1
     im, img = run_gpu(obs, setup, **tuning)
@@ -175,6 +178,7 @@ def test_tuning_does_not_change_result(cfg1, tuning):
 
 
 @pytest.mark.parametrize("kw", [dict(), dict(tile=64), dict(nx=320, s=3), dict(merge=1), dict(gridder=5),
+                                dict(gridder=7), dict(nx=320, s=3, gridder=7),
                                 dict(bulk_min_support=17), dict(nx=320, s=3, bulk_min_support=17)])
 def test_large_supports(oracle, kw):
     """Supports up to 55 (and 105 with odd sampling): the direct gridders
