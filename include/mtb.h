@@ -32,7 +32,8 @@
  *   freq       float   [R]           nu / c per record
  *   vis        float2  [R][P]        pol-interleaved complex (XX, XY, YX, YY)
  *   weights    float   [R][P]
- *   flags      int     [R][P]        non-zero = flagged
+ *   flags      int     [R][P]        0 = keep, any other value = flagged (the reference
+ *                                    weights by 1 - flag, the same for 0 / 1)
  *   table      float2  [sum_k T^2 S_k^2]  per plane [oy][ox][sy][sx], T = s (s odd) or s+1
  *   conv_info  int     [wplanes][2]  {support, first element of the plane in table}
  *   conv_sums  float   [wplanes][T*T]
@@ -147,16 +148,18 @@ typedef struct mtb_grid_params {
     void *gridder_end_event;   /* cudaEvent_t or NULL: recorded after them (the span of the
                                   ConvolutionGridder operator, like GPUSubmissionData's
                                   startEvent/endEvent, GPUSubmissionData.h:27-47)          */
-    int bulk_min_support;      /* 0: off (default); > 0: bucket moduli from max(17, value) up
-                                  are gridded by the bulk-copy gridder (cp.async.bulk rows,
-                                  mbarrier pipeline), the rest by the per-thread gridder   */
+    int bulk_min_support;      /* reserved, must be 0 (an earlier bulk-copy gridder, removed:
+                                  it measured slower than the default)                     */
     int psf;                   /* 1: grid every visibility as 1 + 0i (the PSF; mt-imager's
                                   psf=true, VisibilityForPSFStorageManager.cpp:65-77);
                                   d_vis may then be NULL                                   */
     int exact_delta;           /* compensated mode (d_grid_lo set): 0 (default) the call's
                                   flushes accumulate in an FP32 delta grid merged into
                                   (grid, grid_lo) with TwoSum; 1 they accumulate in FP64
-                                  (order-independent, about half the grid error, slower)   */
+                                  (order-independent, about half the grid error, slower).
+                                  Work items shorter than 128 records (max_chunk) always
+                                  use the FP64 delta: their extra flushes would take the
+                                  FP32 delta's rounding past the 1e-5 image bound           */
     int gridder_threads;       /* 0: 256; threads of a gridder block, which grids one work
                                   item at a time (256 or 512)                              */
     int gridder;               /* 0: default (5, or 3 with gridder_threads 512);
@@ -168,8 +171,15 @@ typedef struct mtb_grid_params {
                                   block barriers; items of at most 512 records).  A gridder
                                   that could not complete sets the normaliser to NaN      */
     int flags_u8;              /* 0: d_flags is int32 [R][P] (the reference's layout); 1: it
-                                  is one byte per flag, uint8 [R][P] (0 = keep, 1 = flagged;
+                                  is one byte per flag, uint8 [R][P] (0 = keep, non-zero = flagged;
                                   a quarter of the bytes to move), passed cast to int *    */
+    int no_grid_lo;            /* 0: the workspace holds the per-call delta grid compensated
+                                  calls (d_grid_lo set) accumulate in: 8 bytes per cell and
+                                  polarisation (FP32), 16 with exact_delta or with work
+                                  items shorter than 128 records (max_chunk), which use the
+                                  FP64 delta; 1: the calls pass d_grid_lo = NULL, the
+                                  workspace holds no delta grid and mtb_grid refuses a
+                                  d_grid_lo.  merge = 1 never needs one                   */
 } mtb_grid_params;
 
 typedef struct mtb_grid_stats {
@@ -203,7 +213,7 @@ int mtb_grid(const mtb_grid_params *p, const void *d_table, const int *d_conv_in
 /* One image of a batched gridding launch. */
 typedef struct mtb_grid_job {
     mtb_grid_params params;      /* per image; npol must be the same for every job of a batch;
-                                    merge and bulk_min_support are ignored (the batch runs the
+                                    merge is ignored (the batch runs the
                                     per-thread direct gridder)                               */
     const void *d_table;         /* the image's kernel table, as for mtb_grid               */
     const int *d_conv_info;
@@ -250,21 +260,24 @@ typedef struct mtb_grid_tuning {
     int support_bucket;   /* odd supports per bin bucket                              */
     int max_chunk;        /* records per work item                                    */
     int gridder_threads;  /* threads per gridder block (one work item at a time)      */
-    int gridder;          /* 3: block-staged items, 5: rolling items (mtb_grid_params) */
+    int gridder;          /* 3: block-staged items, 5: rolling items, 7: streaming
+                             warps (mtb_grid_params)                                   */
     float ms;             /* measured time of one mtb_grid_batch call with these knobs */
 } mtb_grid_tuning;
 
 /* Autotuner.  No counterpart in the reference, whose gridder launch shapes are
  * fixed.  Grids the jobs (as mtb_grid_batch) once with every candidate of
- * tile {16, 32, 64} x support_bucket {1, 2} x five gridder shapes (gridder 3
- * with max_chunk {256, 512} x gridder_threads {256, 512}, and gridder 5 with
- * 256-record items and 256 threads), times each call with CUDA events on
+ * tile {16, 32, 64} x support_bucket {1, 2} x seven gridder shapes (gridder 3
+ * with max_chunk {256, 512} x gridder_threads {256, 512}, gridder 5 with
+ * 256-record items, gridder 7 with max_chunk {256, 512}; 256 threads unless
+ * stated), times each call with CUDA events on
  * `stream` (after one untimed call), and writes the fastest to *best and to
  * every job's params.  Every job must start a fresh image (initialize_output
  * = 1): the grids, normalisers and statistics hold the result of a call with
  * the chosen knobs when it returns.  Synchronises `stream` after every call.
- * `candidates` (may be NULL) receives all 30 timings.  Workspace:
- * mtb_grid_autotune_workspace_size. */
+ * `candidates` (may be NULL) receives all mtb_grid_autotune_candidate_count()
+ * timings (42).  Workspace: mtb_grid_autotune_workspace_size. */
+int mtb_grid_autotune_candidate_count(void);
 int mtb_grid_autotune_workspace_size(const mtb_grid_job *jobs, int njobs, size_t *bytes);
 int mtb_grid_autotune(mtb_grid_job *jobs, int njobs, void *d_workspace, size_t workspace_bytes,
                       mtb_stream_t stream, mtb_grid_tuning *best, mtb_grid_tuning *candidates);
@@ -290,7 +303,7 @@ int mtb_grid_batch(const mtb_grid_job *jobs, int njobs, void *d_workspace, size_
  *   d_to_compress     int [R]    1 = merged into the previous record
  *   d_support         int [R]
  *   d_take_conjugate  float [R]  -1 when w < 0 (u, v negated, imaginary part negated)
- *   d_conv_sum        float [P][R] ConvSums * weight * (1 - flag) */
+ *   d_conv_sum        float [P][R] ConvSums * weight * (1 - flag), flag taken as 0 / 1 */
 int mtb_preprocess_uvw(const mtb_grid_params *p, const int *d_conv_info, const int *h_conv_info,
                        const float *d_conv_sums, const float *d_uvw, const float *d_freq,
                        const float *d_weights, const int *d_flags, int nrecords, int *d_gridding_data,

@@ -188,6 +188,7 @@ public:
         gp.initialize_output = fresh_ ? 1 : 0;
         gp.exact_delta = exact_delta_ ? 1 : 0;
         gp.flags_u8 = flags_u8_ ? 1 : 0;
+        gp.no_grid_lo = compensated_ ? 0 : 1;
         return gp;
     }
 

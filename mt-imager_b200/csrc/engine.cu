@@ -164,11 +164,20 @@ public:
                 k->release_on(0);
                 e->prom.set_value(k);
                 std::lock_guard<std::mutex> lk(m_);
-                e->bytes = k->bytes();
-                used_ += e->bytes;
-                while (used_ > cap_ && lru_.size() > 1) {
-                    used_ -= lru_.back()->bytes;
-                    lru_.pop_back();
+                // count the table only while its entry is still listed, and
+                // evict from the cold end only finished tables other than this
+                // one: an entry another worker is still building holds no bytes
+                // yet, and dropping it would let its bytes be added later for
+                // an entry that is no longer in the list (never subtracted)
+                if (std::find(lru_.begin(), lru_.end(), e) != lru_.end()) {
+                    e->bytes = k->bytes();
+                    used_ += e->bytes;
+                }
+                for (auto it = lru_.end(); used_ > cap_ && it != lru_.begin();) {
+                    --it;
+                    if (*it == e || (*it)->bytes == 0) continue;
+                    used_ -= (*it)->bytes;
+                    it = lru_.erase(it);
                 }
             } catch (...) {
                 e->prom.set_exception(std::current_exception());
@@ -252,6 +261,8 @@ int request_bytes(const mtb_engine_config &cfg, const mtb_image_request *r, size
     gp.u_increment = info.u_increment;
     gp.v_increment = info.v_increment;
     gp.w_sq_increment = info.w_sq_increment;
+    gp.exact_delta = r->exact_delta;
+    gp.no_grid_lo = r->compensated ? 0 : 1;   // plain requests reserve no delta grid
     const int chunk = std::min(r->nrecords, cfg.chunk_records);
     size_t ws = 0;
     s = mtb_grid_workspace_size(&gp, ci.data(), chunk, &ws);
@@ -260,7 +271,6 @@ int request_bytes(const mtb_engine_config &cfg, const mtb_image_request *r, size
     size_t fin = 0;
     s = mtb_finalize_workspace_size(&fp, &fin);
     if (s != MTB_OK) return s;
-    gp.exact_delta = r->exact_delta;
     *out = cells * 8 * (r->compensated ? 2 : 1) + cells * 4 + ws + fin + (1 << 20);
     return MTB_OK;
 }

@@ -38,10 +38,6 @@
 //                  (support-box unit, record stream) jobs are balanced over
 //                  the block's threads.  Kernel taps are fetched a few records
 //                  ahead into a per-thread shared-memory ring with cp.async.
-//   k_grid4        opt-in gridder for large supports: one producer warp copies
-//                  the needed kernel rows of every record into a shared-memory
-//                  ring with cp.async.bulk (mbarrier pipeline); 11 consumer
-//                  warps accumulate from it.
 //   k_grid         shared-memory tile-window variant (merge = 1).
 //   k_merge_delta  compensated mode: flushes go to a delta grid of the call
 //                  (plain reductions; FP32, or FP64 with exact_delta), merged
@@ -92,7 +88,9 @@ __global__ void k_preprocess(int R, const float *__restrict__ uvw, const float *
         bool grid = false;
 #pragma unroll
         for (int p = 0; p < P; p++) {
-            fl[p] = (int)flags[(size_t)r * P + p];
+            // any non-zero flag is a flagged sample; the reference weights by
+            // 1 - flag (WProjPreProcessUVW.cu:84-106), which agrees for 0 / 1
+            fl[p] = flags[(size_t)r * P + p] != 0 ? 1 : 0;
             wt[p] = weights[(size_t)r * P + p];
             if (fl[p] == 0) grid = true;
         }
@@ -287,7 +285,7 @@ __global__ void k_gather(int R, const unsigned *__restrict__ skeys, const int *_
             for (int p = 0; p < P; p++) {
                 const float2 v = psf ? make_float2(1.0f, 0.0f) : vis[(size_t)r * P + p];
                 float wgt = weights[(size_t)r * P + p];
-                float keep = 1.0f - (float)flags[(size_t)r * P + p];
+                float keep = flags[(size_t)r * P + p] != 0 ? 0.0f : 1.0f;
                 acc[p].x += v.x * wgt * keep;
                 acc[p].y += v.y * wgt * keep * im;
             }
@@ -568,6 +566,7 @@ struct Grid2Args {
     const int *n_items;
     int *counter;
     int njobs;
+    long long wait_cycles; // bound of every mbarrier wait of k_grid5
     GridJobDesc jobs[kMaxBatch];
 };
 
@@ -670,11 +669,9 @@ __global__ void k_pad_bases(const int *__restrict__ conv_info, int nw, int T, in
 // of kernel rows (S taps of one sub-kernel row each), so the plane is found
 // once per warp and then followed across plane boundaries.  t2 gets every tap
 // as {re, re, im, im} (one 128-bit load gives both packed operands of the
-// f32x2 complex multiply-add) with a zero tap closing each row; pt (when not
-// null) gets the same rows compact (the bulk-copy gridder reads those).
+// f32x2 complex multiply-add) with a zero tap closing each row.
 __global__ void k_pad_expand(const float2 *__restrict__ t, const int *__restrict__ conv_info,
-                             const int *__restrict__ pbase, int nw, int rows, float2 *__restrict__ pt,
-                             float4 *__restrict__ t2) {
+                             const int *__restrict__ pbase, int nw, int rows, float4 *__restrict__ t2) {
     const int lane = threadIdx.x & 31;
     const int nwarps = (gridDim.x * blockDim.x) >> 5;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -706,8 +703,7 @@ __global__ void k_pad_expand(const float2 *__restrict__ t, const int *__restrict
         const size_t dst = pb + (size_t)sub * S * (S + 1) + (size_t)y * (S + 1);
         for (int x = lane; x <= S; x += 32) {
             const float2 c = x < S ? t[src + x] : make_float2(0.f, 0.f);
-            if (t2) t2[dst + x] = make_float4(c.x, c.x, c.y, c.y);
-            if (pt) pt[dst + x] = c;
+            t2[dst + x] = make_float4(c.x, c.x, c.y, c.y);
         }
     }
 }
@@ -931,60 +927,10 @@ static int launch_grid3(const Grid2Args &a, int threads, cudaStream_t st) {
     return launch_grid3_t<P, kG3Threads>(a, st);
 }
 
-// ---------------------------------------------------------------------------
-// Direct gridder for large supports with bulk-copied kernel rows.
-//
-// A block is 352 consumer threads plus one producer warp.  For every record
-// the producer copies the rows of the record's sub-kernel that the block's
-// slots need in the current pass (one or two contiguous row ranges of the
-// row-padded table, cp.async.bulk into a shared-memory ring of kG4Depth
-// slots, completion counted on a per-slot "full" mbarrier).  Consumers wait on
-// "full", read one 8-byte tap per slot from shared memory, accumulate
-// V * C with packed f32x2 FMAs and arrive on the slot's "empty" mbarrier; the
-// producer refills a slot once every consumer of its stream has arrived.
-// There is no block barrier per record.
-//
-// Slot layout (Romein): thread (col, gl) of stream cs owns support-box slots
-// (col, r0 + gl + j*Gp), j < KS, of the pass's band of nb = Gp*KS slot rows.
-// The ring stores band row r of a record at ring row r - r0 (the record's
-// sub-kernel row sy = (r + rym) mod M), so a slot's shared-memory offset only
-// changes when the record's corner or support changes.
-//
-// Complex product with compact taps: with the visibility stored as the pairs
-// (re, im) and (-im, re), a += (c.re, c.im) * (re, im) and
-// b += (c.re, c.im) * (-im, re) give Re(C V) = a.x - a.y and
-// Im(C V) = b.y - b.x.
-//
-// Every wait is bounded by a clock deadline: on expiry the kernel records an
-// error in *err and every thread leaves its loops.
-// 11 consumer warps + 1 producer warp: 3 warps per SM sub-partition, so each
-// thread may hold up to 168 registers
-static const int kG4Consumers = 352;
-static const int kG4Threads = kG4Consumers + 32;
-static const int kG4Depth = 12;               // ring slots
-// bytes of one ring slot (all streams): a pass needs at most
-// kG4Consumers * KS * 8 * (M + 1) / M <= 11927 bytes for M >= 17
-static const int kG4Slot = 11952;
-static const int kG4ZeroOff = kG4Slot - 16;   // 16 zero bytes closing every slot
-static const int kG4MaxStreams = 4;
-static const int kG4KS = 4;
-static const int kG4MinM = 17;                // smallest modulus k_grid4 handles
-static const long long kG4WaitCycles = 1LL << 31;
-
-struct Grid4Args {
-    const int4 *items;
-    const int *first;      // first item of this gridder's range
-    const int *n_items;
-    int *counter;
-    const int4 *wpos;
-    const float4 *wvis4;
-    const float2 *ptab;
-    float *grid;
-    double *dgrid;         // compensated mode: FP64 delta grid of this call, else null
-    int nx;
-    BucketTable bt;
-    int *err;
-};
+// Bounded mbarrier waits of the rolling-items gridder: a wait gives up after
+// this many SM clock cycles (about a second) unless the host sets another limit
+// (MTB_GRIDDER_WAIT_CYCLES, read at every call: a test makes waits run out).
+static const long long kWaitCycles = 1LL << 31;
 
 __device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
 
@@ -1015,223 +961,15 @@ __device__ __forceinline__ bool mbar_try(unsigned bar, unsigned parity) {
         : "memory");
     return ok != 0;
 }
-// Bounded wait for the completion of the phase with the given parity.
-__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity, volatile int *abort_flag) {
+// Bounded wait for the completion of the phase with the given parity: false
+// when another thread gave up (abort_flag) or `limit` cycles passed.
+__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity, volatile int *abort_flag, long long limit) {
     if (mbar_try(bar, parity)) return true;
     const long long t0 = clock64();
     for (;;) {
         if (mbar_try(bar, parity)) return true;
         if (*abort_flag) return false;
-        if (clock64() - t0 > kG4WaitCycles) return false;
-    }
-}
-__device__ __forceinline__ void bulk_g2s(unsigned dst, const void *src, unsigned bytes, unsigned bar) {
-    asm volatile(
-        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
-        "l"(src), "r"(bytes), "r"(bar)
-        : "memory");
-}
-
-template <int P>
-__device__ __forceinline__ void flush_ab(float *grid, double *dgrid, int cell, const float2 *A, const float2 *B) {
-    float v[2 * P];
-#pragma unroll
-    for (int p = 0; p < P; p++) {
-        const float2 fa = A[p], fb = B[p];
-        v[2 * p] = fa.x - fa.y;
-        v[2 * p + 1] = fb.y - fb.x;
-    }
-    flush_cell<P>(grid, dgrid, cell, v);
-}
-
-template <int P>
-__global__ void __launch_bounds__(kG4Threads, 1) k_grid4(Grid4Args a) {
-    extern __shared__ __align__(128) unsigned char smem_g4[];
-    int4 *s_rec = (int4 *)smem_g4;                                           // [kG3Chunk]
-    ulonglong2 *s_v = (ulonglong2 *)(smem_g4 + kG3Chunk * 16);               // [kG3Chunk][P]
-    unsigned char *ring = smem_g4 + kG3Chunk * 16 * (1 + P);                  // [kG4Depth][kG4Slot]
-    unsigned long long *bars = (unsigned long long *)(ring + kG4Depth * kG4Slot);
-    __shared__ int s_item;
-    __shared__ volatile int s_abort;
-    constexpr int KS = kG4KS, D = kG4Depth;
-    const int t = threadIdx.x;
-    const bool producer = t >= kG4Consumers;
-    const unsigned ring_sa = smem_u32(ring);
-    const unsigned full_sa = smem_u32(bars), empty_sa = full_sa + D * kG4MaxStreams * 8;
-    if (t < D) *(uint4 *)(ring + t * kG4Slot + kG4ZeroOff) = make_uint4(0u, 0u, 0u, 0u);
-    if (t == 0) s_abort = 0;
-    const int first = *a.first, nitems = *a.n_items;
-    const int4 *grec = a.wpos;
-    const uint4 *gvis = (const uint4 *)a.wvis4;
-    for (;;) {
-        __syncthreads();
-        if (t == 0) s_item = first + atomicAdd(a.counter, 1);
-        __syncthreads();
-        const int v = s_item;
-        if (v >= nitems || s_abort) break;
-        const int4 it = a.items[v];
-        const int M = a.bt.M[(unsigned)it.z >> 24];
-        const int G = (M + KS - 1) / KS;
-        int Gp = kG4Consumers / M;
-        if (Gp > G) Gp = G;
-        const int npass = (G + Gp - 1) / Gp;
-        int nstream = 1;
-        if (npass == 1) {
-            nstream = kG4Consumers / (M * G);
-            if (nstream > kG4MaxStreams) nstream = kG4MaxStreams;
-        }
-        const int per_stream = M * Gp;
-        const int nb = Gp * KS;                       // slot rows of one pass
-        const int sregion = nb * (M + 1) * 8;         // ring bytes of one stream
-        if (!producer) {
-            for (int k = t; k < it.y; k += kG4Consumers) cp_async16(&s_rec[k], &grec[it.x + k]);
-            for (int k = t; k < it.y * P; k += kG4Consumers) cp_async16(&s_v[k], &gvis[(size_t)it.x * P + k]);
-            cp_async_commit();
-            cp_async_wait<0>();
-        }
-        if (t == 0) {
-            for (int ss = 0; ss < nstream; ss++)
-                for (int d = 0; d < D; d++) {
-                    mbar_init(full_sa + (d * kG4MaxStreams + ss) * 8, 1);
-                    mbar_init(empty_sa + (d * kG4MaxStreams + ss) * 8, per_stream);
-                }
-            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-        }
-        __syncthreads();
-        if (producer) {
-            // lane ss issues the copies of stream ss in record order; it
-            // blocks (suspended in try_wait, taking no issue slots) until the
-            // slot it refills next has been released by every consumer
-            const int ss = t - kG4Consumers;
-            if (ss < nstream) {
-                const int i0 = (int)(((long)it.y * ss) / nstream), i1 = (int)(((long)it.y * (ss + 1)) / nstream);
-                int slot = 0, phase = 0, issued = 0;
-                for (int pass = 0; pass < npass && !s_abort; pass++) {
-                    const int r0 = pass * nb;
-                    const int nbr = min(M - r0, nb);
-                    for (int i = i0; i < i1; i++) {
-                        const unsigned fb = full_sa + (slot * kG4MaxStreams + ss) * 8;
-                        // the slot's previous use completed empty phase (phase ^ 1)
-                        if (issued >= D &&
-                            !mbar_wait(empty_sa + (slot * kG4MaxStreams + ss) * 8, phase ^ 1, &s_abort)) {
-                            s_abort = 1;
-                            atomicExch(a.err, 1);
-                            break;
-                        }
-                        const int4 rec = s_rec[i];
-                        const int S = rec.w, Sp = S + 1, rym = rec.y >> 16;
-                        int sy0 = r0 + rym;
-                        if (sy0 >= M) sy0 -= M;
-                        const int ca = sy0 < S ? min(S, sy0 + nbr) - sy0 : 0;
-                        const int cb = sy0 + nbr > M ? min(S, sy0 + nbr - M) : 0;
-                        const unsigned dst = ring_sa + slot * kG4Slot + ss * sregion;
-                        mbar_arrive_tx(fb, (unsigned)((ca + cb) * Sp * 8));
-                        const float2 *src = a.ptab + rec.z;
-                        if (ca > 0) bulk_g2s(dst, src + (size_t)sy0 * Sp, (unsigned)(ca * Sp * 8), fb);
-                        if (cb > 0) bulk_g2s(dst + (unsigned)((M - sy0) * Sp * 8), src, (unsigned)(cb * Sp * 8), fb);
-                        issued++;
-                        if (++slot == D) {
-                            slot = 0;
-                            phase ^= 1;
-                        }
-                    }
-                }
-                if (s_abort) {
-                    // leave no copy in flight: wait (bounded) for the copies of
-                    // the last D records issued
-                    volatile int never = 0;
-                    for (int k = 0; k < D && k < issued; k++) {
-                        if (slot-- == 0) {
-                            slot = D - 1;
-                            phase ^= 1;
-                        }
-                        mbar_wait(full_sa + (slot * kG4MaxStreams + ss) * 8, phase, &never);
-                    }
-                }
-            }
-        } else {
-            const int cs = t / per_stream;
-            if (cs < nstream) {
-                const int rr = t - cs * per_stream;
-                const int col = rr % M, gl = rr / M;
-                const int i0 = (int)(((long)it.y * cs) / nstream), i1 = (int)(((long)it.y * (cs + 1)) / nstream);
-                int slot = 0, phase = 0;
-                for (int pass = 0; pass < npass; pass++) {
-                    const int r0 = pass * nb;
-                    int keyx = -1, keyw = -1;
-                    int last[KS];
-                    unsigned off[KS];
-                    float2 A[KS][P], B[KS][P];
-#pragma unroll
-                    for (int j = 0; j < KS; j++) {
-                        last[j] = -1;
-                        off[j] = kG4ZeroOff;
-#pragma unroll
-                        for (int p = 0; p < P; p++) A[j][p] = B[j][p] = make_float2(0.f, 0.f);
-                    }
-                    bool ok = true;
-                    for (int i = i0; i < i1; i++) {
-                        if (!mbar_wait(full_sa + (slot * kG4MaxStreams + cs) * 8, phase, &s_abort)) {
-                            s_abort = 1;
-                            atomicExch(a.err, 2);
-                            ok = false;
-                            break;
-                        }
-                        const int4 rec = s_rec[i];
-                        if (rec.x != keyx || rec.w != keyw) {
-                            keyx = rec.x;
-                            keyw = rec.w;
-                            const int S = rec.w, Sp = S + 1;
-                            int sx = col + (rec.y & 0xFFFF);
-                            sx -= (sx >= M) ? M : 0;
-                            const int rym = rec.y >> 16;
-#pragma unroll
-                            for (int j = 0; j < KS; j++) {
-                                const int r = r0 + gl + j * Gp;
-                                int sy = r + rym;
-                                sy -= (sy >= M) ? M : 0;
-                                const bool valid = (r < M) && (sx < S) && (sy < S);
-                                const int cell = valid ? rec.x + sy * a.nx + sx : -1;
-                                if (cell >= 0 && cell != last[j]) {
-                                    if (last[j] >= 0) flush_ab<P>(a.grid, a.dgrid, last[j], A[j], B[j]);
-                                    last[j] = cell;
-#pragma unroll
-                                    for (int p = 0; p < P; p++) A[j][p] = B[j][p] = make_float2(0.f, 0.f);
-                                }
-                                off[j] = valid ? (unsigned)(cs * sregion + ((r - r0) * Sp + sx) * 8)
-                                               : (unsigned)kG4ZeroOff;
-                            }
-                        }
-                        float2 vp[P], wp[P];
-#pragma unroll
-                        for (int p = 0; p < P; p++) {
-                            const float4 q = ((const float4 *)s_v)[(size_t)i * P + p];
-                            vp[p] = make_float2(q.x, q.y);
-                            wp[p] = make_float2(q.z, q.w);
-                        }
-                        const unsigned char *sb = ring + slot * kG4Slot;
-#pragma unroll
-                        for (int j = 0; j < KS; j++) {
-                            const float2 c = *(const float2 *)(sb + off[j]);
-#pragma unroll
-                            for (int p = 0; p < P; p++) {
-                                A[j][p] = __ffma2_rn(c, vp[p], A[j][p]);
-                                B[j][p] = __ffma2_rn(c, wp[p], B[j][p]);
-                            }
-                        }
-                        mbar_arrive(empty_sa + (slot * kG4MaxStreams + cs) * 8);
-                        if (++slot == D) {
-                            slot = 0;
-                            phase ^= 1;
-                        }
-                    }
-#pragma unroll
-                    for (int j = 0; j < KS; j++)
-                        if (last[j] >= 0) flush_ab<P>(a.grid, a.dgrid, last[j], A[j], B[j]);
-                    if (!ok) break;
-                }
-            }
-        }
+        if (clock64() - t0 > limit) return false;
     }
 }
 
@@ -1347,7 +1085,7 @@ __global__ void __launch_bounds__(kG3Threads, 2) k_grid5(Grid2Args a, int *err) 
     for (int k = 0;; k++) {
         const int b = k & 1;
         const unsigned ph = (unsigned)(k >> 1) & 1u;
-        if (!mbar_wait(full0 + 8 * b, ph, &s_abort)) {
+        if (!mbar_wait(full0 + 8 * b, ph, &s_abort, a.wait_cycles)) {
             fail();
             break;
         }
@@ -1362,7 +1100,7 @@ __global__ void __launch_bounds__(kG3Threads, 2) k_grid5(Grid2Args a, int *err) 
                                    (const unsigned short *)(B + LY::runend), ring);
         mbar_arrive(empty0 + 8 * b);
         if (warp == 0) {
-            if (!mbar_wait(empty0 + 8 * b, ph, &s_abort)) {
+            if (!mbar_wait(empty0 + 8 * b, ph, &s_abort, a.wait_cycles)) {
                 fail();
                 break;
             }
@@ -1788,44 +1526,10 @@ static int launch_grid5(const Grid2Args &a, int *err, cudaStream_t st) {
     return MTB_OK;
 }
 
-template <int P>
-static size_t grid4_smem() {
-    return (size_t)kG3Chunk * 16 * (1 + P) + (size_t)kG4Depth * kG4Slot + 2 * kG4Depth * kG4MaxStreams * 8;
-}
-
-template <int P>
-static int launch_grid4(const Grid4Args &a, cudaStream_t st) {
-    auto kern = k_grid4<P>;
-    const size_t smem = grid4_smem<P>();
-    MTB_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    int per_sm = 0;
-    MTB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kG4Threads, smem));
-    if (per_sm < 1) return MTB_ERR_BAD_SHAPE;
-    kern<<<per_sm * sm_count(), kG4Threads, smem, st>>>(a);
-    MTB_LAUNCHED();
-    return MTB_OK;
-}
-
 __global__ void k_set_moduli(BucketTable bt, int *__restrict__ M) {
     for (int b = threadIdx.x; b < kMaxBuckets; b += blockDim.x) M[b] = bt.M[b];
 }
 
-// First work item whose bucket goes to k_grid4 (items are in bucket order).
-__global__ void k_split(const int *__restrict__ bounds, const int *__restrict__ n_items, BucketTable bt, int min_m,
-                        int *__restrict__ split) {
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        int sp = *n_items;
-        for (int b = bt.n - 1; b >= 0; b--)
-            if (bt.M[b] >= min_m && bounds[2 * b + 1] > bounds[2 * b]) sp = bounds[2 * b];
-        *split = sp;
-    }
-}
-
-// Compensated merge of one call's FP64 contribution into the two-float grid:
-// (hi + lo) + delta evaluated in FP64 and split back into the float pair.  One
-// pass over the cells, no atomics; cells the call did not touch are skipped.
-// FP32 delta grid (default): hi + lo += delta with the rounding error of
-// hi + delta kept in lo (TwoSum).
 __global__ void k_merge_delta32(float4 *__restrict__ hi, float4 *__restrict__ lo, const float4 *__restrict__ delta,
                                 size_t n4) {
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n4; i += (size_t)gridDim.x * blockDim.x) {
@@ -1891,12 +1595,9 @@ struct GridSpace {
     unsigned long long *stats;
     void *cub;
     size_t cub_bytes;
-    float2 *ptab;        // row-padded copy of the table (rows of S + 1 taps)
     float4 *table2;      // padded table with each tap as {re, re, im, im} (k_grid3)
     int *pbase;          // first padded element, then first row, of every plane (k_pad_bases)
     int *moduli;         // bucket moduli of the plan (device copy)
-    int *split;          // first work item of k_grid4
-    int *counter4;       // k_grid4 work counter
     int *err;            // gridder pipeline error flag
     double *delta;       // this call's grid contribution (compensated mode; FP64 or FP32)
     G7Segment *segs;     // k_grid7 job segments (kMaxBuckets + 1)
@@ -1914,7 +1615,8 @@ static size_t cub_bytes(int n) {
     return std::max(a, std::max(b, c));
 }
 
-static void carve_grid(Arena &A, int R, int P, int chunk, size_t table_elems, size_t grid_cells, GridSpace *s,
+// delta_bytes: bytes of the per-call delta grid (0: none)
+static void carve_grid(Arena &A, int R, int P, int chunk, size_t table_elems, size_t delta_bytes, GridSpace *s,
                        int nw = 1) {
     size_t n = (size_t)(R > 0 ? R : 1);
     size_t nitems = n + n / (size_t)chunk + 2;
@@ -1940,14 +1642,11 @@ static void carve_grid(Arena &A, int R, int P, int chunk, size_t table_elems, si
     s->stats = A.take<unsigned long long>(4);
     s->cub_bytes = cub_bytes((int)n);
     s->cub = A.take<char>(s->cub_bytes);
-    s->ptab = A.take<float2>(table_elems ? table_elems : 1);
     s->table2 = A.take<float4>(table_elems ? table_elems : 1);
     s->pbase = A.take<int>(2 * (nw > 0 ? nw : 1) + 1);
     s->moduli = A.take<int>(kMaxBuckets);
-    s->split = A.take<int>(1);
-    s->counter4 = A.take<int>(1);
     s->err = A.take<int>(1);
-    s->delta = A.take<double>(grid_cells ? grid_cells * 2 * P : 1);
+    s->delta = A.take<double>(delta_bytes ? (delta_bytes + sizeof(double) - 1) / sizeof(double) : 1);
     s->segs = A.take<G7Segment>(kMaxBuckets + 1);
     s->n_segs = A.take<int>(1);
     s->counter7 = A.take<int>(1);
@@ -1983,15 +1682,43 @@ static bool capturing(cudaStream_t st) {
     return cudaStreamIsCapturing(st, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone;
 }
 
+// Wait bound of the rolling-items gridder's mbarrier waits: kWaitCycles, or
+// the MTB_GRIDDER_WAIT_CYCLES environment variable (read at every call, so a
+// test can make the waits run out and then restore the default).
+static long long wait_cycles() {
+    const char *e = std::getenv("MTB_GRIDDER_WAIT_CYCLES");
+    if (!e || !e[0]) return kWaitCycles;
+    const long long v = std::atoll(e);
+    return v >= 0 ? v : kWaitCycles;
+}
+
 static int gridder_of(const mtb_grid_params *p) {
     if (p->gridder != 0) return p->gridder;
     if (p->gridder_threads == 512) return 3;
-    return p->bulk_min_support > 0 ? 5 : 7;
+    return 7;
 }
 
-// the gridders that read the {re, re, im, im} table and the compact one
-static bool wants_expanded(const mtb_grid_params *) { return true; }
-static bool wants_compact(const mtb_grid_params *p) { return p->bulk_min_support > 0; }
+// Work items shorter than this many records multiply the flushes into each
+// cell: with the FP32 per-call delta grid, 37-record items took the first
+// configuration's image error to 1.2e-5 of its peak (above the 1e-5 bound),
+// so shorter items always accumulate the call in the FP64 delta grid.
+static const int kSafeChunk = 128;
+
+// The call's delta grid is FP64: asked for (exact_delta), or forced by short items.
+static bool exact_of(const mtb_grid_params *p) {
+    return p->exact_delta != 0 || (p->max_chunk > 0 && p->max_chunk < kSafeChunk);
+}
+
+// Bytes of the per-call delta grid a call reserves per grid cell and
+// polarisation: none when the calls pass no grid_lo (no_grid_lo) or merge in
+// shared memory (merge = 1, which writes (grid, grid_lo) itself), 8 for the
+// FP32 delta, 16 for the FP64 one.
+static size_t delta_bytes_per_cell_pol(const mtb_grid_params *p) {
+    if (p->no_grid_lo || p->merge == 1) return 0;
+    return exact_of(p) ? 2 * sizeof(double) : 2 * sizeof(float);
+}
+
+
 
 static int effective_chunk(const mtb_grid_params *p) {
     int c = p->max_chunk > 0 ? p->max_chunk : kDefaultChunk;
@@ -2009,11 +1736,10 @@ static int check_params(const mtb_grid_params *p) {
     if (!(p->u_increment > 0.0) || !(p->v_increment > 0.0) || !(p->w_sq_increment > 0.0)) return MTB_ERR_BAD_PARAM;
     if (p->tile < 0 || p->support_bucket < 0 || p->max_chunk < 0) return MTB_ERR_BAD_PARAM;
     if (p->merge < 0 || p->merge > 2) return MTB_ERR_BAD_PARAM;
-    if (p->bulk_min_support < 0) return MTB_ERR_BAD_PARAM;
+    if (p->bulk_min_support != 0) return MTB_ERR_BAD_PARAM;   // reserved (no bulk-copy gridder)
     if (p->gridder_threads != 0 && p->gridder_threads != 256 && p->gridder_threads != 512) return MTB_ERR_BAD_PARAM;
     if (p->gridder != 0 && p->gridder != 3 && p->gridder != 5 && p->gridder != 7) return MTB_ERR_BAD_PARAM;
     if ((p->gridder == 5 || p->gridder == 7) && p->gridder_threads == 512) return MTB_ERR_BAD_PARAM;
-    if (p->gridder == 7 && p->bulk_min_support > 0) return MTB_ERR_BAD_PARAM;
     return MTB_OK;
 }
 
@@ -2191,28 +1917,22 @@ static int prepare_grid(const mtb_grid_params *p, const GridPlan &plan, const fl
     }
     (void)end_bit;
     {
-        // compact padded rows for the bulk-copy gridder, the expanded copy
-        // for the others
-        float2 *pt = wants_compact(p) ? s.ptab : nullptr;
-        float4 *t2 = wants_expanded(p) ? s.table2 : nullptr;
+        // the expanded padded table the direct gridders read
         const int rows = plan.table_rows;
         const int pb = (int)std::min<size_t>(((size_t)rows + 7) / 8, (size_t)sms * 16);
-        k_pad_expand<<<pb > 0 ? pb : 1, 256, 0, st>>>(table, conv_info, s.pbase, p->wplanes, rows, pt, t2);
+        k_pad_expand<<<pb > 0 ? pb : 1, 256, 0, st>>>(table, conv_info, s.pbase, p->wplanes, rows, s.table2);
         MTB_LAUNCHED();
         (void)table_elems;
         (void)padded;
     }
     k_set_moduli<<<1, 32, 0, st>>>(plan.bt, s.moduli);
     MTB_LAUNCHED();
-    MTB_CUDA_TRY(cudaMemsetAsync(s.counter4, 0, sizeof(int), st));
     MTB_CUDA_TRY(cudaMemsetAsync(s.err, 0, sizeof(int), st));
     // compensated mode: the call's flushes go to a zeroed delta grid with
     // plain reductions (no returned values, so no stall at a flush) and one
     // pass merges it into the float pair (grid, grid_lo)
     if (compensated)
-        MTB_CUDA_TRY(cudaMemsetAsync(s.delta, 0,
-                                     (size_t)p->nx * p->ny * 2 * P * (p->exact_delta ? sizeof(double) : sizeof(float)),
-                                     st));
+        MTB_CUDA_TRY(cudaMemsetAsync(s.delta, 0, (size_t)p->nx * p->ny * P * delta_bytes_per_cell_pol(p), st));
     return MTB_OK;
 }
 
@@ -2224,8 +1944,8 @@ static GridJobDesc job_desc(const mtb_grid_params *p, float *grid, bool compensa
     d.table2 = s.table2;
     // compensated: flushes go to the call's delta grid, FP32 (vector
     // reductions, the default) or FP64 (exact_delta)
-    d.grid = (compensated && !p->exact_delta) ? (float *)s.delta : grid;
-    d.dgrid = (compensated && p->exact_delta) ? s.delta : nullptr;
+    d.grid = (compensated && !exact_of(p)) ? (float *)s.delta : grid;
+    d.dgrid = (compensated && exact_of(p)) ? s.delta : nullptr;
     d.M = s.moduli;
     d.nx = p->nx;
     // one odd support per bucket: every record's support is its bucket's modulus
@@ -2241,7 +1961,7 @@ static int finish_grid(const mtb_grid_params *p, float *grid, float *grid_lo, fl
     const int sms = sm_count();
     if (grid_lo) {
         const size_t n2 = (size_t)p->nx * p->ny * P;     // complex values
-        if (p->exact_delta) {
+        if (exact_of(p)) {
             int mb = (int)std::min<size_t>((n2 + 255) / 256, (size_t)sms * 16);
             k_merge_delta<<<mb > 0 ? mb : 1, 256, 0, st>>>((float2 *)grid, (float2 *)grid_lo,
                                                          (const double2 *)s.delta, n2);
@@ -2301,19 +2021,12 @@ static int run_grid(const mtb_grid_params *p, const GridPlan &plan, const float2
         MTB_LAUNCHED();
         return MTB_OK;
     }
-    // k_grid4 is opt-in (bulk_min_support > 0): it measured slower than
-    // k_grid3 on the mid-size workload
-    const bool bulk = p->bulk_min_support > 0;
-    if (bulk) {
-        const int min_m = p->bulk_min_support;
-        k_split<<<1, 1, 0, st>>>(s.bounds, s.n_items, plan.bt, min_m < kG4MinM ? kG4MinM : min_m, s.split);
-        MTB_LAUNCHED();
-    }
     Grid2Args g2;
     g2.items = s.items;
-    g2.n_items = bulk ? s.split : s.n_items;   // k_grid3 takes the items before the split
+    g2.n_items = s.n_items;
     g2.counter = s.counters;
     g2.njobs = 1;
+    g2.wait_cycles = wait_cycles();
     g2.jobs[0] = job_desc<P>(p, grid, grid_lo != nullptr, s);
     const int which = gridder_of(p);
     const bool rolling = which == 5;
@@ -2339,21 +2052,7 @@ static int run_grid(const mtb_grid_params *p, const GridPlan &plan, const float2
     } else {
         MTB_TRY(launch_grid3<P>(g2, p->gridder_threads, st));
     }
-    Grid4Args g4;
-    g4.items = s.items;
-    g4.first = s.split;
-    g4.n_items = s.n_items;
-    g4.counter = s.counter4;
-    g4.wpos = s.wpos;
-    g4.wvis4 = (const float4 *)s.wvis;
-    g4.ptab = s.ptab;
-    g4.grid = g2.jobs[0].grid;
-    g4.dgrid = g2.jobs[0].dgrid;
-    g4.nx = p->nx;
-    g4.bt = plan.bt;
-    g4.err = s.err;
-    if (bulk) MTB_TRY(launch_grid4<P>(g4, st));
-    if ((bulk || rolling) && check_gridder() && !capturing(st)) {
+    if (rolling && check_gridder() && !capturing(st)) {
         int e = 0;
         MTB_CUDA_TRY(cudaMemcpyAsync(&e, s.err, sizeof(int), cudaMemcpyDeviceToHost, st));
         MTB_CUDA_TRY(cudaStreamSynchronize(st));
@@ -2397,7 +2096,8 @@ extern "C" int mtb_grid_workspace_size(const mtb_grid_params *p, const int *h_co
     int chunk = effective_chunk(p);
     Arena A;
     GridSpace s;
-    carve_grid(A, nrecords, p->npol, chunk, padded_elems_of(p, h_conv_info), (size_t)p->nx * p->ny, &s,
+    carve_grid(A, nrecords, p->npol, chunk, padded_elems_of(p, h_conv_info),
+               (size_t)p->nx * p->ny * p->npol * delta_bytes_per_cell_pol(p), &s,
                p->wplanes);
     *bytes = A.used;
     return MTB_OK;
@@ -2427,9 +2127,11 @@ extern "C" int mtb_grid(const mtb_grid_params *p, const void *d_table, const int
     if (!d_table || !d_conv_info || !d_conv_sums || !d_uvw || !d_freq || (!d_vis && !p->psf) || !d_weights ||
         !d_flags || !d_workspace)
         return MTB_ERR_NULL;
+    if (d_grid_lo && p->no_grid_lo) return MTB_ERR_BAD_PARAM;   // its workspace holds no delta grid
     Arena A(d_workspace, workspace_bytes);
     GridSpace s;
-    carve_grid(A, nrecords, P, plan.chunk, padded_elems_of(p, h_conv_info), (size_t)p->nx * p->ny, &s,
+    carve_grid(A, nrecords, P, plan.chunk, padded_elems_of(p, h_conv_info),
+               (size_t)p->nx * p->ny * P * delta_bytes_per_cell_pol(p), &s,
                p->wplanes);
     if (!A.ok()) return MTB_ERR_WORKSPACE;
     const float2 *tb = (const float2 *)d_table;
@@ -2499,9 +2201,10 @@ static void carve_batch(Arena &A, const mtb_grid_job *jobs, int njobs, const Gri
                         int4 **items, int **n_total, int **counter, G7Segment **segs) {
     size_t cap = 0;
     for (int j = 0; j < njobs; j++) {
-        const mtb_grid_params *p = &jobs[j].params;
-        carve_grid(A, jobs[j].nrecords, p->npol, plans[j].chunk, padded_elems_of(p, jobs[j].h_conv_info),
-                   (size_t)p->nx * p->ny, &spaces[j], p->wplanes);
+        mtb_grid_params p = jobs[j].params;
+        p.merge = 0;                      // the batch runs the direct gridders
+        carve_grid(A, jobs[j].nrecords, p.npol, plans[j].chunk, padded_elems_of(&p, jobs[j].h_conv_info),
+                   (size_t)p.nx * p.ny * p.npol * delta_bytes_per_cell_pol(&p), &spaces[j], p.wplanes);
         const size_t r = (size_t)(jobs[j].nrecords > 0 ? jobs[j].nrecords : 1);
         cap += r + r / (size_t)plans[j].chunk + 2;
     }
@@ -2532,6 +2235,7 @@ static int run_batch(const mtb_grid_job *jobs, int njobs, const GridPlan *plans,
     BatchQueues q;
     Grid2Args g2;
     g2.njobs = njobs;
+    g2.wait_cycles = wait_cycles();
     for (int j = 0; j < njobs; j++) {
         const mtb_grid_job &J = jobs[j];
         mtb_grid_params p = J.params;
@@ -2606,6 +2310,7 @@ extern "C" int mtb_grid_batch(const mtb_grid_job *jobs, int njobs, void *d_works
         if (J.nrecords > 0 && (!J.d_table || !J.d_conv_info || !J.d_conv_sums || !J.d_uvw || !J.d_freq ||
                                (!J.d_vis && !J.params.psf) || !J.d_weights || !J.d_flags))
             return MTB_ERR_NULL;
+        if (J.d_grid_lo && J.params.no_grid_lo) return MTB_ERR_BAD_PARAM;
     }
     if (!d_workspace) return MTB_ERR_NULL;
     GridPlan plans[kMaxBatch];

@@ -15,9 +15,10 @@ const int kTiles[] = {16, 32, 64};
 const int kBuckets[] = {1, 2};
 // (gridder, records per work item, block size): the block-staged gridder at
 // two item lengths and two block sizes, the rolling-items gridder (items of at
-// most 256 records, 256 threads)
-const int kShapes[][3] = {{3, 256, 256}, {3, 256, 512}, {3, 512, 256}, {3, 512, 512}, {5, 256, 256}};
-const int kNShapes = 5;
+// most 256 records, 256 threads), the streaming gridder at two item lengths
+const int kShapes[][3] = {{3, 256, 256}, {3, 256, 512}, {3, 512, 256}, {3, 512, 512},
+                          {5, 256, 256}, {7, 256, 256}, {7, 512, 256}};
+const int kNShapes = 7;
 const int kCandidates = 3 * 2 * kNShapes;
 
 mtb_grid_tuning candidate(int c) {
@@ -51,6 +52,8 @@ struct Events {
 };
 
 }  // namespace
+
+extern "C" int mtb_grid_autotune_candidate_count(void) { return kCandidates; }
 
 extern "C" int mtb_grid_autotune_workspace_size(const mtb_grid_job *jobs, int njobs, size_t *bytes) {
     if (!jobs || !bytes) return MTB_ERR_NULL;

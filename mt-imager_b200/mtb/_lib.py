@@ -34,7 +34,7 @@ EXPORTS = (
     "mtb_finalize_workspace_size", "mtb_finalize", "mtb_status_string", "mtb_version",
     "mtb_release_caches", "mtb_kernel_launch_count", "mtb_calibrate_fp32",
     "mtb_taper_kernel_build", "mtb_grid_batch_workspace_size", "mtb_grid_batch",
-    "mtb_grid_autotune_workspace_size", "mtb_grid_autotune", "mtb_sort_index", "mtb_gather_rows", "mtb_fits_create", "mtb_fits_write_channel", "mtb_fits_close",
+    "mtb_grid_autotune_workspace_size", "mtb_grid_autotune", "mtb_grid_autotune_candidate_count", "mtb_sort_index", "mtb_gather_rows", "mtb_fits_create", "mtb_fits_write_channel", "mtb_fits_close",
     "mtb_engine_create", "mtb_engine_submit", "mtb_engine_wait", "mtb_engine_request_bytes", "mtb_engine_destroy",
 )
 
@@ -67,7 +67,8 @@ class GridParams(ctypes.Structure):
                 ("support_bucket", ctypes.c_int), ("max_chunk", ctypes.c_int), ("merge", ctypes.c_int),
                 ("gridder_start_event", ctypes.c_void_p), ("gridder_end_event", ctypes.c_void_p),
                 ("bulk_min_support", ctypes.c_int), ("psf", ctypes.c_int), ("exact_delta", ctypes.c_int),
-                ("gridder_threads", ctypes.c_int), ("gridder", ctypes.c_int), ("flags_u8", ctypes.c_int)]
+                ("gridder_threads", ctypes.c_int), ("gridder", ctypes.c_int), ("flags_u8", ctypes.c_int),
+                ("no_grid_lo", ctypes.c_int)]
 
 
 class GridStats(ctypes.Structure):
@@ -157,6 +158,7 @@ def load(path: str = LIB_PATH):
     L.mtb_sort_index.argtypes = [p, p, i, i, p, ctypes.POINTER(i)]
     L.mtb_gather_rows.argtypes = [p, sz, sz, sz, p, i, p, i]
     L.mtb_grid_autotune_workspace_size.argtypes = [ctypes.POINTER(GridJob), i, ctypes.POINTER(sz)]
+    L.mtb_grid_autotune_candidate_count.argtypes = []
     L.mtb_grid_autotune.argtypes = [ctypes.POINTER(GridJob), i, p, sz, p, ctypes.POINTER(GridTuning),
                                     ctypes.POINTER(GridTuning)]
     L.mtb_fits_create.argtypes = [ctypes.c_char_p, ctypes.POINTER(FitsHeader), ctypes.POINTER(p)]

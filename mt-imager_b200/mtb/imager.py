@@ -143,7 +143,7 @@ class WProjectionImager:
 
     def __init__(self, nx, ny, l_increment, m_increment=None, wplanes=32, sampling=8, npol=4,
                  trial_support=0, max_support=0, w_max=0.0, pol_type=L.MTB_POL_LINEAR, compensated=True,
-                 tile=0, support_bucket=0, max_chunk=0, merge=0, bulk_min_support=0, device="cuda",
+                 tile=0, support_bucket=0, max_chunk=0, merge=0, device="cuda",
                  kernels: KernelTable | None = None, psf=False, mode="wproj", taper_support=7,
                  exact_delta=False, gridder_threads=0, gridder=0):
         """mode "wproj" (W-projection kernels) or "normal" (taper-only kernel of
@@ -166,7 +166,7 @@ class WProjectionImager:
         self.compensated = compensated
         self.pol_type = pol_type
         self.tuning = dict(tile=tile, support_bucket=support_bucket, max_chunk=max_chunk, merge=merge,
-                           bulk_min_support=bulk_min_support, gridder_threads=gridder_threads, gridder=gridder)
+                           gridder_threads=gridder_threads, gridder=gridder)
         self.grid = torch.zeros((ny, nx, npol), dtype=torch.complex64, device=self.device)
         self.grid_lo = torch.zeros_like(self.grid) if compensated else None
         self.normalizer = torch.zeros(npol, dtype=torch.float32, device=self.device)
@@ -195,9 +195,9 @@ class WProjectionImager:
                           k.info.u_increment, k.info.v_increment, k.info.w_sq_increment, int(initialize),
                           self.tuning["tile"], self.tuning["support_bucket"], self.tuning["max_chunk"],
                           self.tuning["merge"])
-        gp.bulk_min_support = self.tuning["bulk_min_support"]
         gp.psf = int(self.psf)
         gp.exact_delta = int(self.exact_delta)
+        gp.no_grid_lo = 0 if self.compensated else 1
         gp.gridder_threads = self.tuning["gridder_threads"]
         gp.gridder = self.tuning["gridder"]
         if self.gridder_events is not None:
@@ -330,7 +330,6 @@ def grid_batch(entries, workspace=None, stream=None):
 
 
 TUNING_KEYS = ("tile", "support_bucket", "max_chunk", "gridder_threads", "gridder")
-N_CANDIDATES = 30
 
 
 def autotune(entries, workspace=None, stream=None):
@@ -352,7 +351,7 @@ def autotune(entries, workspace=None, stream=None):
     if workspace is None or workspace.numel() < need.value:
         workspace = torch.empty(max(1, need.value), dtype=torch.uint8, device=entries[0][0].device)
     best = L.GridTuning()
-    cands = (L.GridTuning * N_CANDIDATES)()
+    cands = (L.GridTuning * lib.mtb_grid_autotune_candidate_count())()
     L.check(lib.mtb_grid_autotune(jobs, len(entries), _ptr(workspace), need.value, _stream(stream),
                                   ctypes.byref(best), cands), "mtb_grid_autotune")
     as_dict = lambda t: dict({k: getattr(t, k) for k in TUNING_KEYS}, ms=t.ms)  # noqa: E731

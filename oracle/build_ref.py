@@ -8,7 +8,10 @@ files and the library under oracle/_ref/ (git-ignored).  The library is used
 to make the golden fixtures under tests/golden/ (tests/golden/make_golden.py)
 and is never loaded by the product.
 
-    python oracle/build_ref.py [--reference DIR]
+    python oracle/build_ref.py --reference DIR      (or MTB_REFERENCE_DIR=DIR)
+
+The reference tree's location comes from the argument or the environment
+variable only; without either, nothing is built.
 """
 from __future__ import annotations
 
@@ -20,7 +23,7 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "_ref")
-DEFAULT_REF = "/root/reference"
+ENV_REF = "MTB_REFERENCE_DIR"
 
 # (directory inside the reference's code/ tree, source file)
 SOURCES = [
@@ -53,7 +56,13 @@ def nvcc():
     return cand if os.path.exists(cand) else "nvcc"
 
 
-def build(reference: str = DEFAULT_REF, verbose: bool = False) -> str | None:
+def build(reference: str | None = None, verbose: bool = False) -> str | None:
+    """Builds the library from the reference tree at `reference` (default: the
+    MTB_REFERENCE_DIR environment variable); returns None when no tree is
+    given or found."""
+    reference = reference or os.environ.get(ENV_REF)
+    if not reference:
+        return None
     code = os.path.join(reference, "code")
     if not os.path.isdir(code):
         return None
@@ -96,8 +105,8 @@ def _stub_mtime():
 
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default=DEFAULT_REF)
+    ap.add_argument("--reference", default=None, help="the reference tree (default: $%s)" % ENV_REF)
     a = ap.parse_args()
     out = build(a.reference, verbose=True)
     if out is None:
-        sys.exit("reference tree not found at %s" % a.reference)
+        sys.exit("no reference tree: pass --reference DIR or set %s" % ENV_REF)

@@ -167,6 +167,7 @@ def _valid_grid_params():
     ("merge", 3, L.MTB_ERR_BAD_PARAM),
     ("gridder_threads", 384, L.MTB_ERR_BAD_PARAM),
     ("gridder", 4, L.MTB_ERR_BAD_PARAM),
+    ("bulk_min_support", 17, L.MTB_ERR_BAD_PARAM),   # reserved: the bulk-copy gridder was removed
     ("max_chunk", -1, L.MTB_ERR_BAD_PARAM),
 ])
 def test_grid_parameter_refusals(mtblib, field, value, status):
@@ -189,9 +190,10 @@ def test_grid_refuses_negative_records_and_rolling_512(mtblib):
     p = _valid_grid_params()
     assert mtblib.mtb_grid_workspace_size(ctypes.byref(p), ctypes.cast(info, ctypes.c_void_p), -1,
                                           ctypes.byref(n)) == L.MTB_ERR_BAD_SHAPE
-    p.gridder, p.gridder_threads = 5, 512     # the rolling-items gridder runs 256-thread blocks only
-    assert mtblib.mtb_grid_workspace_size(ctypes.byref(p), ctypes.cast(info, ctypes.c_void_p), 10,
-                                          ctypes.byref(n)) == L.MTB_ERR_BAD_PARAM
+    for g in (5, 7):                          # the rolling and streaming gridders run 256-thread blocks only
+        p.gridder, p.gridder_threads = g, 512
+        assert mtblib.mtb_grid_workspace_size(ctypes.byref(p), ctypes.cast(info, ctypes.c_void_p), 10,
+                                              ctypes.byref(n)) == L.MTB_ERR_BAD_PARAM
     assert mtblib.mtb_grid_workspace_size(None, ctypes.cast(info, ctypes.c_void_p), 10,
                                           ctypes.byref(n)) == L.MTB_ERR_NULL
 
@@ -225,3 +227,40 @@ def test_wkernel_parameter_refusals(mtblib, kw, status):
     base.update(kw)
     p = L.WKernelParams(**base)
     assert mtblib.mtb_wkernel_query(ctypes.byref(p), ctypes.byref(L.WKernelInfo())) == status
+
+
+def _ws(mtblib, p, records=1000):
+    info = (ctypes.c_int * 2)(7, 0)
+    n = ctypes.c_size_t(0)
+    assert mtblib.mtb_grid_workspace_size(ctypes.byref(p), ctypes.cast(info, ctypes.c_void_p), records,
+                                          ctypes.byref(n)) == L.MTB_OK
+    return n.value
+
+
+def test_workspace_delta_grid_by_mode(mtblib):
+    """The per-call delta grid is sized by the accumulation mode: none for
+    calls without grid_lo (no_grid_lo) or with the shared-memory tile merge,
+    8 bytes per cell and polarisation for the FP32 delta, 16 for the FP64 one
+    (exact_delta, or work items shorter than 128 records, which always use it)."""
+    cells = 1024 * 1024 * 4
+    base = _valid_grid_params()
+    p = L.GridParams.from_buffer_copy(base)
+    p.no_grid_lo = 1
+    none = _ws(mtblib, p)
+    fp32 = _ws(mtblib, base)
+    p = L.GridParams.from_buffer_copy(base)
+    p.exact_delta = 1
+    fp64 = _ws(mtblib, p)
+    p = L.GridParams.from_buffer_copy(base)
+    p.max_chunk = 64
+    short = _ws(mtblib, p)
+    p = L.GridParams.from_buffer_copy(base)
+    p.merge = 1
+    window = _ws(mtblib, p)
+    assert abs((fp32 - none) - 8 * cells) < 512
+    assert abs((fp64 - none) - 16 * cells) < 512
+    assert abs((short - none) - 16 * cells) < 512      # short items use the FP64 delta
+    assert abs(window - none) < 512
+    p = L.GridParams.from_buffer_copy(base)
+    p.max_chunk = 128
+    assert abs(_ws(mtblib, p) - fp32) < 512             # at the safe length the FP32 delta stays

@@ -95,10 +95,10 @@ def test_autotune_grids_with_the_chosen_knobs():
     cs = cases()[:3]
     ims = [imager(setup) for setup, *_ in cs]
     best, cands, ws = autotune([(im, *arrs) for im, (setup, *arrs) in zip(ims, cs)])
-    assert len(cands) == 30 and all(c["ms"] > 0 for c in cands)
+    assert len(cands) == 42 and all(c["ms"] > 0 for c in cands)
     assert best["ms"] == min(c["ms"] for c in cands)
     assert {c["tile"] for c in cands} == {16, 32, 64} and {c["gridder_threads"] for c in cands} == {256, 512}
-    assert {c["gridder"] for c in cands} == {3, 5}
+    assert {c["gridder"] for c in cands} == {3, 5, 7}
     knobs = {k: best[k] for k in TUNING_KEYS}
     single = []
     for setup, *arrs in cs:

@@ -53,6 +53,20 @@ def test_mtb_grid_byte_flags_equal_int32():
     assert same(b, a) and same(c, a)
 
 
+def test_any_nonzero_flag_is_flagged():
+    """The flag contract is 0 = keep, any other value = flagged: flags of 2
+    (int32) and 0xFF (a bool column written as bytes) grid exactly like 1.  The
+    reference weights by 1 - flag, which agrees for 0 / 1 and would give a
+    negative weight for other values."""
+    obs, setup = case(seed=33)
+    fl = obs.flags[0].astype(np.int32)
+    a, sa, _ = image(obs, setup, fl)
+    b, sb, _ = image(obs, setup, fl * 2)
+    c, sc, _ = image(obs, setup, (fl * 255).astype(np.uint8))
+    assert sa == sb == sc
+    assert same(b, a) and same(c, a)
+
+
 def test_preprocess_byte_flags_bit_exact():
     obs, setup = case(seed=32)
     im = imager(setup)

@@ -163,7 +163,7 @@ def test_chunked_equals_single(cfg1):
 @pytest.mark.parametrize("tuning", [dict(tile=16), dict(tile=64), dict(support_bucket=3),
                                     dict(max_chunk=37, exact_delta=True),
                                     dict(merge=1), dict(merge=2), dict(merge=1, tile=16),
-                                    dict(bulk_min_support=17), dict(bulk_min_support=25), dict(exact_delta=True),
+                                    dict(exact_delta=True),
                                     dict(gridder_threads=512), dict(gridder_threads=512, tile=16, max_chunk=256),
                                     dict(gridder=5), dict(gridder=5, tile=64),
                                     dict(gridder=7), dict(gridder=7, tile=64), dict(gridder=7, tile=16),
@@ -179,7 +179,7 @@ def test_tuning_does_not_change_result(cfg1, tuning):
 
 @pytest.mark.parametrize("kw", [dict(), dict(tile=64), dict(nx=320, s=3), dict(merge=1), dict(gridder=5),
                                 dict(gridder=7), dict(nx=320, s=3, gridder=7),
-                                dict(bulk_min_support=17), dict(nx=320, s=3, bulk_min_support=17)])
+                                ])
 def test_large_supports(oracle, kw):
     """Supports up to 55 (and 105 with odd sampling): the direct gridders
     (block-staged, rolling-items and bulk-copy; one and several record
@@ -187,13 +187,12 @@ def test_large_supports(oracle, kw):
     blocks."""
     tile = kw.pop("tile", 0)
     merge = kw.pop("merge", 0)
-    bulk = kw.pop("bulk_min_support", 0)
     gridder = kw.pop("gridder", 0)
     obs, setup = wide_case(**kw)
     geo = oracle.geometry_for(setup)
     kern = oracle.wkernels(geo)
     img_o, grid_o, norm_o = oracle.image_channel(obs, 0, setup, kern, geo)
-    im, img = run_gpu(obs, setup, tile=tile, merge=merge, bulk_min_support=bulk, gridder=gridder)
+    im, img = run_gpu(obs, setup, tile=tile, merge=merge, gridder=gridder)
     assert np.array_equal(im.kernels.conv_info, kern["conv_info"])
     assert np.abs(im.kernels.table.cpu().numpy() - kern["table"]).max() <= KERNEL_TOL
     g = im.grid_sum().cpu().numpy()
