@@ -214,7 +214,8 @@ def run_reference(args, rank, world):
     from oracle import oracle as O
     spec = workload_spec(args)
     rng = np.random.default_rng(2)
-    nbl = args.ref_baselines if spec["name"] == "mid" else None
+    nt_full = int(round(spec["hours"] * 3600.0 / spec["dt"]))
+    nbl = max(1, cpu_sample_records(args, spec, nt_full) // nt_full) if spec["name"] == "mid" else None
     uvw, _, _ = make_uvw(spec, "cpu", torch, rng, nbl_limit=nbl)
     full, _, _ = make_uvw(spec, "cpu", torch, np.random.default_rng(2), nbl_limit=None, nt_limit=8)
     dl = cell_for(spec, float(full[:2].abs().max()), torch)
@@ -297,6 +298,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-serve", action="store_true", help="skip the request-stream measurement")
+    ap.add_argument("--no-oracle", action="store_true", help="skip the FP64 oracle check of the first channel")
+    ap.add_argument("--no-cube", action="store_true", help="skip the batched-cubes measurement")
     ap.add_argument("--cube-images", type=int, default=64)
     ap.add_argument("--cube-min-hours", type=float, default=1.0)
     ap.add_argument("--cube-max-hours", type=float, default=8.0)
@@ -305,9 +308,6 @@ def main():
     ap.add_argument("--serve-rate", type=float, default=20.0, help="Poisson arrival rate, requests per second")
     ap.add_argument("--serve-min-records", type=float, default=1e5)
     ap.add_argument("--serve-max-records", type=float, default=5e7)
-    ap.add_argument("--serve-sample-requests", type=int, default=40,
-                    help="requests of the shortened stream the default (mid-size) run measures")
-    ap.add_argument("--serve-sample-max-records", type=float, default=5e6)
     ap.add_argument("--serve-slots", type=int, default=8)
     ap.add_argument("--clock-log", default=None,
                     help="directory that keeps the nvidia-smi clock samples of the timed region")
@@ -512,24 +512,30 @@ def main():
             e2e = {"value": None, "skipped": "pinned host copies of %d ranks (%.0f GB) exceed 60 %% of the host's "
                                           "available memory" % (local_ranks, pinned * local_ranks / 1e9)}
 
+    # ---- the first channel's image against the FP64 oracle (rank 0, one GPU)
+    oracle = None
+    if rank == 0 and world == 1 and not args.no_oracle:
+        oracle = oracle_check(spec, dl, uvw, chans[0], images[0], kern)
+
     # ---- CPU baseline (rank 0, one GPU)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        cpu = cpu_baseline(args, spec, uvw, chans, kern, dl, torch)
+        cpu = cpu_baseline(args, spec, uvw, chans, kern, dl, torch, nt)
 
-    # ---- request stream: engine vs plain path (rank 0, one GPU)
-    serve = None
-    if rank == 0 and world == 1 and not args.no_serve:
+    # ---- batched cubes and the request stream (rank 0, one GPU): the other
+    # two configurations of the workload, measured after the main line
+    cube, serve = None, None
+    if rank == 0 and world == 1 and (not args.no_cube or not args.no_serve):
         chans.clear()
         imagers.clear()
         images.clear()
+        del uvw, weights
         torch.cuda.empty_cache()
-        # a shortened stream of the serving configuration (same arrivals, image
-        # sizes and record distribution, fewer and smaller requests)
-        sample = argparse.Namespace(**vars(args))
-        sample.serve_requests = args.serve_sample_requests
-        sample.serve_max_records = args.serve_sample_max_records
-        serve = run_serve(sample, torch, dev)
+        if not args.no_cube:
+            cube = run_cube(args, torch, dev)
+            torch.cuda.empty_cache()
+        if not args.no_serve:
+            serve = run_serve(args, torch, dev)
 
     if rank == 0:
         sup = kern.supports
@@ -556,6 +562,10 @@ def main():
             line["cpu_baseline"] = cpu
         if clk:
             line["clocks"] = clk
+        if oracle:
+            line["oracle_check"] = oracle
+        if cube:
+            line["cube"] = cube
         if serve:
             line["serving"] = serve
         print(json.dumps(line), flush=True)
@@ -853,9 +863,17 @@ def run_serve(args, torch, dev):
     for n in sorted({r["nx"] for r in reqs}):
         warm.append(min((r for r in reqs if r["nx"] == n), key=lambda r: r["freq"].size))
 
-    def plain(r):
-        im = WProjectionImager(r["nx"], r["nx"], r["dl"], wplanes=r["wplanes"], device=dev, **common)
-        im.build_kernels()
+    kcache = {}
+
+    def plain(r, cached=False):
+        """One request alone: w-kernels built for it (as the reference does
+        per run) or, cached=True, taken from a per-geometry cache."""
+        key = (r["nx"], r["dl"], r["wplanes"])
+        im = WProjectionImager(r["nx"], r["nx"], r["dl"], wplanes=r["wplanes"], device=dev,
+                               kernels=kcache.get(key) if cached else None, **common)
+        k = im.build_kernels()
+        if cached:
+            kcache[key] = k
         R = r["freq"].size
         for a in range(0, R, 1 << 22):
             b = min(R, a + (1 << 22))
@@ -869,19 +887,24 @@ def run_serve(args, torch, dev):
     torch.cuda.synchronize()
 
     # (b) plain path: service times measured back to back, then FIFO queueing
-    service = []
-    samples_plain = 0
-    for r in reqs:
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        samples_plain += plain(r)
-        service.append(time.perf_counter() - t0)
-    done, lat_plain = 0.0, []
-    for r, sv in zip(reqs, service):
-        start = max(r["arrival"], done)
-        done = start + sv
-        lat_plain.append((done - r["arrival"]) * 1e3)
-    span_plain = done - reqs[0]["arrival"]
+    def plain_stream(cached):
+        service, samples = [], 0
+        for r in reqs:
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            samples += plain(r, cached)
+            service.append(time.perf_counter() - t0)
+        done, lat = 0.0, []
+        for r, sv in zip(reqs, service):
+            start = max(r["arrival"], done)
+            done = start + sv
+            lat.append((done - r["arrival"]) * 1e3)
+        return service, samples, lat, done - reqs[0]["arrival"]
+
+    service, samples_plain, lat_plain, span_plain = plain_stream(False)
+    for r in warm:                # the cache starts with the warm-up geometries, as the engine's does
+        plain(r, True)
+    service_c, samples_c, lat_c, span_c = plain_stream(True)
 
     # (a) engine, real-time arrivals; a waiter thread collects results as they
     # finish (images dropped) while this thread submits
@@ -962,23 +985,68 @@ def run_serve(args, torch, dev):
                    "max_service_ms": float(np.max([v for _, v in queue_service]))},
         "plain": {"samples_per_s": samples_plain / span_plain, "p50_ms": float(np.percentile(lat_plain, 50)),
                   "p99_ms": float(np.percentile(lat_plain, 99)), "makespan_s": span_plain,
-                  "mean_service_ms": float(np.mean(service)) * 1e3},
+                  "mean_service_ms": float(np.mean(service)) * 1e3,
+                  "w_kernels": "built for every request (as the reference does per run)"},
+        "plain_cached_kernels": {"samples_per_s": samples_c / span_c, "p50_ms": float(np.percentile(lat_c, 50)),
+                                 "p99_ms": float(np.percentile(lat_c, 99)), "makespan_s": span_c,
+                                 "mean_service_ms": float(np.mean(service_c)) * 1e3,
+                                 "w_kernels": "cached per geometry (isolates the engine's overlap from its cache)"},
         "speedup_samples_per_s": (samples_eng / span_eng) / (samples_plain / span_plain),
+        "speedup_vs_cached_plain": (samples_eng / span_eng) / (samples_c / span_c),
         "saturation": {"engine_samples_per_s": sum(4 * n for _, n in burst) / burst_s, "engine_makespan_s": burst_s,
                        "plain_samples_per_s": samples_plain / float(np.sum(service)),
+                       "plain_cached_samples_per_s": samples_c / float(np.sum(service_c)),
                        "speedup": (sum(4 * n for _, n in burst) / burst_s) / (samples_plain / float(np.sum(service))),
+                       "speedup_vs_cached_plain": (sum(4 * n for _, n in burst) / burst_s) /
+                                                  (samples_c / float(np.sum(service_c))),
                        "note": "all requests queued at once; plain = total samples / summed service times"},
         "datagen_s": t_gen,
     }
 
 
-def cpu_baseline(args, spec, uvw_d, chans, kern, dl, torch, min_seconds=12.0, max_passes=40):
+def oracle_check(spec, dl, uvw_d, chan, image_d, kern):
+    """The image of one full channel against the FP64 W-projection oracle
+    (oracle/, on the host cores), outside the timed region: the RMS error of
+    every Stokes plane relative to the Stokes I peak (bound 1e-5), and the
+    kernel table's largest deviation (bound 1e-6)."""
+    from oracle import oracle as O
+    t0 = time.perf_counter()
+    n = spec["nx"]
+    geo = O.kernel_geometry(n, n, dl, dl, spec["wplanes"], spec["sampling"], spec["trial_support"],
+                            spec["max_support"])
+    ko = O.wkernels(geo)
+    if not np.array_equal(ko["conv_info"], kern.conv_info):
+        return {"error": "kernel supports differ from the oracle's"}
+    tab_err = float(np.abs(kern.table.cpu().numpy() - ko["table"]).max())
+    freq, vis, weights, flags = chan
+    g, nrm, _ = O.grid_chunk(uvw_d.cpu().numpy(), freq.cpu().numpy(), vis.cpu().numpy(), weights.cpu().numpy(),
+                             flags.cpu().numpy().astype(np.int32), geo, ko)
+    img_o = O.finalize(g, nrm, geo)
+    img = image_d.cpu().numpy()
+    peak = float(np.abs(img_o[0]).max())
+    err = {s: float(np.sqrt(np.mean((img[p] - img_o[p]) ** 2)) / peak) for p, s in enumerate("IQUV")}
+    return {"image_rms_vs_oracle": err, "bound": 1e-5, "kernel_table_max_abs_err": tab_err, "kernel_bound": 1e-6,
+            "records": int(uvw_d.shape[1]), "oracle_s": time.perf_counter() - t0,
+            "oracle": "FP64 W-projection restatement (oracle/wproj_oracle.c + numpy FFT), host cores"}
+
+
+def cpu_sample_records(args, spec, nt):
+    """Records of the CPU sample, the same for this line's cpu_baseline and the
+    --impl reference arm: the first args.ref_baselines baselines of one channel
+    over the full track (records are baseline-major), or --cpu-records."""
+    if args.cpu_records:
+        return int(args.cpu_records)
+    nbl_all = spec["n_ant"] * (spec["n_ant"] - 1) // 2
+    return min(args.ref_baselines, nbl_all) * nt if spec["name"] == "mid" else nbl_all * nt
+
+
+def cpu_baseline(args, spec, uvw_d, chans, kern, dl, torch, nt, min_seconds=12.0, max_passes=40):
     """FP32 OpenMP port of the reference's gridding on the host cores, on a
-    bounded sample: the first records of one channel, gridded repeatedly until
-    about min_seconds of CPU time have been spent."""
+    bounded sample (cpu_sample_records) of one channel, gridded repeatedly
+    until about min_seconds of CPU time have been spent."""
     from oracle import oracle as O
     R = uvw_d.shape[1]
-    n_rec = args.cpu_records or min(R, 4_000_000)
+    n_rec = min(R, cpu_sample_records(args, spec, nt))
     freq, vis, weights, flags = chans[len(chans) // 2]
     u = np.ascontiguousarray(uvw_d[:, :n_rec].cpu().numpy())
     fq = np.ascontiguousarray(freq[:n_rec].cpu().numpy())
@@ -1002,9 +1070,11 @@ def cpu_baseline(args, spec, uvw_d, chans, kern, dl, torch, min_seconds=12.0, ma
         dt += time.perf_counter() - t0
         samples += int(st[0] + st[1]) * 4
         passes += 1
+    nbl_all = spec["n_ant"] * (spec["n_ant"] - 1) // 2
     return {"value": samples / dt, "unit": "samples/s", "cores": P.port_threads(), "kind": "port",
-            "sample": "first %d records of one channel, %d passes (%d samples gridded in %.1f s), FP32 OpenMP port"
-                      % (n_rec, passes, samples, dt)}
+            "sample": "%d records of one %s channel (%d of %d baselines, full track), %d passes (%d samples "
+                      "gridded in %.1f s), FP32 OpenMP port"
+                      % (n_rec, spec["name"], n_rec // max(1, nt), nbl_all, passes, samples, dt)}
 
 
 if __name__ == "__main__":

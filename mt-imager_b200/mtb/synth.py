@@ -195,7 +195,7 @@ def small_config(seed=0, n_ant=8, ntimes=40, nx=64, cell_arcsec=20.0, wplanes=8,
     return obs, setup
 
 
-def config3(seed=3, full=True):
+def config3(seed=3, full=True, torch=None):
     """Precision stress, wide field: 64 antennas within 10 km, 1 channel at
     725 MHz (|u| up to ~48 klambda fits the 8192^2 grid at 1.5 arcsec, and
     |w| reaches ~5e4 lambda), 12 h at 4 s (2016 x 10,800 = 21,772,800
@@ -203,12 +203,16 @@ def config3(seed=3, full=True):
     oversampling 8, support <= 129 (trial support 131), w_max = max |w|.
     full=False keeps the field, the array extent and the kernels' support
     range with 12 antennas, 12 h at 120 s (66 x 360 = 23,760 records) and 64
-    w-planes: a case the FP64 oracle finishes in about a minute."""
+    w-planes: a case the FP64 oracle finishes in about a minute.
+    Visibilities are predicted on the device when `torch` is given."""
     freq = 725e6
     nx, cell = 8192, 1.5
     obs = make_observation(n_ant=64 if full else 12, radius_m=10000.0, freqs_hz=(freq,), hours=12.0,
                            dt_s=4.0 if full else 120.0, dec_deg=-45.0, nsrc=20, fov_rad=nx * cell * ARCSEC,
-                           noise=0.0, seed=seed)
+                           noise=0.0, seed=seed, predict=torch is None)
+    if torch is not None:
+        obs.vis[0] = predict_vis_torch(torch.from_numpy(obs.uvw).cuda(), freq, obs.meta["sources"],
+                                       torch).cpu().numpy()
     w_max = float(np.abs(obs.uvw[2].astype(np.float64)).max() * freq / C_LIGHT)
     setup = ImagingSetup(nx=nx, ny=nx, cell_arcsec=cell, wplanes=256 if full else 64, sampling=8,
                          trial_support=131, max_support=129, w_max=w_max)

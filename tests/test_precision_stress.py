@@ -2,16 +2,18 @@
 the FP64 W-projection oracle, with the RMS error of every Stokes image
 relative to the Stokes I peak printed and held to 1e-5, and the kernel table
 held to 1e-6.
-  wide  precision stress, wide field: 8192^2, 256 w-planes, support <= 129,
-        |w| to ~5e4 lambda (synth.config3)
+  wide  precision stress, wide field, at full size: 8192^2, 256 w-planes,
+        supports 7-129, |w| to ~4e4 lambda, 21,772,800 records (synth.config3;
+        about a minute of FP64 oracle gridding on 16 host cores)
+  wide_reduced  the same field, array extent and support range with 23,760
+        records and 64 w-planes
   mid   one channel of the mid-size configuration: 4096^2, 128 w-planes,
-        supports 7-65, 25 % flagged (synth.config2_channel)
+        supports 7-65, 25 % flagged (synth.config2_channel), by default with
+        fewer records; MTB_PRECISION_FULL=1 runs it at full size (29.0 M
+        records; the benchmark checks a full channel against the oracle too)
 
-By default both run with fewer records (and the wide field with fewer
-w-planes); MTB_PRECISION_FULL=1 runs the full configurations (21.8 M and
-29.0 M records; minutes of FP64 oracle work on the host).  The GPU grids in
-chunks of 4,194,304 records into the compensated two-float grid, as a long
-observation is imaged.
+The GPU grids in chunks of 4,194,304 records into the compensated two-float
+grid, as a long observation is imaged.
 """
 import os
 import time
@@ -30,11 +32,11 @@ IMAGE_RMS_TOL = 1e-5
 CHUNK = 1 << 22
 
 
-@pytest.mark.parametrize("case", ["wide", "mid"])
+@pytest.mark.parametrize("case", ["wide", "wide_reduced", "mid"])
 def test_stated_image_error(oracle, case):
-    full = os.environ.get("MTB_PRECISION_FULL") == "1"
-    if case == "wide":
-        obs, setup = synth.config3(full=full)
+    full = case == "wide" or os.environ.get("MTB_PRECISION_FULL") == "1"
+    if case.startswith("wide"):
+        obs, setup = synth.config3(full=full, torch=torch)
     else:
         obs, setup = synth.config2_channel(full=full, torch=torch)
     t0 = time.perf_counter()
