@@ -264,7 +264,74 @@ def run_reference(args, rank, world):
             "impl": "reference", "config": {"workload": workload_name(spec), "sample": sample},
             "cpu_baseline": {"value": v, "unit": "samples/s", "cores": cores, "kind": "port", "sample": sample},
             "e2e": {"value": v, "unit": "samples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if not args.no_ref_gpu:
+        line["reference_gpu"] = reference_gpu(spec, geo, table, sums, kern["conv_info"], uvw_np, freq, vis,
+                                              weights, flags, samples // max(1, args.steps), torch)
     print(json.dumps(line), flush=True)
+
+
+REF_CHUNK = 1000000   # records per WImager chunk: mt-imager's default `records` (mtimager.properties:47-48)
+
+
+def reference_gpu(spec, geo, table, sums, conv_info, uvw, freq, vis, weights, flags, samples, torch):
+    """mt-imager's own gridding operators on this GPU: the reference's
+    PreProcessUVW ... ConvolutionGridder sources rebuilt unchanged for sm_100a
+    (oracle/_ref/libmtref.so, oracle/ref_harness.cu), run over the same sample
+    in chunks of the reference's default 1,000,000 records, each chunk through
+    the operator graph of one WImager chunk.  Reported: samples/s over the
+    ConvolutionGridder kernels' own events, and over the whole graph (each
+    operator's span; the harness synchronises between operators)."""
+    path = os.path.join(ROOT, "oracle", "_ref", "libmtref.so")
+    if not torch.cuda.is_available():
+        return {"unavailable": "no CUDA device"}
+    if not os.path.exists(path):
+        return {"unavailable": "oracle/_ref/libmtref.so not built (needs the reference sources)"}
+    lib = ctypes.CDLL(path)
+    lib.mtref_grid_chunk.restype = ctypes.c_int
+    lib.mtref_last_chunk_ms.restype = ctypes.c_int
+    n = spec["nx"]
+    R = uvw.shape[1]
+    table = np.ascontiguousarray(table, np.complex64)
+    sums = np.ascontiguousarray(sums, np.float32)
+    ci = np.ascontiguousarray(conv_info, np.int32)
+    grid = np.zeros((n, n, 4), np.complex64)
+    err = ctypes.create_string_buffer(512)
+    nul = ctypes.c_void_p(None)
+    bounds = [(a, min(R, a + REF_CHUNK)) for a in range(0, R, REF_CHUNK)]
+    if len(bounds) > 1 and bounds[-1][1] - bounds[-1][0] < 2048:
+        bounds[-2:] = [(bounds[-2][0], R)]
+
+    def chunk(a, b, first):
+        u = np.ascontiguousarray(uvw[:, a:b])
+        parts = [np.ascontiguousarray(x[a:b]) for x in (freq, vis, weights, flags)]
+        rc = lib.mtref_grid_chunk(n, n, 4, spec["sampling"], spec["wplanes"], ctypes.c_float(geo["du"]),
+                                  ctypes.c_float(geo["dv"]), ctypes.c_float(geo["w_inc"]), _ptr(table),
+                                  int(table.size), _ptr(ci), _ptr(sums), _ptr(u), *[_ptr(x) for x in parts],
+                                  int(b - a), 1 if first else 0, _ptr(grid), nul, nul, nul, nul, nul, nul, nul,
+                                  err, 512)
+        if rc != 0:
+            raise RuntimeError(err.value.decode())
+        g, c = ctypes.c_float(0), ctypes.c_float(0)
+        lib.mtref_last_chunk_ms(ctypes.byref(g), ctypes.byref(c))
+        return g.value, c.value
+    try:
+        chunk(*bounds[0], True)                       # module load and first-launch costs
+        g_ms = c_ms = 0.0
+        for i, (a, b) in enumerate(bounds):
+            g, c = chunk(a, b, i == 0)
+            g_ms += g
+            c_ms += c
+    except RuntimeError as e:
+        return {"unavailable": "reference operators refused this sample: %s" % e}
+    return {"value": samples / (c_ms * 1e-3), "unit": "samples/s",
+            "gridder_value": samples / (g_ms * 1e-3), "gridder_ms": g_ms, "graph_ms": c_ms,
+            "chunks": len(bounds), "chunk_records": REF_CHUNK, "device": torch.cuda.get_device_name(0),
+            "kind": "reference operators rebuilt for sm_100a (oracle/_ref), run one at a time",
+            "sample": "the cpu_baseline sample (%d records) in chunks of %d records" % (R, REF_CHUNK)}
+
+
+def _ptr(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
 
 
 def workload_name(spec):
@@ -300,6 +367,8 @@ def main():
     ap.add_argument("--no-serve", action="store_true", help="skip the request-stream measurement")
     ap.add_argument("--no-oracle", action="store_true", help="skip the FP64 oracle check of the first channel")
     ap.add_argument("--no-cube", action="store_true", help="skip the batched-cubes measurement")
+    ap.add_argument("--no-ref-gpu", action="store_true",
+                    help="reference arm: skip timing the reference's own gridding operators on the GPU")
     ap.add_argument("--cube-images", type=int, default=64)
     ap.add_argument("--cube-min-hours", type=float, default=1.0)
     ap.add_argument("--cube-max-hours", type=float, default=8.0)

@@ -180,7 +180,17 @@ typedef struct mtb_grid_params {
                                   FP64 delta; 1: the calls pass d_grid_lo = NULL, the
                                   workspace holds no delta grid and mtb_grid refuses a
                                   d_grid_lo.  merge = 1 never needs one                   */
+    int external_delta;        /* 1: the per-call delta grid is the caller's d_delta (of
+                                  mtb_grid_delta_bytes bytes) and the workspace holds none:
+                                  an engine that caps scratch buffers (GAFW's int buffer
+                                  size) keeps it as a reusable array of its own           */
+    void *d_delta;             /* with external_delta: the delta grid (device, 256-byte
+                                  aligned); contents need not be kept between calls       */
 } mtb_grid_params;
+
+/* Bytes of the per-call delta grid a compensated call uses (0 when it needs
+ * none: no_grid_lo or merge = 1); what d_delta must hold with external_delta. */
+int mtb_grid_delta_bytes(const mtb_grid_params *p, size_t *bytes);
 
 typedef struct mtb_grid_stats {
     unsigned long long gridded_records;     /* Statistic:TotalGriddedRecords    (WImager.cpp:173) */
@@ -342,9 +352,16 @@ typedef struct mtb_finalize_params {
     int nx, ny, npol;
     int sampling;            /* SincCorrector "sampling" = wproj.convFunction.sampling */
     int pol_type;            /* MTB_POL_LINEAR or MTB_POL_CIRCULAR                     */
+    int external_planes;     /* 1: the FP64 FFT planes are the caller's d_planes (of
+                                mtb_finalize_planes_bytes bytes) and the workspace holds
+                                only the cuFFT work area (for engines that cap scratch
+                                buffers, such as GAFW's int buffer size)                */
+    void *d_planes;          /* with external_planes: complex128 [P][ny][nx] (device,
+                                256-byte aligned); contents need not be kept            */
 } mtb_finalize_params;
 
 int mtb_finalize_workspace_size(const mtb_finalize_params *p, size_t *bytes);
+int mtb_finalize_planes_bytes(const mtb_finalize_params *p, size_t *bytes);
 
 /* Grid (+ optional compensation term) and normaliser to the corrected Stokes
  * cube: ImageFinalizer::calculate (ImageFinalizer.cpp:60-65). */

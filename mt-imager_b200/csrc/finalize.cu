@@ -106,12 +106,14 @@ struct FSpace {
     size_t work_bytes;
 };
 
+// The FP64 planes come from the workspace, or are the caller's (external_planes).
 static int carve_fin(const mtb_finalize_params *p, void *ws, size_t bytes, FSpace *f, size_t *need) {
     cufftHandle h;
     size_t fw = 0;
     MTB_TRY(fft_plan(CUFFT_Z2Z, p->ny, p->nx, p->npol, &h, &fw));
     Arena A(ws, bytes);
-    f->planes = A.take<double2>((size_t)p->nx * p->ny * p->npol);
+    if (p->external_planes) f->planes = (double2 *)p->d_planes;
+    else f->planes = A.take<double2>((size_t)p->nx * p->ny * p->npol);
     f->fx = A.take<double>(p->nx);
     f->fy = A.take<double>(p->ny);
     f->work = A.take<char>(fw ? fw : 1);
@@ -140,11 +142,20 @@ extern "C" int mtb_finalize_workspace_size(const mtb_finalize_params *p, size_t 
     return carve_fin(p, nullptr, 0, &f, bytes);
 }
 
+extern "C" int mtb_finalize_planes_bytes(const mtb_finalize_params *p, size_t *bytes) {
+    if (!bytes) return MTB_ERR_NULL;
+    MTB_TRY(check_fin(p));
+    *bytes = (size_t)p->nx * p->ny * p->npol * sizeof(double2);
+    return MTB_OK;
+}
+
 extern "C" int mtb_finalize(const mtb_finalize_params *p, const void *d_grid, const void *d_grid_lo,
                             const float *d_normalizer, float *d_image, void *d_workspace, size_t workspace_bytes,
                             mtb_stream_t stream) {
     MTB_TRY(check_fin(p));
     if (!d_grid || !d_normalizer || !d_image || !d_workspace) return MTB_ERR_NULL;
+    if (p->external_planes && !p->d_planes) return MTB_ERR_NULL;
+    if (p->external_planes && (uintptr_t)p->d_planes % 256) return MTB_ERR_BAD_PARAM;
     cudaStream_t st = (cudaStream_t)stream;
     FSpace f;
     size_t need = 0;

@@ -1718,6 +1718,13 @@ static size_t delta_bytes_per_cell_pol(const mtb_grid_params *p) {
     return exact_of(p) ? 2 * sizeof(double) : 2 * sizeof(float);
 }
 
+// Bytes of the delta grid the call needs, and those its workspace holds (none
+// when the caller passes its own: external_delta).
+static size_t delta_bytes(const mtb_grid_params *p) {
+    return (size_t)p->nx * p->ny * p->npol * delta_bytes_per_cell_pol(p);
+}
+static size_t workspace_delta_bytes(const mtb_grid_params *p) { return p->external_delta ? 0 : delta_bytes(p); }
+
 
 
 static int effective_chunk(const mtb_grid_params *p) {
@@ -1932,7 +1939,7 @@ static int prepare_grid(const mtb_grid_params *p, const GridPlan &plan, const fl
     // plain reductions (no returned values, so no stall at a flush) and one
     // pass merges it into the float pair (grid, grid_lo)
     if (compensated)
-        MTB_CUDA_TRY(cudaMemsetAsync(s.delta, 0, (size_t)p->nx * p->ny * P * delta_bytes_per_cell_pol(p), st));
+        MTB_CUDA_TRY(cudaMemsetAsync(s.delta, 0, delta_bytes(p), st));
     return MTB_OK;
 }
 
@@ -2096,10 +2103,16 @@ extern "C" int mtb_grid_workspace_size(const mtb_grid_params *p, const int *h_co
     int chunk = effective_chunk(p);
     Arena A;
     GridSpace s;
-    carve_grid(A, nrecords, p->npol, chunk, padded_elems_of(p, h_conv_info),
-               (size_t)p->nx * p->ny * p->npol * delta_bytes_per_cell_pol(p), &s,
+    carve_grid(A, nrecords, p->npol, chunk, padded_elems_of(p, h_conv_info), workspace_delta_bytes(p), &s,
                p->wplanes);
     *bytes = A.used;
+    return MTB_OK;
+}
+
+extern "C" int mtb_grid_delta_bytes(const mtb_grid_params *p, size_t *bytes) {
+    if (!bytes) return MTB_ERR_NULL;
+    MTB_TRY(check_params(p));
+    *bytes = delta_bytes(p);
     return MTB_OK;
 }
 
@@ -2130,10 +2143,14 @@ extern "C" int mtb_grid(const mtb_grid_params *p, const void *d_table, const int
     if (d_grid_lo && p->no_grid_lo) return MTB_ERR_BAD_PARAM;   // its workspace holds no delta grid
     Arena A(d_workspace, workspace_bytes);
     GridSpace s;
-    carve_grid(A, nrecords, P, plan.chunk, padded_elems_of(p, h_conv_info),
-               (size_t)p->nx * p->ny * P * delta_bytes_per_cell_pol(p), &s,
+    carve_grid(A, nrecords, P, plan.chunk, padded_elems_of(p, h_conv_info), workspace_delta_bytes(p), &s,
                p->wplanes);
     if (!A.ok()) return MTB_ERR_WORKSPACE;
+    if (p->external_delta && delta_bytes(p)) {
+        if (!p->d_delta) return MTB_ERR_NULL;
+        if ((uintptr_t)p->d_delta % 256) return MTB_ERR_BAD_PARAM;
+        s.delta = (double *)p->d_delta;
+    }
     const float2 *tb = (const float2 *)d_table;
     const float2 *vis = (const float2 *)d_vis;
     float *g = (float *)d_grid, *lo = (float *)d_grid_lo;
@@ -2181,6 +2198,7 @@ static int check_batch(const mtb_grid_job *jobs, int njobs) {
         if (jobs[j].params.npol != jobs[0].params.npol) return MTB_ERR_BAD_SHAPE;
         if (jobs[j].params.gridder_threads != jobs[0].params.gridder_threads) return MTB_ERR_BAD_PARAM;
         if (jobs[j].params.gridder != jobs[0].params.gridder) return MTB_ERR_BAD_PARAM;
+        if (jobs[j].params.external_delta) return MTB_ERR_BAD_PARAM;   // batches carve their delta grids
         if (jobs[j].nrecords < 0) return MTB_ERR_BAD_SHAPE;
         if (!jobs[j].h_conv_info) return MTB_ERR_NULL;
     }
@@ -2204,7 +2222,7 @@ static void carve_batch(Arena &A, const mtb_grid_job *jobs, int njobs, const Gri
         mtb_grid_params p = jobs[j].params;
         p.merge = 0;                      // the batch runs the direct gridders
         carve_grid(A, jobs[j].nrecords, p.npol, plans[j].chunk, padded_elems_of(&p, jobs[j].h_conv_info),
-                   (size_t)p.nx * p.ny * p.npol * delta_bytes_per_cell_pol(&p), &spaces[j], p.wplanes);
+                   workspace_delta_bytes(&p), &spaces[j], p.wplanes);
         const size_t r = (size_t)(jobs[j].nrecords > 0 ? jobs[j].nrecords : 1);
         cap += r + r / (size_t)plans[j].chunk + 2;
     }

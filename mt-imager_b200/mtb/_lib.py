@@ -31,7 +31,8 @@ MTB_POL_CIRCULAR = 1
 EXPORTS = (
     "mtb_wkernel_query", "mtb_wkernel_build", "mtb_grid_workspace_size", "mtb_grid", "mtb_preprocess_uvw",
     "mtb_preprocess_uvw_noalloc", "mtb_preprocess_uvw_noalloc_capacity",
-    "mtb_finalize_workspace_size", "mtb_finalize", "mtb_status_string", "mtb_version",
+    "mtb_finalize_workspace_size", "mtb_finalize", "mtb_finalize_planes_bytes", "mtb_grid_delta_bytes",
+    "mtb_status_string", "mtb_version",
     "mtb_release_caches", "mtb_kernel_launch_count", "mtb_calibrate_fp32",
     "mtb_taper_kernel_build", "mtb_grid_batch_workspace_size", "mtb_grid_batch",
     "mtb_grid_autotune_workspace_size", "mtb_grid_autotune", "mtb_grid_autotune_candidate_count", "mtb_sort_index", "mtb_gather_rows", "mtb_fits_create", "mtb_fits_write_channel", "mtb_fits_close",
@@ -68,7 +69,7 @@ class GridParams(ctypes.Structure):
                 ("gridder_start_event", ctypes.c_void_p), ("gridder_end_event", ctypes.c_void_p),
                 ("bulk_min_support", ctypes.c_int), ("psf", ctypes.c_int), ("exact_delta", ctypes.c_int),
                 ("gridder_threads", ctypes.c_int), ("gridder", ctypes.c_int), ("flags_u8", ctypes.c_int),
-                ("no_grid_lo", ctypes.c_int)]
+                ("no_grid_lo", ctypes.c_int), ("external_delta", ctypes.c_int), ("d_delta", ctypes.c_void_p)]
 
 
 class GridStats(ctypes.Structure):
@@ -78,7 +79,7 @@ class GridStats(ctypes.Structure):
 
 class FinalizeParams(ctypes.Structure):
     _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("npol", ctypes.c_int), ("sampling", ctypes.c_int),
-                ("pol_type", ctypes.c_int)]
+                ("pol_type", ctypes.c_int), ("external_planes", ctypes.c_int), ("d_planes", ctypes.c_void_p)]
 
 
 class GridJob(ctypes.Structure):
@@ -143,6 +144,8 @@ def load(path: str = LIB_PATH):
     L.mtb_taper_kernel_build.argtypes = [i, i, p, sz, p, p, p, ctypes.POINTER(sz), p]
     L.mtb_finalize_workspace_size.argtypes = [ctypes.POINTER(FinalizeParams), ctypes.POINTER(sz)]
     L.mtb_finalize.argtypes = [ctypes.POINTER(FinalizeParams), p, p, p, p, p, sz, p]
+    L.mtb_finalize_planes_bytes.argtypes = [ctypes.POINTER(FinalizeParams), ctypes.POINTER(sz)]
+    L.mtb_grid_delta_bytes.argtypes = [ctypes.POINTER(GridParams), ctypes.POINTER(sz)]
     for name in EXPORTS:
         getattr(L, name).restype = i
     L.mtb_status_string.restype = ctypes.c_char_p

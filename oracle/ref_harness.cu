@@ -117,16 +117,23 @@ Arr make(std::vector<unsigned> dims, StoreType t, size_t eb) { return Arr(new De
 
 struct Runner {
     cudaStream_t stream = 0;
-    cudaEvent_t ev0, ev1;
+    cudaEvent_t ev0, ev1;          // handed to the operators (GPUSubmissionData)
+    cudaEvent_t t0, t1;            // the harness's own span around each submission
+    double chain_ms = 0.0;         // sum of the submissions' spans
+    float own_ms = 0.0f;           // the last operator's own start..end events, when it records both
     GAFW::GPU::GPUDeviceDescriptor device;
     Runner() {
         checkCudaError(cudaStreamCreate(&stream), "stream");
         checkCudaError(cudaEventCreate(&ev0), "event");
         checkCudaError(cudaEventCreate(&ev1), "event");
+        checkCudaError(cudaEventCreate(&t0), "event");
+        checkCudaError(cudaEventCreate(&t1), "event");
     }
     ~Runner() {
         cudaEventDestroy(ev0);
         cudaEventDestroy(ev1);
+        cudaEventDestroy(t0);
+        cudaEventDestroy(t1);
         cudaStreamDestroy(stream);
     }
     // One submitToGPU with the engine's bookkeeping: events, post-run hook,
@@ -148,9 +155,16 @@ struct Runner {
         d.endEvent = &ev1;
         d.params = params;
         d.deviceDescriptor = &device;
+        checkCudaError(cudaEventRecord(t0, stream), "event");
         op.submitToGPU(d);
+        checkCudaError(cudaEventRecord(t1, stream), "event");
         checkCudaError(cudaGetLastError(), "launch of " + op.nickname);
         checkCudaError(cudaStreamSynchronize(stream), "run of " + op.nickname);
+        float ms = 0.0f;
+        checkCudaError(cudaEventElapsedTime(&ms, t0, t1), "elapsed");
+        chain_ms += ms;
+        own_ms = ms;
+        if (d.endEventRecorded && cudaEventElapsedTime(&ms, ev0, ev1) == cudaSuccess) own_ms = ms;
         if (post) op.postRunExecute(post);
     }
 };
@@ -187,6 +201,10 @@ int fail(char *err, int errlen, const char *msg) {
     return 1;
 }
 
+// Spans of the last mtref_grid_chunk call (milliseconds).
+float g_gridder_ms = 0.0f;   // ConvolutionGridder's own start..end events: its two kernels
+float g_chain_ms = 0.0f;     // every operator of the chunk's graph, PreProcessUVW to the gridder
+
 }  // namespace
 
 extern "C" {
@@ -208,6 +226,15 @@ int mtref_grid_chunk(int nx, int ny, int npol, int sampling, int wplanes, float 
     try {
         if (npol != 1 && npol != 2 && npol != 4) return fail(err, errlen, "npol must be 1, 2 or 4");
         if (R < 2048) return fail(err, errlen, "the reference plan kernels need at least 2048 records");
+        // ConvolutionGridder reads the table through a linear texture whose
+        // creation it does not check (ConvolutionGridder.cu:520-534)
+        {
+            int dev = 0, width = 0;
+            checkCudaError(cudaGetDevice(&dev), "device");
+            checkCudaError(cudaDeviceGetAttribute(&width, cudaDevAttrMaxTexture1DLinearWidth, dev), "attribute");
+            if (table_elems <= 0 || table_elems > width)
+                return fail(err, errlen, "kernel table larger than a linear texture");
+        }
         const unsigned U = (unsigned)R, P = (unsigned)npol, W = (unsigned)wplanes;
         const unsigned T = (unsigned)(sampling % 2 ? sampling : sampling + 1);
         Runner run;
@@ -308,9 +335,21 @@ int mtref_grid_chunk(int nx, int ny, int npol, int sampling, int wplanes, float 
         run.submit(gridder, {bdi2.get(), d_index.get(), g_data.get(), cvis.get(), a_table.get(), d_cidx.get()},
                    {g.get()}, gp);
         g->download(grid);
+        g_gridder_ms = run.own_ms;
+        g_chain_ms = (float)run.chain_ms;
     } catch (const std::exception &e) {
         return fail(err, errlen, e.what());
     }
+    return 0;
+}
+
+/* Device time of the last successful mtref_grid_chunk: the ConvolutionGridder
+ * operator's kernels (its own events) and the whole operator graph of the
+ * chunk (each submission's span, summed; the harness synchronises between
+ * them as GAFW's engine does not). */
+int mtref_last_chunk_ms(float *gridder_ms, float *chain_ms) {
+    if (gridder_ms) *gridder_ms = g_gridder_ms;
+    if (chain_ms) *chain_ms = g_chain_ms;
     return 0;
 }
 

@@ -4,12 +4,16 @@
  * A minimal stand-in for the GAFW engine headers, written for this project,
  * so that mt-imager's own operator sources (their kernels and submitToGPU
  * launch code) compile unchanged outside GAFW and can be driven by
- * oracle/ref_harness.cu to produce reference outputs.  Only the names those
- * sources use are provided; the interface mirrors GAFW's
+ * oracle/ref_harness.cu to produce reference outputs, and so that the GAFW
+ * operator adapter (mt-imager_b200/gafw_adapter/) compiles and runs in the
+ * tests.  Only the names those sources use are provided; the interface
+ * mirrors GAFW's
  * (gafw/Implimentation/GPUImplimentation/GPUafw.h:28-70,
  *  GPUSubmissionData.h:27-47, GPUArrayOperator.h:27-43,
- *  gafw/pil/ArrayDimensions.h:62-83) because the operator sources are
- * written against it.  The engine itself (scheduling, memory, validation)
+ *  gafw/pil/ArrayDimensions.h:31-83, GeneralImplimentation/Array.h:59-78,
+ *  GeneralImplimentation/ArrayOperator.h:41-91,
+ *  GeneralImplimentation/GAFWValidationException.h:29-45) because the operator
+ * sources are written against it.  The engine itself (scheduling, memory, validation)
  * is not reproduced: the harness allocates every buffer and calls
  * submitToGPU directly.
  */
@@ -52,6 +56,10 @@ class ArrayDimensions {
 public:
     ArrayDimensions() {}
     explicit ArrayDimensions(const std::vector<unsigned> &d) : dims(d) {}
+    ArrayDimensions(int noOfDims, int dim0 = 0, int dim1 = 0, int dim2 = 0, int dim3 = 0, int dim4 = 0) {
+        const int d[5] = {dim0, dim1, dim2, dim3, dim4};
+        for (int i = 0; i < noOfDims && i < 5; i++) dims.push_back((unsigned)d[i]);
+    }
     int getNoOfDimensions() const { return (int)dims.size(); }
     unsigned getNoOfColumns() const { return dims.empty() ? 0 : dims.back(); }
     unsigned getNoOfRows() const { return dims.size() < 2 ? 1 : dims[dims.size() - 2]; }
@@ -69,7 +77,25 @@ public:
 namespace GeneralImplimentation {
 enum StoreType { real_int, real_uint, real_float, real_double, complex_float, complex_double, real_longint,
                  real_ulongint, real_shortint, real_ushortint, StoreTypeUnknown };
-}
+
+// An operator's input or output as validate() sees it.
+class Array {
+public:
+    ArrayDimensions getDimensions() { return dim; }
+    void setDimensions(ArrayDimensions d) { dim = d; }
+    StoreType getType() { return type; }
+    void setType(StoreType t) { type = t; }
+    bool isDefined() { return dim.getNoOfDimensions() > 0; }
+    ArrayDimensions dim;
+    StoreType type = StoreTypeUnknown;
+};
+
+class GAFWValidationException : public GeneralException {
+public:
+    GAFWValidationException(std::string desc, void *, int linenumber, std::string file)
+        : GeneralException(desc + " (" + file + ":" + std::to_string(linenumber) + ")") {}
+};
+}  // namespace GeneralImplimentation
 
 namespace Tools { namespace CppProperties {
 class Properties {
@@ -164,8 +190,19 @@ public:
     void logInfo(int, const std::string &) {}
     GAFW::Tools::CppProperties::Properties params;
     std::string nickname, name;
+    std::vector<GAFW::GeneralImplimentation::Array *> inputs;
+    std::vector<GAFW::GeneralImplimentation::Array *> outputs;
+    // throws unless the parameter is set with this type
+    void checkParameter(std::string param, GAFW::Tools::CppProperties::Properties::PropertyType type) {
+        if (params.getPropertyType(param) != type)
+            throw GAFW::GeneralImplimentation::GAFWValidationException("parameter " + param + " has another type",
+                                                                       this, __LINE__, __FILE__);
+    }
 };
 }  // namespace GPU
 }  // namespace GAFW
+
+#define ValidationException(description) \
+    GAFW::GeneralImplimentation::GAFWValidationException(description, this, __LINE__, __FILE__)
 
 #endif

@@ -66,8 +66,15 @@ int main(void)
     int conv_info[2] = {7, 0};
     size_t bytes = 0;
     CHECK(mtb_grid_workspace_size(&gp, conv_info, 100, &bytes) == MTB_ERR_BAD_SHAPE);
-    mtb_finalize_params fp = {1024, 1024, 4, 8, 2};   /* pol_type 2: neither linear nor circular */
+    /* the per-call delta grid: FP32 pairs by default, none without grid_lo */
+    gp.npol = 4;
+    CHECK(mtb_grid_delta_bytes(&gp, &bytes) == MTB_OK && bytes == (size_t)1024 * 1024 * 4 * 8);
+    gp.no_grid_lo = 1;
+    CHECK(mtb_grid_delta_bytes(&gp, &bytes) == MTB_OK && bytes == 0);
+    mtb_finalize_params fp = {1024, 1024, 4, 8, 2, 0, NULL};   /* pol_type 2: neither linear nor circular */
     CHECK(mtb_finalize_workspace_size(&fp, &bytes) == MTB_ERR_BAD_PARAM);
+    fp.pol_type = MTB_POL_LINEAR;
+    CHECK(mtb_finalize_planes_bytes(&fp, &bytes) == MTB_OK && bytes == (size_t)4 * 1024 * 1024 * 16);
     mtb_wkernel_params wp;
     memset(&wp, 0, sizeof(wp));
     wp.nx = wp.ny = 256;
