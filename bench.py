@@ -270,6 +270,7 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+GRIDDER_TRAFFIC = {7: 5.018e9}   # bytes per launch, one 8 h mid-size channel (ncu)
 REF_CHUNK = 1000000   # records per WImager chunk: mt-imager's default `records` (mtimager.properties:47-48)
 
 
@@ -550,15 +551,23 @@ def main():
             "mtb_calibrate_fp32")
     gridder_ms = float(np.mean(gms))
     achieved = flops_per_step / (gridder_ms * 1e-3) / 1e12
-    # DRAM bytes of one gridder launch of this workload's channel (8 h, 4096^2),
-    # measured with ncu (dram__bytes_read.sum + dram__bytes_write.sum, 1 pass);
-    # other workloads were not captured
-    traffic = 4.90e9 if (spec["name"] == "mid" and spec["hours"] == 8.0 and R == 29030400) else None
+    # DRAM bytes of one gridder launch over one channel of this workload (8 h,
+    # 4096^2), measured with ncu (dram__bytes_read.sum + dram__bytes_write.sum,
+    # one pass; profiles/k_grid7_mid4096_8h_dram.md); other workloads and
+    # gridders were not captured
+    gridder = args.gridder or 7
+    traffic = (GRIDDER_TRAFFIC.get(gridder) if (spec["name"] == "mid" and spec["hours"] == 8.0 and R == 29030400)
+               else None)
+    props = torch.cuda.get_device_properties(dev)
+    spec_peak = props.multi_processor_count * 128 * 2 * 1.965e9 / 1e12
     roof = {"bound": "fp32", "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
             "frac": achieved / peak.value if peak.value else None, "traffic": traffic,
             "traffic_unit": "bytes per gridder launch (one channel), ncu dram__bytes_read+write",
-            "kernel": "k_grid (all support buckets of one mtb_grid call, span timed by events)",
-            "peak_source": "measured: mtb_calibrate_fp32 (packed f32x2 FMA chains, this GPU)"}
+            "kernel": "k_grid7 (gridder %d: job segments + the streaming gridder of one mtb_grid call, "
+                      "span timed by events)" % gridder if gridder in (7, 8) else "gridder %d" % gridder,
+            "peak_source": "measured: mtb_calibrate_fp32 (packed f32x2 FMA chains, this GPU)",
+            "peak_spec": spec_peak, "frac_of_spec": achieved / spec_peak,
+            "peak_spec_source": "SMs x 128 FP32 lanes x 2 flop x 1965 MHz (clocks.max.sm)"}
 
     # ---- end to end: host buffers, H2D per channel overlapped with compute
     e2e = None

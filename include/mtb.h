@@ -162,14 +162,17 @@ typedef struct mtb_grid_params {
                                   FP32 delta's rounding past the 1e-5 image bound           */
     int gridder_threads;       /* 0: 256; threads of a gridder block, which grids one work
                                   item at a time (256 or 512)                              */
-    int gridder;               /* 0: default (5, or 3 with gridder_threads 512);
+    int gridder;               /* 0: default (7, or 3 with gridder_threads 512);
                                   3: k_grid3 (block-wide staging of each work item);
                                   5: k_grid5 (two item buffers refilled by one warp, no
                                   block barriers; items of at most 256 records);
                                   7: k_grid7 (every warp streams its own jobs -- one work
                                   item against 128 slots of its support box -- with no
-                                  block barriers; items of at most 512 records).  A gridder
-                                  that could not complete sets the normaliser to NaN      */
+                                  block barriers; items of at most 512 records);
+                                  8: k_grid7 with 256 slots per job (8 per lane: twice
+                                  the packed FMAs per record handled, 12 warps per SM).
+                                  A gridder that could not complete sets the normaliser
+                                  to NaN                                                   */
     int flags_u8;              /* 0: d_flags is int32 [R][P] (the reference's layout); 1: it
                                   is one byte per flag, uint8 [R][P] (0 = keep, non-zero = flagged;
                                   a quarter of the bytes to move), passed cast to int *    */
@@ -277,16 +280,16 @@ typedef struct mtb_grid_tuning {
 
 /* Autotuner.  No counterpart in the reference, whose gridder launch shapes are
  * fixed.  Grids the jobs (as mtb_grid_batch) once with every candidate of
- * tile {16, 32, 64} x support_bucket {1, 2} x seven gridder shapes (gridder 3
+ * tile {16, 32, 64} x support_bucket {1, 2} x nine gridder shapes (gridder 3
  * with max_chunk {256, 512} x gridder_threads {256, 512}, gridder 5 with
- * 256-record items, gridder 7 with max_chunk {256, 512}; 256 threads unless
- * stated), times each call with CUDA events on
+ * 256-record items, gridders 7 and 8 with max_chunk {256, 512}; 256 threads
+ * unless stated), times each call with CUDA events on
  * `stream` (after one untimed call), and writes the fastest to *best and to
  * every job's params.  Every job must start a fresh image (initialize_output
  * = 1): the grids, normalisers and statistics hold the result of a call with
  * the chosen knobs when it returns.  Synchronises `stream` after every call.
  * `candidates` (may be NULL) receives all mtb_grid_autotune_candidate_count()
- * timings (42).  Workspace: mtb_grid_autotune_workspace_size. */
+ * timings (54).  Workspace: mtb_grid_autotune_workspace_size. */
 int mtb_grid_autotune_candidate_count(void);
 int mtb_grid_autotune_workspace_size(const mtb_grid_job *jobs, int njobs, size_t *bytes);
 int mtb_grid_autotune(mtb_grid_job *jobs, int njobs, void *d_workspace, size_t workspace_bytes,

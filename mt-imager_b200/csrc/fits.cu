@@ -111,6 +111,9 @@ extern "C" int mtb_fits_create(const char *path, const mtb_fits_header *h, mtb_f
     cards.push_back(card("LATPOLE", num(h->dec_deg)));
     if (h->telescope) cards.push_back(card("TELESCOP", str(h->telescope)));
     if (h->observer) cards.push_back(card("OBSERVER", str(h->observer)));
+    // ObsInfo's pointing centre is the phase centre (ImageManager.cpp:100)
+    cards.push_back(card("OBSRA", num(h->ra_deg)));
+    cards.push_back(card("OBSDEC", num(h->dec_deg)));
     if (h->obs_mjd > 0) cards.push_back(card("DATE-OBS", str(iso_date(h->obs_mjd))));
     const double now_mjd = (double)std::time(nullptr) / 86400.0 + 40587.0;
     cards.push_back(card("DATE", str(iso_date(now_mjd)), "Date FITS file was written"));

@@ -1141,15 +1141,28 @@ __global__ void __launch_bounds__(kG3Threads, 2) k_grid5(Grid2Args a, int *err) 
 //
 // Jobs are ordered by segment (image, support bucket), largest support
 // first, so the longest jobs are handed out first.
-static const int kG7Warps = 8;
-static const int kG7Threads = 32 * kG7Warps;
-static const int kG7KS = 4;                        // slots per lane
-static const int kG7Depth = 4;                     // taps fetched this many records ahead
-static const int kG7RecRing = 16;                  // record-ring entries (records fetched 2 * kG7Depth ahead)
-static const int kG7PartSlots = 32 * kG7KS;        // slots of one job
-static const int kG7Chunk = 512;                   // records of one work item
-static const int kG7TapStride = kG7Depth * kG7KS * 32;   // tap-ring / FIFO entries per warp
-static_assert(kG7RecRing >= 2 * kG7Depth + 1, "the record ring holds every record in flight");
+//
+// Two shapes (G7Cfg): gridder 7, 4 slots per lane (128 per job), taps 4
+// records ahead, 8-warp blocks, 2 per SM; gridder 8, 8 slots per lane (256 per
+// job: twice the packed FMAs per record for the same record handling), taps 2
+// records ahead, 4-warp blocks, 3 per SM (the doubled accumulators cost
+// registers; the smaller rings keep 12 warps' within the SM's shared memory).
+template <int KS_, int D_, int WARPS_, int MINB_>
+struct G7Cfg {
+    static constexpr int KS = KS_;                       // slots per lane
+    static constexpr int D = D_;                         // taps fetched this many records ahead
+    static constexpr int Warps = WARPS_;                 // warps per block
+    static constexpr int Threads = 32 * WARPS_;
+    static constexpr int MinBlocks = MINB_;              // blocks per SM the registers are capped for
+    static constexpr int RR = 2 * D_ + 1 <= 8 ? 8 : 16;  // record-ring entries (records fetched 2D ahead)
+    static constexpr int PartSlots = 32 * KS_;           // slots of one job
+    static constexpr int TapStride = D_ * KS_ * 32;      // tap-ring / FIFO entries per warp
+    static_assert(RR >= 2 * D_ + 1, "the record ring holds every record in flight");
+    static_assert((D_ & (D_ - 1)) == 0, "ring indices are masked");
+};
+using G7Narrow = G7Cfg<4, 4, 8, 2>;    // gridder 7
+using G7Wide = G7Cfg<8, 2, 4, 3>;      // gridder 8
+static const int kG7Chunk = 512;       // records of one work item
 
 // Jobs [job0, next.job0) are items [item0, item0 + n) x wu parts of modulus m.
 struct G7Segment {
@@ -1175,7 +1188,8 @@ struct G7SegSrc {
 // One block of kMaxBuckets threads: the segments of every image in image
 // order (the order of the concatenated item list), buckets by descending
 // modulus within an image.
-__global__ void k_g7_segments(G7SegSrc src, int nimages, G7Segment *__restrict__ segs, int *__restrict__ n_segs) {
+__global__ void k_g7_segments(G7SegSrc src, int nimages, int part_slots, G7Segment *__restrict__ segs,
+                              int *__restrict__ n_segs) {
     using Scan = cub::BlockScan<int, kMaxBuckets>;
     __shared__ typename Scan::TempStorage tmp;
     __shared__ int s_nseg, s_job0, s_base;
@@ -1192,7 +1206,7 @@ __global__ void k_g7_segments(G7SegSrc src, int nimages, G7Segment *__restrict__
             m = src.M[j][bb];
             if (m <= 0 || cnt <= 0) cnt = 0;
         }
-        const int wu = cnt ? (m * m + kG7PartSlots - 1) / kG7PartSlots : 0;
+        const int wu = cnt ? (m * m + part_slots - 1) / part_slots : 0;
         int idx, njob, aggr_seg, aggr_job;
         Scan(tmp).ExclusiveSum(cnt ? 1 : 0, idx, aggr_seg);
         __syncthreads();
@@ -1276,10 +1290,10 @@ __global__ void k_mark_runs(const int4 *__restrict__ items, const int *__restric
 // changes) and the record whose fetch opens a run on the look-ahead side (new
 // table offsets).  Between those points the loop holds no branch and no
 // conditional update of the accumulators.
-template <int P, bool UNIFORM, bool EXACT>
+template <class C, int P, bool UNIFORM, bool EXACT>
 __device__ __forceinline__ void grid_job7(const GridJobDesc &J, const int first, const int N, const int M,
                                           const int part, float4 *tring, int *fifo, float4 *rring) {
-    constexpr int KS = kG7KS, D = kG7Depth, RR = kG7RecRing, E = 1 + P;
+    constexpr int KS = C::KS, D = C::D, RR = C::RR, E = 1 + P;
     const int lane = threadIdx.x & 31;
     const float4 *const tab = J.table2;
     float *const ggrid = EXACT ? nullptr : J.grid;
@@ -1291,7 +1305,7 @@ __device__ __forceinline__ void grid_job7(const GridJobDesc &J, const int first,
     int nb[KS];                  // copy size of each slot's tap: 16, or 0 outside the box
 #pragma unroll
     for (int j = 0; j < KS; j++) {
-        const int q = part * kG7PartSlots + j * 32 + lane;
+        const int q = part * C::PartSlots + j * 32 + lane;
         const int b = q / M;
         qa[j] = q - b * M;
         qb[j] = q < MM ? b : -1;
@@ -1459,15 +1473,14 @@ __device__ __forceinline__ void grid_job7(const GridJobDesc &J, const int first,
         if (last[j] >= 0) flush2<P>(ggrid, gdelta, last[j], acc[j]);
 }
 
-template <int P, bool UNIFORM, bool EXACT>
-__global__ void __launch_bounds__(kG7Threads, 2) k_grid7(Grid7Args a) {
-    constexpr int E = 1 + P;
+template <class C, int P, bool UNIFORM, bool EXACT>
+__global__ void __launch_bounds__(C::Threads, C::MinBlocks) k_grid7(Grid7Args a) {
+    constexpr int E = 1 + P, TS = C::TapStride;
     extern __shared__ float4 smem7[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    float4 *const tring = smem7 + warp * kG7TapStride + lane;                                  // [warp][D][KS][32]
-    int *const fifo = (int *)(smem7 + kG7Warps * kG7TapStride) + warp * kG7TapStride + lane;    // [warp][D][KS][32]
-    float4 *const rring = smem7 + kG7Warps * kG7TapStride + kG7Warps * kG7TapStride / 4 +
-                          warp * kG7RecRing * E;                                                // [warp][RR][E]
+    float4 *const tring = smem7 + warp * TS + lane;                                  // [warp][D][KS][32]
+    int *const fifo = (int *)(smem7 + C::Warps * TS) + warp * TS + lane;             // [warp][D][KS][32]
+    float4 *const rring = smem7 + C::Warps * TS + C::Warps * TS / 4 + warp * C::RR * E;   // [warp][RR][E]
     const int nsegs = *a.n_segs;
     const int total = a.segs[nsegs].job0;
     int seg = 0;
@@ -1481,31 +1494,39 @@ __global__ void __launch_bounds__(kG7Threads, 2) k_grid7(Grid7Args a) {
         const int rel = t - g.job0;
         const int k = rel / g.wu;
         const int4 it = a.items[g.item0 + k];
-        grid_job7<P, UNIFORM, EXACT>(a.jobs[it.w], it.x, it.y, g.m, rel - k * g.wu, tring, fifo, rring);
+        grid_job7<C, P, UNIFORM, EXACT>(a.jobs[it.w], it.x, it.y, g.m, rel - k * g.wu, tring, fifo, rring);
     }
 }
 
-template <int P>
+template <class C, int P>
 static size_t grid7_smem() {
-    return (size_t)kG7Warps * (kG7TapStride * (sizeof(float4) + sizeof(int)) + kG7RecRing * (1 + P) * sizeof(float4));
+    return (size_t)C::Warps * (C::TapStride * (sizeof(float4) + sizeof(int)) + C::RR * (1 + P) * sizeof(float4));
 }
 
 // UNIFORM kernel when every image of the launch has one support per bucket
-template <int P>
-static int launch_grid7(const Grid7Args &a, cudaStream_t st) {
+template <class C, int P>
+static int launch_grid7c(const Grid7Args &a, cudaStream_t st) {
     bool uniform = true;
     for (int j = 0; j < kMaxBatch && a.jobs[j].wpos; j++) uniform = uniform && a.jobs[j].uniform;
     const bool exact = a.jobs[0].dgrid != nullptr;
-    auto kern = uniform ? (exact ? k_grid7<P, true, true> : k_grid7<P, true, false>)
-                        : (exact ? k_grid7<P, false, true> : k_grid7<P, false, false>);
-    const size_t smem = grid7_smem<P>();
+    auto kern = uniform ? (exact ? k_grid7<C, P, true, true> : k_grid7<C, P, true, false>)
+                        : (exact ? k_grid7<C, P, false, true> : k_grid7<C, P, false, false>);
+    const size_t smem = grid7_smem<C, P>();
     MTB_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
-    MTB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kG7Threads, smem));
+    MTB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, C::Threads, smem));
     if (per_sm < 1) return MTB_ERR_BAD_SHAPE;
-    kern<<<per_sm * sm_count(), kG7Threads, smem, st>>>(a);
+    kern<<<per_sm * sm_count(), C::Threads, smem, st>>>(a);
     MTB_LAUNCHED();
     return MTB_OK;
+}
+
+// Slots of one job of the streaming gridder `which` (7 or 8).
+static int g7_part_slots(int which) { return which == 8 ? G7Wide::PartSlots : G7Narrow::PartSlots; }
+
+template <int P>
+static int launch_grid7(const Grid7Args &a, int which, cudaStream_t st) {
+    return which == 8 ? launch_grid7c<G7Wide, P>(a, st) : launch_grid7c<G7Narrow, P>(a, st);
 }
 
 template <int P>
@@ -1698,6 +1719,9 @@ static int gridder_of(const mtb_grid_params *p) {
     return 7;
 }
 
+// The per-warp streaming gridders (k_grid7 in its two shapes).
+static bool streaming(int which) { return which == 7 || which == 8; }
+
 // Work items shorter than this many records multiply the flushes into each
 // cell: with the FP32 per-call delta grid, 37-record items took the first
 // configuration's image error to 1.2e-5 of its peak (above the 1e-5 bound),
@@ -1731,7 +1755,7 @@ static int effective_chunk(const mtb_grid_params *p) {
     int c = p->max_chunk > 0 ? p->max_chunk : kDefaultChunk;
     if (p->merge != 1 && c > kG3Chunk) c = kG3Chunk;
     if (p->merge != 1 && gridder_of(p) == 5 && c > kG5Chunk) c = kG5Chunk;
-    if (p->merge != 1 && gridder_of(p) == 7 && c > kG7Chunk) c = kG7Chunk;
+    if (p->merge != 1 && streaming(gridder_of(p)) && c > kG7Chunk) c = kG7Chunk;
     return c;
 }
 
@@ -1745,8 +1769,8 @@ static int check_params(const mtb_grid_params *p) {
     if (p->merge < 0 || p->merge > 2) return MTB_ERR_BAD_PARAM;
     if (p->bulk_min_support != 0) return MTB_ERR_BAD_PARAM;   // reserved (no bulk-copy gridder)
     if (p->gridder_threads != 0 && p->gridder_threads != 256 && p->gridder_threads != 512) return MTB_ERR_BAD_PARAM;
-    if (p->gridder != 0 && p->gridder != 3 && p->gridder != 5 && p->gridder != 7) return MTB_ERR_BAD_PARAM;
-    if ((p->gridder == 5 || p->gridder == 7) && p->gridder_threads == 512) return MTB_ERR_BAD_PARAM;
+    if (p->gridder != 0 && p->gridder != 3 && p->gridder != 5 && !streaming(p->gridder)) return MTB_ERR_BAD_PARAM;
+    if ((p->gridder == 5 || streaming(p->gridder)) && p->gridder_threads == 512) return MTB_ERR_BAD_PARAM;
     return MTB_OK;
 }
 
@@ -1915,7 +1939,7 @@ static int prepare_grid(const mtb_grid_params *p, const GridPlan &plan, const fl
     MTB_LAUNCHED();
     launch_gather<P, true>(p, blocks, st, R, s, vis, weights, flags, plan, conv_info, s.pbase, p->wplanes);
     MTB_LAUNCHED();
-    if (gridder_of(p) == 7) {
+    if (streaming(gridder_of(p))) {
         // one warp per work item; the item count is on the device: cover the
         // largest count this chunk can have and let the kernel read the rest
         const int wb = std::min((R / 8 + 7) / 8 + 1, sms * 16);
@@ -2037,13 +2061,13 @@ static int run_grid(const mtb_grid_params *p, const GridPlan &plan, const float2
     g2.jobs[0] = job_desc<P>(p, grid, grid_lo != nullptr, s);
     const int which = gridder_of(p);
     const bool rolling = which == 5;
-    if (which == 7) {
+    if (streaming(which)) {
         G7SegSrc src;
         std::memset(&src, 0, sizeof(src));
         src.bounds[0] = s.bounds;
         src.n_items[0] = s.n_items;
         src.M[0] = s.moduli;
-        k_g7_segments<<<1, kMaxBuckets, 0, st>>>(src, 1, s.segs, s.n_segs);
+        k_g7_segments<<<1, kMaxBuckets, 0, st>>>(src, 1, g7_part_slots(which), s.segs, s.n_segs);
         MTB_LAUNCHED();
         MTB_CUDA_TRY(cudaMemsetAsync(s.counter7, 0, sizeof(int), st));
         Grid7Args g7;
@@ -2053,7 +2077,7 @@ static int run_grid(const mtb_grid_params *p, const GridPlan &plan, const float2
         g7.n_segs = s.n_segs;
         g7.counter = s.counter7;
         g7.jobs[0] = g2.jobs[0];
-        MTB_TRY(launch_grid7<P>(g7, st));
+        MTB_TRY(launch_grid7<P>(g7, which, st));
     } else if (which == 5) {
         MTB_TRY(launch_grid5<P>(g2, s.err, st));
     } else {
@@ -2278,7 +2302,8 @@ static int run_batch(const mtb_grid_job *jobs, int njobs, const GridPlan *plans,
     g2.counter = counter;
     // the batch's gridder error flag (read by every image's k_finish)
     MTB_CUDA_TRY(cudaMemsetAsync(spaces[0].err, 0, sizeof(int), st));
-    if (gridder_of(&p0) == 7) {
+    const int which = gridder_of(&p0);
+    if (streaming(which)) {
         G7SegSrc src;
         std::memset(&src, 0, sizeof(src));
         for (int j = 0; j < njobs; j++) {
@@ -2286,7 +2311,7 @@ static int run_batch(const mtb_grid_job *jobs, int njobs, const GridPlan *plans,
             src.n_items[j] = jobs[j].nrecords > 0 ? spaces[j].n_items : nullptr;
             src.M[j] = spaces[j].moduli;
         }
-        k_g7_segments<<<1, kMaxBuckets, 0, st>>>(src, njobs, segs, spaces[0].n_segs);
+        k_g7_segments<<<1, kMaxBuckets, 0, st>>>(src, njobs, g7_part_slots(which), segs, spaces[0].n_segs);
         MTB_LAUNCHED();
         MTB_CUDA_TRY(cudaMemsetAsync(spaces[0].counter7, 0, sizeof(int), st));
         Grid7Args g7;
@@ -2296,7 +2321,7 @@ static int run_batch(const mtb_grid_job *jobs, int njobs, const GridPlan *plans,
         g7.n_segs = spaces[0].n_segs;
         g7.counter = spaces[0].counter7;
         for (int j = 0; j < njobs; j++) g7.jobs[j] = g2.jobs[j];
-        MTB_TRY(launch_grid7<P>(g7, st));
+        MTB_TRY(launch_grid7<P>(g7, which, st));
     } else if (gridder_of(&p0) == 5) {
         MTB_TRY(launch_grid5<P>(g2, spaces[0].err, st));
         if (check_gridder() && !capturing(st)) {

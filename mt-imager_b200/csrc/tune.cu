@@ -15,10 +15,11 @@ const int kTiles[] = {16, 32, 64};
 const int kBuckets[] = {1, 2};
 // (gridder, records per work item, block size): the block-staged gridder at
 // two item lengths and two block sizes, the rolling-items gridder (items of at
-// most 256 records, 256 threads), the streaming gridder at two item lengths
+// most 256 records, 256 threads), the streaming gridder in both shapes (128
+// and 256 slots per job; its block size is fixed) at two item lengths
 const int kShapes[][3] = {{3, 256, 256}, {3, 256, 512}, {3, 512, 256}, {3, 512, 512},
-                          {5, 256, 256}, {7, 256, 256}, {7, 512, 256}};
-const int kNShapes = 7;
+                          {5, 256, 256}, {7, 256, 256}, {7, 512, 256}, {8, 256, 256}, {8, 512, 256}};
+const int kNShapes = 9;
 const int kCandidates = 3 * 2 * kNShapes;
 
 mtb_grid_tuning candidate(int c) {

@@ -167,6 +167,7 @@ def _valid_grid_params():
     ("merge", 3, L.MTB_ERR_BAD_PARAM),
     ("gridder_threads", 384, L.MTB_ERR_BAD_PARAM),
     ("gridder", 4, L.MTB_ERR_BAD_PARAM),
+    ("gridder", 9, L.MTB_ERR_BAD_PARAM),
     ("bulk_min_support", 17, L.MTB_ERR_BAD_PARAM),   # reserved: the bulk-copy gridder was removed
     ("max_chunk", -1, L.MTB_ERR_BAD_PARAM),
 ])
@@ -190,7 +191,7 @@ def test_grid_refuses_negative_records_and_rolling_512(mtblib):
     p = _valid_grid_params()
     assert mtblib.mtb_grid_workspace_size(ctypes.byref(p), ctypes.cast(info, ctypes.c_void_p), -1,
                                           ctypes.byref(n)) == L.MTB_ERR_BAD_SHAPE
-    for g in (5, 7):                          # the rolling and streaming gridders run 256-thread blocks only
+    for g in (5, 7, 8):                       # the rolling and streaming gridders take no block size
         p.gridder, p.gridder_threads = g, 512
         assert mtblib.mtb_grid_workspace_size(ctypes.byref(p), ctypes.cast(info, ctypes.c_void_p), 10,
                                               ctypes.byref(n)) == L.MTB_ERR_BAD_PARAM

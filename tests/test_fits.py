@@ -65,3 +65,48 @@ def test_fits_single_stokes(tmp_path):
     cards, data = read_fits(path)
     assert int(cards["NAXIS3"]) == 1 and int(cards["NAXIS4"]) == 1
     assert np.array_equal(data[0], img)
+
+
+def test_fits_header_matches_expected_cards(tmp_path):
+    """Every card of tests/golden/fits_header_iv_nonuniform.json: the header
+    the reference's ImageManager::createFITS writes (ImageManager.cpp:68-108,
+    132-188) for two circular polarisations (Stokes I, V) and a non-uniform
+    channel list, restated card by card.  Numbers to 1e-12 relative."""
+    import json
+    import os
+    fx = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "fits_header_iv_nonuniform.json")))
+    i = fx["input"]
+    arcsec = math.pi / (180 * 3600)
+    path = tmp_path / "iv.fits"
+    imgs = np.random.default_rng(1).standard_normal((len(i["freqs_hz"]), 2, i["ny"], i["nx"])).astype(np.float32)
+    with FitsCube(path, i["nx"], i["ny"], i["freqs_hz"], i["l_increment_arcsec"] * arcsec,
+                  m_increment=i["m_increment_arcsec"] * arcsec, stokes=i["stokes"], ra_deg=i["ra_deg"],
+                  dec_deg=i["dec_deg"], telescope=i["telescope"], observer=i["observer"],
+                  obs_mjd=i["obs_mjd"]) as f:
+        for c in range(len(i["freqs_hz"])):
+            f.write(c, imgs[c])
+    cards, data = read_fits(path)
+    for key, want in fx["cards"].items():
+        assert key in cards, key
+        v = want["value"]
+        if isinstance(v, str):
+            assert cards[key] == v, (key, cards[key], v)
+        else:
+            assert math.isclose(float(cards[key]), float(v), rel_tol=1e-12, abs_tol=1e-300), (key, cards[key], v)
+    for key in fx["present"]:
+        assert key in cards, key
+    # channel planes in list order, each [Stokes][m][l]
+    assert data.shape == (4, 2, i["ny"], i["nx"]) and np.array_equal(data, imgs)
+
+
+def test_fits_stokes_axis_codes(tmp_path):
+    """The Stokes axis is linear in the FITS codes of the list
+    ConfigurationManager.cpp:137-154 builds: I (1 pol), I Q (2 linear),
+    I V (2 circular), I Q U V (4)."""
+    for stokes, crval, cdelt in (("I", 1, 1), ("IQ", 1, 1), ("IV", 1, 3), ("IQUV", 1, 1)):
+        path = tmp_path / ("s_%s.fits" % stokes)
+        with FitsCube(path, 4, 4, [1.4e9], 1e-5, stokes=stokes) as f:
+            f.write(0, np.zeros((len(stokes), 4, 4), np.float32))
+        cards, _ = read_fits(path)
+        assert int(cards["NAXIS3"]) == len(stokes)
+        assert float(cards["CRVAL3"]) == crval and float(cards["CDELT3"]) == cdelt

@@ -168,7 +168,9 @@ def test_chunked_equals_single(cfg1):
                                     dict(gridder=5), dict(gridder=5, tile=64),
                                     dict(gridder=7), dict(gridder=7, tile=64), dict(gridder=7, tile=16),
                                     dict(gridder=7, support_bucket=3), dict(gridder=7, exact_delta=True),
-                                    dict(gridder=7, max_chunk=37, exact_delta=True)])
+                                    dict(gridder=7, max_chunk=37, exact_delta=True),
+                                    dict(gridder=8), dict(gridder=8, tile=16), dict(gridder=8, support_bucket=3),
+                                    dict(gridder=8, exact_delta=True), dict(gridder=8, max_chunk=37, exact_delta=True)])
 def test_tuning_does_not_change_result(cfg1, tuning):
     obs, setup, geo, kern, img_o, grid_o, norm_o = cfg1
     im, img = run_gpu(obs, setup, **tuning)
@@ -178,13 +180,14 @@ def test_tuning_does_not_change_result(cfg1, tuning):
 
 
 @pytest.mark.parametrize("kw", [dict(), dict(tile=64), dict(nx=320, s=3), dict(merge=1), dict(gridder=5),
-                                dict(gridder=7), dict(nx=320, s=3, gridder=7),
+                                dict(gridder=7), dict(nx=320, s=3, gridder=7), dict(gridder=8),
+                                dict(nx=320, s=3, gridder=8),
                                 ])
 def test_large_supports(oracle, kw):
     """Supports up to 55 (and 105 with odd sampling): the direct gridders
-    (block-staged, rolling-items and bulk-copy; one and several record
-    streams), the shared-memory window variant, and support bands split across
-    blocks."""
+    (block-staged, rolling-items, streaming with 4 and 8 slots per lane; one
+    and several record streams), the shared-memory window variant, and
+    support bands split across blocks."""
     tile = kw.pop("tile", 0)
     merge = kw.pop("merge", 0)
     gridder = kw.pop("gridder", 0)
@@ -283,3 +286,28 @@ def test_status_codes(oracle):
                       _ptr(torch.zeros((R, 4), device="cuda")), _ptr(torch.zeros((R, 4), dtype=torch.int32, device="cuda")),
                       R, _ptr(im2.grid), None, _ptr(im2.normalizer), None, _ptr(ws), 16, _stream())
     assert st == 3   # workspace too small
+
+
+@pytest.mark.parametrize("ny,gridder", [(96, 0), (160, 0), (160, 8), (96, 3)])
+def test_rectangular_image_parity(oracle, ny, gridder):
+    """nx != ny (ConfigurationManager.cpp:170-202 sizes the axes
+    independently): Δv = 1/(Δm·ny), rows of the grid and image indexed by ny
+    and columns by nx in the preprocessing, the gridders, the inverse FFT, the
+    Stokes conversion and the taper and sinc corrections.  Grid and every
+    Stokes plane against the FP64 oracle, statistics exact."""
+    import dataclasses
+    obs, setup = synth.small_config(seed=3, n_ant=10, ntimes=60, nx=128, cell_arcsec=20, flag_frac=0.1)
+    setup = dataclasses.replace(setup, ny=ny)
+    geo = oracle.geometry_for(setup)
+    kern = oracle.wkernels(geo)
+    img_o, grid_o, norm_o = oracle.image_channel(obs, 0, setup, kern, geo)
+    im, img = run_gpu(obs, setup, gridder=gridder)
+    assert img.shape == img_o.shape == (4, ny, 128)
+    g = im.grid_sum().cpu().numpy()
+    assert g.shape == grid_o.shape
+    assert np.abs(g - grid_o).max() <= GRID_TOL * np.abs(grid_o).max()
+    peak = np.abs(img_o[0]).max()
+    for p in range(4):
+        assert np.sqrt(np.mean((img[p] - img_o[p]) ** 2)) <= IMAGE_RMS_TOL * peak, p
+    st = oracle.stats(oracle.preprocess(obs.uvw, obs.freq_over_c(0), obs.weights[0], obs.flags[0], geo, kern))
+    assert im.statistics() == st

@@ -80,3 +80,17 @@ def test_noalloc_refuses_more_than_capacity():
                                            d, d, d, cap + 1, d, d, d, d, d, d, d, _stream())
     assert rc == L.MTB_ERR_TOO_LARGE
     assert b"capacity" in im.lib.mtb_status_string(rc)
+
+
+def test_noalloc_matches_oracle(oracle):
+    """The no-alloc entry point against the FP64 oracle directly: the six
+    integer outputs bit for bit, ConvSums·weight to 1e-6 of its peak."""
+    obs, setup = wide_case(nx=320, cell=150, s=3, seed=11)
+    geo = oracle.geometry_for(setup)
+    kern = oracle.wkernels(geo)
+    im = imager_for(setup)
+    got = preprocess_noalloc(im, obs)
+    pre = oracle.preprocess(obs.uvw, obs.freq_over_c(0), obs.weights[0], obs.flags[0], geo, kern)
+    for key in KEYS:
+        assert np.array_equal(got[key], pre[key]), key
+    assert np.abs(got["convsum"] - pre["convsum"]).max() <= CONVSUM_TOL * np.abs(pre["convsum"]).max()
