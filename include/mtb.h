@@ -67,7 +67,8 @@ enum {
     MTB_ERR_CUFFT = 6,         /* FFTException                                       */
     MTB_ERR_KERNEL = 7,        /* ImagerException: w=0 origin not real / no support  */
     MTB_ERR_NULL = 8,          /* a required pointer is NULL                         */
-    MTB_ERR_TOO_LARGE = 9      /* request exceeds a fixed-size entry point's capacity */
+    MTB_ERR_TOO_LARGE = 9,     /* request exceeds a fixed-size entry point's capacity */
+    MTB_ERR_CANCELLED = 10     /* an engine request cancelled before it completed    */
 };
 
 /* ------------------------------------------------------------ w-kernels -- */

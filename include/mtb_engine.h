@@ -75,6 +75,13 @@ int mtb_engine_create(const mtb_engine_config *cfg, mtb_engine **engine);
 int mtb_engine_submit(mtb_engine *engine, const mtb_image_request *req, long long *ticket);
 /* Blocks until the request is done and returns its result (once per ticket). */
 int mtb_engine_wait(mtb_engine *engine, long long ticket, mtb_image_result *result);
+/* Cancels a request that has not completed: a queued request is dropped at
+ * once; a running one stops at its next chunk boundary (the work already
+ * enqueued on its stream completes first) and skips the finalisation.  Its
+ * result, from mtb_engine_wait, carries MTB_ERR_CANCELLED and its image is
+ * undefined; a request that had already completed keeps its result.
+ * Unknown (or already waited-for) tickets return MTB_ERR_BAD_PARAM. */
+int mtb_engine_cancel(mtb_engine *engine, long long ticket);
 /* Device bytes a request is admitted with. */
 int mtb_engine_request_bytes(const mtb_engine *engine, const mtb_image_request *req, size_t *bytes);
 /* Finishes the queued requests, stops the workers and frees everything. */

@@ -19,6 +19,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cstdint>
 #include <condition_variable>
@@ -35,6 +36,7 @@
 
 #include "mtb.hpp"
 #include "mtb_engine.h"
+#include "mtb_internal.cuh"
 
 namespace mtb {
 namespace {
@@ -126,8 +128,12 @@ struct Job {
     size_t bytes = 0;
     Clock::time_point t_submit, t_admit, t_done;
     bool done = false;
+    std::atomic<bool> cancel{false};    // set by mtb_engine_cancel, read between chunks
     mtb_image_result res{};
 };
+
+// A running request's cancellation, seen at a chunk boundary.
+struct Cancelled {};
 
 // w-kernel tables by geometry, least recently used evicted beyond `cap` bytes.
 // A table in use by a request stays alive (shared_ptr) after eviction.
@@ -344,6 +350,7 @@ void mtb_engine::worker(int slot) {
 }
 
 void mtb_engine::run(mtb::Job *j, Slot &sl) {
+    MTB_RANGE("mtb_engine_request");
     const mtb_image_request &r = j->req;
     const int P = r.npol, R = r.nrecords;
     cudaStream_t st = sl.st;
@@ -356,6 +363,7 @@ void mtb_engine::run(mtb::Job *j, Slot &sl) {
         const int chunk = cfg.chunk_records;
         int b = 0;
         for (int c0 = 0; c0 < R; c0 += chunk, b ^= 1) {
+            if (j->cancel.load()) throw mtb::Cancelled();
             const int n = std::min(chunk, R - c0);
             // staging b is free once the copy issued from it two chunks ago is done
             mtb::cuda_check(cudaEventSynchronize(sl.ev[b]), "staging");
@@ -378,6 +386,7 @@ void mtb_engine::run(mtb::Job *j, Slot &sl) {
                     (const int *)(d + off_fl), n);
         }
         if (R == 0) im.grid(nullptr, nullptr, nullptr, nullptr, nullptr, 0);
+        if (j->cancel.load()) throw mtb::Cancelled();
         const size_t npix = (size_t)P * r.geometry.nx * r.geometry.ny;
         mtb::ImagerBuffers::ensure(sl.img, npix, st);
         im.finalize(sl.img.data());
@@ -399,6 +408,9 @@ void mtb_engine::run(mtb::Job *j, Slot &sl) {
         }
         j->res.stats = im.stats();   // synchronises the stream
         j->res.status = MTB_OK;
+    } catch (const mtb::Cancelled &) {
+        j->res.status = MTB_ERR_CANCELLED;
+        cudaStreamSynchronize(st);    // the chunks already enqueued finish before the slot is reused
     } catch (const mtb::Error &e) {
         j->res.status = e.status;
         cudaStreamSynchronize(st);
@@ -474,6 +486,28 @@ extern "C" int mtb_engine_submit(mtb_engine *engine, const mtb_image_request *re
         *ticket = j->ticket;
     }
     engine->cv.notify_all();
+    return MTB_OK;
+}
+
+extern "C" int mtb_engine_cancel(mtb_engine *engine, long long ticket) {
+    if (!engine) return MTB_ERR_NULL;
+    {
+        std::lock_guard<std::mutex> lk(engine->m);
+        auto it = engine->jobs.find(ticket);
+        if (it == engine->jobs.end()) return MTB_ERR_BAD_PARAM;
+        mtb::Job *j = it->second;
+        if (j->done) return MTB_OK;
+        j->cancel.store(true);
+        auto q = std::find(engine->queue.begin(), engine->queue.end(), j);
+        if (q == engine->queue.end()) return MTB_OK;    // running: its worker stops at a chunk boundary
+        engine->queue.erase(q);
+        j->t_admit = j->t_done = mtb::Clock::now();
+        j->res.status = MTB_ERR_CANCELLED;
+        j->res.queue_ms = j->res.latency_ms = mtb::ms_between(j->t_submit, j->t_done);
+        j->res.service_ms = 0.0;
+        j->done = true;
+    }
+    engine->cv.notify_all();    // waiters of this ticket, and workers whose queue head changed
     return MTB_OK;
 }
 

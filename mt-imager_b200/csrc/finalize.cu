@@ -152,6 +152,7 @@ extern "C" int mtb_finalize_planes_bytes(const mtb_finalize_params *p, size_t *b
 extern "C" int mtb_finalize(const mtb_finalize_params *p, const void *d_grid, const void *d_grid_lo,
                             const float *d_normalizer, float *d_image, void *d_workspace, size_t workspace_bytes,
                             mtb_stream_t stream) {
+    MTB_RANGE("mtb_finalize");
     MTB_TRY(check_fin(p));
     if (!d_grid || !d_normalizer || !d_image || !d_workspace) return MTB_ERR_NULL;
     if (p->external_planes && !p->d_planes) return MTB_ERR_NULL;

@@ -2146,6 +2146,7 @@ extern "C" int mtb_grid(const mtb_grid_params *p, const void *d_table, const int
                         int nrecords, void *d_grid, void *d_grid_lo, float *d_normalizer,
                         mtb_grid_stats *d_stats, void *d_workspace, size_t workspace_bytes,
                         mtb_stream_t stream) {
+    MTB_RANGE("mtb_grid");
     MTB_TRY(check_params(p));
     if (nrecords < 0) return MTB_ERR_BAD_SHAPE;
     if (!d_grid || !d_normalizer || !h_conv_info) return MTB_ERR_NULL;
@@ -2345,6 +2346,7 @@ static int run_batch(const mtb_grid_job *jobs, int njobs, const GridPlan *plans,
 
 extern "C" int mtb_grid_batch(const mtb_grid_job *jobs, int njobs, void *d_workspace, size_t workspace_bytes,
                               mtb_stream_t stream) {
+    MTB_RANGE("mtb_grid_batch");
     MTB_TRY(check_batch(jobs, njobs));
     cudaStream_t st = (cudaStream_t)stream;
     for (int j = 0; j < njobs; j++) {
@@ -2387,6 +2389,7 @@ extern "C" int mtb_preprocess_uvw(const mtb_grid_params *p, const int *d_conv_in
                                   int *d_conv_index, int *d_to_grid, int *d_to_compress, int *d_support,
                                   float *d_take_conjugate, float *d_conv_sum, void *d_workspace,
                                   size_t workspace_bytes, mtb_stream_t stream) {
+    MTB_RANGE("mtb_preprocess_uvw");
     MTB_TRY(check_params(p));
     if (nrecords < 0) return MTB_ERR_BAD_SHAPE;
     if (nrecords == 0) return MTB_OK;
@@ -2467,6 +2470,7 @@ extern "C" int mtb_preprocess_uvw_noalloc(const mtb_grid_params *p, const int *d
                                           int *d_gridding_data, int *d_conv_index, int *d_to_grid,
                                           int *d_to_compress, int *d_support, float *d_take_conjugate,
                                           float *d_conv_sum, mtb_stream_t stream) {
+    MTB_RANGE("mtb_preprocess_uvw_noalloc");
     MTB_TRY(check_params(p));
     if (nrecords < 0) return MTB_ERR_BAD_SHAPE;
     if (nrecords > kNoAllocMaxRecords) return MTB_ERR_TOO_LARGE;

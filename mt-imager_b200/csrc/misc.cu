@@ -24,6 +24,7 @@ extern "C" const char *mtb_status_string(int status) {
         case MTB_ERR_KERNEL: return "w-kernel generation failed (origin not real or no support)";
         case MTB_ERR_NULL: return "required pointer is NULL";
         case MTB_ERR_TOO_LARGE: return "request exceeds the entry point's fixed scratch capacity";
+        case MTB_ERR_CANCELLED: return "request cancelled";
         default: return "unknown status";
     }
 }

@@ -1,11 +1,24 @@
 // Internal helpers shared by the sm_100a kernels of the W-projection path.
 #pragma once
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 #include <cstddef>
 #include <cstdint>
 #include "mtb.h"
 
 namespace mtb {
+
+// NVTX range over one entry point's host scope, named after the entry point:
+// profilers attribute the kernels it launches to it (ncu --nvtx
+// --nvtx-include "mtb_grid/").  Header-only NVTX: with no tool attached a
+// push and a pop cost a few nanoseconds.
+struct Range {
+    explicit Range(const char *name) { nvtxRangePushA(name); }
+    ~Range() { nvtxRangePop(); }
+    Range(const Range &) = delete;
+    Range &operator=(const Range &) = delete;
+};
+#define MTB_RANGE(name) ::mtb::Range mtb_range_scope_(name)
 
 #define MTB_CUDA_TRY(expr)                                   \
     do {                                                     \

@@ -73,6 +73,7 @@ extern "C" int mtb_grid_autotune_workspace_size(const mtb_grid_job *jobs, int nj
 
 extern "C" int mtb_grid_autotune(mtb_grid_job *jobs, int njobs, void *d_workspace, size_t workspace_bytes,
                                  mtb_stream_t stream, mtb_grid_tuning *best, mtb_grid_tuning *candidates) {
+    MTB_RANGE("mtb_grid_autotune");
     if (!jobs || !best) return MTB_ERR_NULL;
     if (njobs < 1 || njobs > 64) return MTB_ERR_BAD_SHAPE;
     for (int j = 0; j < njobs; j++)

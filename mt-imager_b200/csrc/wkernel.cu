@@ -243,6 +243,7 @@ extern "C" int mtb_wkernel_query(const mtb_wkernel_params *p, mtb_wkernel_info *
 extern "C" int mtb_wkernel_build(const mtb_wkernel_params *p, void *d_workspace, size_t workspace_bytes,
                                  void *d_table, size_t table_capacity, int *d_conv_info, int *h_conv_info,
                                  float *d_conv_sums, size_t *table_elems, mtb_stream_t stream) {
+    MTB_RANGE("mtb_wkernel_build");
     if (!d_workspace || !d_table || !h_conv_info || !d_conv_sums) return MTB_ERR_NULL;
     cudaStream_t st = (cudaStream_t)stream;
     WGeom g;
@@ -317,6 +318,7 @@ extern "C" int mtb_wkernel_build(const mtb_wkernel_params *p, void *d_workspace,
 extern "C" int mtb_taper_kernel_build(int support, int sampling, void *d_table, size_t table_capacity,
                                       int *d_conv_info, int *h_conv_info, float *d_conv_sums, size_t *table_elems,
                                       mtb_stream_t stream) {
+    MTB_RANGE("mtb_taper_kernel_build");
     using namespace mtb;
     if (!d_table || !h_conv_info || !d_conv_sums || !table_elems) return MTB_ERR_NULL;
     if (support < 1 || support % 2 == 0 || support > 255 || sampling < 1 || sampling > 64) return MTB_ERR_BAD_PARAM;

@@ -24,6 +24,7 @@ MTB_ERR_CUFFT = 6
 MTB_ERR_KERNEL = 7
 MTB_ERR_NULL = 8
 MTB_ERR_TOO_LARGE = 9
+MTB_ERR_CANCELLED = 10
 MTB_POL_LINEAR = 0
 MTB_POL_CIRCULAR = 1
 
@@ -36,7 +37,8 @@ EXPORTS = (
     "mtb_release_caches", "mtb_kernel_launch_count", "mtb_calibrate_fp32",
     "mtb_taper_kernel_build", "mtb_grid_batch_workspace_size", "mtb_grid_batch",
     "mtb_grid_autotune_workspace_size", "mtb_grid_autotune", "mtb_grid_autotune_candidate_count", "mtb_sort_index", "mtb_gather_rows", "mtb_fits_create", "mtb_fits_write_channel", "mtb_fits_close",
-    "mtb_engine_create", "mtb_engine_submit", "mtb_engine_wait", "mtb_engine_request_bytes", "mtb_engine_destroy",
+    "mtb_engine_create", "mtb_engine_submit", "mtb_engine_wait", "mtb_engine_cancel", "mtb_engine_request_bytes",
+    "mtb_engine_destroy",
 )
 
 
@@ -170,6 +172,7 @@ def load(path: str = LIB_PATH):
     L.mtb_engine_create.argtypes = [ctypes.POINTER(EngineConfig), ctypes.POINTER(p)]
     L.mtb_engine_submit.argtypes = [p, ctypes.POINTER(ImageRequest), ctypes.POINTER(ctypes.c_longlong)]
     L.mtb_engine_wait.argtypes = [p, ctypes.c_longlong, ctypes.POINTER(ImageResult)]
+    L.mtb_engine_cancel.argtypes = [p, ctypes.c_longlong]
     L.mtb_engine_request_bytes.argtypes = [p, ctypes.POINTER(ImageRequest), ctypes.POINTER(sz)]
     L.mtb_engine_destroy.argtypes = [p]
     _lib = L

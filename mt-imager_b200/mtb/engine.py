@@ -85,6 +85,13 @@ class Engine:
         self._pending[t.value] = keep
         return t.value
 
+    def cancel(self, ticket: int) -> None:
+        """Cancel a request: dropped if still queued, stopped at its next chunk
+        boundary if running; wait() then returns status MTB_ERR_CANCELLED (a
+        request that had completed keeps its result).  The host arrays stay
+        referenced until wait()."""
+        L.check(self.lib.mtb_engine_cancel(self._h, ticket), "mtb_engine_cancel")
+
     def wait(self, ticket: int) -> Result:
         res = L.ImageResult()
         L.check(self.lib.mtb_engine_wait(self._h, ticket, ctypes.byref(res)), "mtb_engine_wait")

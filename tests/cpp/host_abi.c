@@ -85,6 +85,8 @@ int main(void)
     mtb_wkernel_info info;
     CHECK(mtb_wkernel_query(&wp, &info) == MTB_ERR_BAD_PARAM);
     CHECK(mtb_engine_destroy(NULL) == MTB_ERR_NULL);
+    CHECK(mtb_engine_cancel(NULL, 1) == MTB_ERR_NULL);
+    CHECK(strcmp(mtb_status_string(MTB_ERR_CANCELLED), "request cancelled") == 0);
     CHECK(mtb_fits_create(NULL, NULL, NULL) != MTB_OK);
 
     printf("ok\n");

@@ -86,7 +86,7 @@ def test_status_codes_match_header():
     import re
     src = open(os.path.join(ROOT, "include", "mtb.h")).read()
     codes = {m.group(1): int(m.group(2)) for m in re.finditer(r"\b(MTB_(?:OK|ERR_\w+))\s*=\s*(\d+)", src)}
-    assert len(codes) == 10
+    assert len(codes) == 11
     for name, v in codes.items():
         assert getattr(L, name) == v, name
 

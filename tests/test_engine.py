@@ -142,3 +142,38 @@ def test_cpp_host_api(tmp_path):
     im.grid_chunk(c["uvw"], c["freq"], c["vis"], c["weights"], c["flags"])
     ref = im.finalize().cpu().numpy()
     assert np.abs(img - ref).max() <= MIX_TOL * np.abs(ref[0]).max()
+
+
+def test_cancel_queued_and_running_requests():
+    """mtb_engine_cancel: with one slot, a long request (many small chunks)
+    and two queued ones.  The queued request cancelled before admission is
+    dropped (no service time); the long one, cancelled while it is admitted
+    or queued, ends with MTB_ERR_CANCELLED; the untouched request still images
+    as it does alone.  A request that completed keeps its result, and an
+    unknown ticket is refused."""
+    import time
+    from mtb.engine import Engine
+    big = case(47, 128, 4, ntimes=600)[0]
+    small = case(48, 64, 4, nw=4)[0]
+    with Engine(slots=1, chunk_records=256) as e:
+        t1 = submit(e, big, exact_delta=True)
+        t2 = submit(e, small, exact_delta=True)
+        t3 = submit(e, small, exact_delta=True)
+        e.cancel(t2)
+        e.cancel(t1)                          # just admitted (building its kernels) or still queued
+        r1, r2, r3 = e.wait(t1), e.wait(t2), e.wait(t3)
+        assert r2.status == L.MTB_ERR_CANCELLED and r2.service_ms == 0.0
+        assert r1.status == L.MTB_ERR_CANCELLED
+        assert r3.status == 0 and r3.stats["gridded_records"] > 0
+        t4 = submit(e, small, exact_delta=True)
+        r4 = e.wait(t4)
+        assert r4.status == 0
+        assert np.abs(r3.image - r4.image).max() <= MIX_TOL * np.abs(r4.image[0]).max()
+        t5 = submit(e, small, exact_delta=True)
+        time.sleep(2.0)                       # long done: cancelling it changes nothing
+        e.cancel(t5)
+        r5 = e.wait(t5)
+        assert r5.status == 0 and np.array_equal(r5.image, r4.image)
+        with pytest.raises(L.MtbError) as err:
+            e.cancel(t5)                      # already waited for
+        assert err.value.status == L.MTB_ERR_BAD_PARAM
