@@ -196,6 +196,18 @@ typedef struct mtb_grid_params {
  * none: no_grid_lo or merge = 1); what d_delta must hold with external_delta. */
 int mtb_grid_delta_bytes(const mtb_grid_params *p, size_t *bytes);
 
+/* Status word of the bounds-checked build (libmtb_checked.so, built with
+ * -DMTB_CHECKED by `build.py --checked`).  In that build the gridders check
+ * every kernel-table tap they read and every grid cell they add to before the
+ * access; an index out of range is skipped and the first one is recorded in a
+ * device word instead of faulting.  *checked = 1 in that build, 0 otherwise
+ * (and *word = 0).  *word: 0 = no index out of range since the last call;
+ * 1 streaming gridder tap, 2 staged gridder tap, 3 direct-gridder flush,
+ * 4 tile-window tap, 5 tile-window flush.  Reads and clears the word; call it
+ * after synchronising the streams that ran the work (a copy from a device
+ * symbol, ordered with the legacy default stream). */
+int mtb_bounds_status(int *checked, unsigned *word);
+
 typedef struct mtb_grid_stats {
     unsigned long long gridded_records;     /* Statistic:TotalGriddedRecords    (WImager.cpp:173) */
     unsigned long long compressed_records;  /* Statistic:TotalCompressedRecords (WImager.cpp:174) */

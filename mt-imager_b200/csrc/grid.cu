@@ -325,6 +325,32 @@ __global__ void k_finish(int P, const double *__restrict__ norm_acc, float *__re
     }
 }
 
+// ------------------------------------------------------- checked build --
+// Built with -DMTB_CHECKED (libmtb_checked.so, build.py --checked): every
+// data-dependent index of the gridders -- the kernel-table taps each slot
+// reads and the grid cell each flush adds to -- is checked before use; an
+// index out of range is skipped and the first such site is recorded in a
+// device status word (mtb_bounds_status) instead of faulting.  Other indices
+// of the path are loop-bounded by construction.  The unchecked build
+// compiles the checks away.
+enum BoundsSite : unsigned {
+    kSiteTapStreaming = 1,   // k_grid7: tap read outside the padded table
+    kSiteTapStaged = 2,      // k_grid3 / k_grid5: tap read outside the padded table
+    kSiteFlush = 3,          // direct gridders: flush outside the grid
+    kSiteTapWindow = 4,      // k_grid: tap read outside the table
+    kSiteCellWindow = 5      // k_grid: flush outside the tile window or the grid
+};
+#ifdef MTB_CHECKED
+__device__ unsigned g_bounds_word;
+__device__ __forceinline__ bool in_bounds(long long i, long long n, unsigned site) {
+    if (i >= 0 && i < n) return true;
+    atomicCAS(&g_bounds_word, 0u, site);
+    return false;
+}
+#else
+__device__ __forceinline__ bool in_bounds(long long, long long, unsigned) { return true; }
+#endif
+
 // ---------------------------------------------------------------- gridder --
 struct GridArgs {
     const int4 *items;
@@ -337,6 +363,7 @@ struct GridArgs {
     float *grid_lo;             // may be null
     int nx, ny;
     int bucket, M, rows, nbands, tile, W;
+    int table_elems, cells;     // bounds of the checked build
 };
 
 // Two-float merge: hi += t with the rounding error of that add accumulated in lo.
@@ -459,7 +486,8 @@ __global__ void __launch_bounds__(KMAX >= 8 ? 576 : 1024) k_grid(GridArgs a) {
 #pragma unroll
                 for (int j = 0; j < KMAX; j++) {
                     const int b = b0 + j * rows;
-                    if (b < M && sy < S) {
+                    if (b < M && sy < S && in_bounds(tbase + sy * S, a.table_elems, kSiteTapWindow) &&
+                        in_bounds(cbase + sy * stride, WINDOW ? W * W : a.cells, kSiteCellWindow)) {
                         const int cell = cbase + sy * stride;
                         const float2 cw = __ldg(&a.table[tbase + sy * S]);
                         if (cell != last[j]) {
@@ -558,7 +586,10 @@ struct GridJobDesc {
     const int *M;          // [kMaxBuckets] bucket moduli (device)
     int nx;
     int uniform;           // 1: every record's support equals its bucket's modulus
+    int table2_elems;      // entries of table2 (bounds of the checked build)
+    int cells;             // nx * ny (bounds of the checked build)
 };
+
 static const int kMaxBatch = 64;   // images one batched launch grids
 
 struct Grid2Args {
@@ -589,7 +620,8 @@ __device__ __forceinline__ void cp_async_wait() {
 // One cell's flush: vector FP32 reductions into the grid, or, when dgrid is
 // set (compensated mode), FP64 reductions into the call's delta grid.
 template <int P>
-__device__ __forceinline__ void flush_cell(float *grid, double *dgrid, int cell, const float *v) {
+__device__ __forceinline__ void flush_cell(float *grid, double *dgrid, int cell, int cells, const float *v) {
+    if (!in_bounds(cell, cells, kSiteFlush)) return;
     const size_t g = (size_t)cell * 2 * P;
     if (dgrid) {
 #pragma unroll
@@ -601,14 +633,14 @@ __device__ __forceinline__ void flush_cell(float *grid, double *dgrid, int cell,
 }
 
 template <int P>
-__device__ __forceinline__ void flush2(float *grid, double *dgrid, int cell, const float2 *acc) {
+__device__ __forceinline__ void flush2(float *grid, double *dgrid, int cell, int cells, const float2 *acc) {
     float v[2 * P];
 #pragma unroll
     for (int p = 0; p < P; p++) {
         v[2 * p] = acc[p].x;
         v[2 * p + 1] = acc[p].y;
     }
-    flush_cell<P>(grid, dgrid, cell, v);
+    flush_cell<P>(grid, dgrid, cell, cells, v);
 }
 
 // Work schedule of one item for modulus M (KS slots per thread, all in one
@@ -777,7 +809,10 @@ __device__ __forceinline__ void grid_item(const Grid2Args &a, const int4 it, con
             const unsigned dst = ring_s + (unsigned)(k & (D - 1)) * (KS * T * 16);
             // slots outside the box get zeros (toff = 0 keeps the address valid)
 #pragma unroll
-            for (int j = 0; j < KS; j++) cp_async16_zfill_n(dst + j * (T * 16), tab + (z + toffL[j]), vbL[j]);
+            for (int j = 0; j < KS; j++) {
+                const bool in = in_bounds((long long)z + toffL[j], J.table2_elems, kSiteTapStaged);
+                cp_async16_zfill_n(dst + j * (T * 16), tab + (in ? z + toffL[j] : 0), in ? vbL[j] : 0);
+            }
         };
 #pragma unroll
         for (int d = 0; d < D; d++) {
@@ -803,7 +838,7 @@ __device__ __forceinline__ void grid_item(const Grid2Args &a, const int4 it, con
 #pragma unroll
                 for (int j = 0; j < KS; j++) {
                     if (cellN[j] >= 0 && cellN[j] != last[j]) {
-                        if (last[j] >= 0) flush2<P>(ggrid, gdelta, last[j], acc[j]);
+                        if (last[j] >= 0) flush2<P>(ggrid, gdelta, last[j], J.cells, acc[j]);
                         last[j] = cellN[j];
 #pragma unroll
                         for (int p = 0; p < P; p++) acc[j][p] = make_float2(0.f, 0.f);
@@ -843,7 +878,7 @@ __device__ __forceinline__ void grid_item(const Grid2Args &a, const int4 it, con
         cp_async_wait<0>();
 #pragma unroll
         for (int j = 0; j < KS; j++)
-            if (last[j] >= 0) flush2<P>(ggrid, gdelta, last[j], acc[j]);
+            if (last[j] >= 0) flush2<P>(ggrid, gdelta, last[j], J.cells, acc[j]);
     }
 }
 
@@ -1345,7 +1380,10 @@ __device__ __forceinline__ void grid_job7(const GridJobDesc &J, const int first,
     auto tfetch = [&](int k, int z) {
         const unsigned d = tdst + (unsigned)((k & (D - 1)) * KS * 32) * 16;
 #pragma unroll
-        for (int j = 0; j < KS; j++) cp_async16_zfill_n(d + j * 32 * 16, src[j] + z, nb[j]);
+        for (int j = 0; j < KS; j++) {
+            const bool in = in_bounds((long long)(src[j] - tab) + z, J.table2_elems, kSiteTapStreaming);
+            cp_async16_zfill_n(d + j * 32 * 16, in ? src[j] + z : tab, in ? nb[j] : 0);
+        }
     };
     // prologue: records 0 .. 2D-1, then the taps of records 0 .. D-1
 #pragma unroll 1
@@ -1425,7 +1463,7 @@ __device__ __forceinline__ void grid_job7(const GridJobDesc &J, const int first,
             if (chg) {
 #pragma unroll
                 for (int j = 0; j < KS; j++)
-                    if (cell[j] >= 0 && cell[j] != last[j] && last[j] >= 0) flush2<P>(ggrid, gdelta, last[j], acc[j]);
+                    if (cell[j] >= 0 && cell[j] != last[j] && last[j] >= 0) flush2<P>(ggrid, gdelta, last[j], J.cells, acc[j]);
             }
             // Reset of the flushed slots by a packed multiply with 0 (1 keeps
             // the sum): branch-free, so the accumulators keep their registers
@@ -1470,7 +1508,7 @@ __device__ __forceinline__ void grid_job7(const GridJobDesc &J, const int first,
     __syncwarp();              // the rings are reused by the next job
 #pragma unroll
     for (int j = 0; j < KS; j++)
-        if (last[j] >= 0) flush2<P>(ggrid, gdelta, last[j], acc[j]);
+        if (last[j] >= 0) flush2<P>(ggrid, gdelta, last[j], J.cells, acc[j]);
 }
 
 template <class C, int P, bool UNIFORM, bool EXACT>
@@ -1617,6 +1655,7 @@ struct GridSpace {
     void *cub;
     size_t cub_bytes;
     float4 *table2;      // padded table with each tap as {re, re, im, im} (k_grid3)
+    size_t table2_elems;
     int *pbase;          // first padded element, then first row, of every plane (k_pad_bases)
     int *moduli;         // bucket moduli of the plan (device copy)
     int *err;            // gridder pipeline error flag
@@ -1664,6 +1703,7 @@ static void carve_grid(Arena &A, int R, int P, int chunk, size_t table_elems, si
     s->cub_bytes = cub_bytes((int)n);
     s->cub = A.take<char>(s->cub_bytes);
     s->table2 = A.take<float4>(table_elems ? table_elems : 1);
+    s->table2_elems = table_elems;
     s->pbase = A.take<int>(2 * (nw > 0 ? nw : 1) + 1);
     s->moduli = A.take<int>(kMaxBuckets);
     s->err = A.take<int>(1);
@@ -1979,6 +2019,8 @@ static GridJobDesc job_desc(const mtb_grid_params *p, float *grid, bool compensa
     d.dgrid = (compensated && exact_of(p)) ? s.delta : nullptr;
     d.M = s.moduli;
     d.nx = p->nx;
+    d.table2_elems = (int)s.table2_elems;
+    d.cells = p->nx * p->ny;
     // one odd support per bucket: every record's support is its bucket's modulus
     d.uniform = p->support_bucket <= 1 ? 1 : 0;
     return d;
@@ -2037,6 +2079,8 @@ static int run_grid(const mtb_grid_params *p, const GridPlan &plan, const float2
         a.grid_lo = grid_lo;
         a.nx = p->nx;
         a.ny = p->ny;
+        a.table_elems = (int)table_elems;
+        a.cells = p->nx * p->ny;
         for (int b = 0; b < plan.bt.n; b++) {
             int M = plan.bt.M[b];
             if (M <= 0) continue;
@@ -2130,6 +2174,20 @@ extern "C" int mtb_grid_workspace_size(const mtb_grid_params *p, const int *h_co
     carve_grid(A, nrecords, p->npol, chunk, padded_elems_of(p, h_conv_info), workspace_delta_bytes(p), &s,
                p->wplanes);
     *bytes = A.used;
+    return MTB_OK;
+}
+
+extern "C" int mtb_bounds_status(int *checked, unsigned *word) {
+    if (!checked || !word) return MTB_ERR_NULL;
+#ifdef MTB_CHECKED
+    *checked = 1;
+    MTB_CUDA_TRY(cudaMemcpyFromSymbol(word, mtb::g_bounds_word, sizeof(unsigned)));
+    const unsigned zero = 0;
+    MTB_CUDA_TRY(cudaMemcpyToSymbol(mtb::g_bounds_word, &zero, sizeof(unsigned)));
+#else
+    *checked = 0;
+    *word = 0;
+#endif
     return MTB_OK;
 }
 

@@ -11,7 +11,8 @@ import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 PKG = os.path.dirname(HERE)
-LIB_PATH = os.path.join(PKG, "libmtb.so")
+# MTB_LIBRARY=checked selects the bounds-checked build (build.py --checked)
+LIB_PATH = os.path.join(PKG, "libmtb_checked.so" if os.environ.get("MTB_LIBRARY") == "checked" else "libmtb.so")
 
 # status codes (include/mtb.h)
 MTB_OK = 0
@@ -38,7 +39,7 @@ EXPORTS = (
     "mtb_taper_kernel_build", "mtb_grid_batch_workspace_size", "mtb_grid_batch",
     "mtb_grid_autotune_workspace_size", "mtb_grid_autotune", "mtb_grid_autotune_candidate_count", "mtb_sort_index", "mtb_gather_rows", "mtb_fits_create", "mtb_fits_write_channel", "mtb_fits_close",
     "mtb_engine_create", "mtb_engine_submit", "mtb_engine_wait", "mtb_engine_cancel", "mtb_engine_request_bytes",
-    "mtb_engine_destroy",
+    "mtb_engine_destroy", "mtb_bounds_status",
 )
 
 
@@ -132,7 +133,8 @@ def load(path: str = LIB_PATH):
     if _lib is not None:
         return _lib
     if not os.path.exists(path):
-        raise RuntimeError("libmtb.so not found at %s: build it with python mt-imager_b200/build.py" % path)
+        raise RuntimeError("%s not found: build it with python mt-imager_b200/build.py%s"
+                           % (path, " --checked" if path.endswith("_checked.so") else ""))
     L = ctypes.CDLL(path)
     p, i, sz = ctypes.c_void_p, ctypes.c_int, ctypes.c_size_t
     L.mtb_wkernel_query.argtypes = [ctypes.POINTER(WKernelParams), ctypes.POINTER(WKernelInfo)]
@@ -173,6 +175,7 @@ def load(path: str = LIB_PATH):
     L.mtb_engine_submit.argtypes = [p, ctypes.POINTER(ImageRequest), ctypes.POINTER(ctypes.c_longlong)]
     L.mtb_engine_wait.argtypes = [p, ctypes.c_longlong, ctypes.POINTER(ImageResult)]
     L.mtb_engine_cancel.argtypes = [p, ctypes.c_longlong]
+    L.mtb_bounds_status.argtypes = [ctypes.POINTER(i), ctypes.POINTER(ctypes.c_uint)]
     L.mtb_engine_request_bytes.argtypes = [p, ctypes.POINTER(ImageRequest), ctypes.POINTER(sz)]
     L.mtb_engine_destroy.argtypes = [p]
     _lib = L
