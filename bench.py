@@ -600,6 +600,11 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline(args, spec, uvw, chans, kern, dl, torch, nt)
 
+    # ---- this gridder on the sample and chunking of the reference arm's GPU leg
+    same = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        same = reference_sample_gpu(args, spec, uvw, chans, kern, dl, torch, nt, dev)
+
     # ---- batched cubes and the request stream (rank 0, one GPU): the other
     # two configurations of the workload, measured after the main line
     cube, serve = None, None
@@ -638,6 +643,8 @@ def main():
             line["e2e"] = e2e
         if cpu:
             line["cpu_baseline"] = cpu
+        if same:
+            line["reference_sample_gpu"] = same
         if clk:
             line["clocks"] = clk
         if oracle:
@@ -1106,6 +1113,47 @@ def oracle_check(spec, dl, uvw_d, chan, image_d, kern):
     return {"image_rms_vs_oracle": err, "bound": 1e-5, "kernel_table_max_abs_err": tab_err, "kernel_bound": 1e-6,
             "records": int(uvw_d.shape[1]), "oracle_s": time.perf_counter() - t0,
             "oracle": "FP64 W-projection restatement (oracle/wproj_oracle.c + numpy FFT), host cores"}
+
+
+def reference_sample_gpu(args, spec, uvw_d, chans, kern, dl, torch, nt, dev):
+    """mtb_grid on the records the reference arm's GPU leg grids (the CPU
+    sample: the first baselines of the middle channel over the full track) in
+    chunks of the reference's default 1,000,000 records, timed with CUDA
+    events: samples/s over the gridder kernels' span and over whole mtb_grid
+    calls.  The like-for-like comparison with that leg's reference operators."""
+    from mtb.imager import WProjectionImager
+    n_rec = min(uvw_d.shape[1], cpu_sample_records(args, spec, nt))
+    freq, vis, weights, flags = chans[len(chans) // 2]
+    n = spec["nx"]
+    im = WProjectionImager(n, n, dl, wplanes=spec["wplanes"], sampling=spec["sampling"],
+                           trial_support=spec["trial_support"], max_support=spec["max_support"], kernels=kern,
+                           gridder=args.gridder)
+    gev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+    bounds = list(range(0, n_rec, REF_CHUNK)) + [n_rec]
+    chunks = [(uvw_d[:, a:b].contiguous(), freq[a:b].contiguous(), vis[a:b].contiguous(),
+               weights[a:b].contiguous(), flags[a:b].contiguous()) for a, b in zip(bounds[:-1], bounds[1:])]
+
+    def once():
+        im.reset()
+        g_ms, c_ms = 0.0, 0.0
+        for c in chunks:
+            im.gridder_events = gev
+            c0, c1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            c0.record()
+            im.grid_device(*c)
+            c1.record()
+            torch.cuda.synchronize()
+            g_ms += gev[0].elapsed_time(gev[1])
+            c_ms += c0.elapsed_time(c1)
+        return g_ms, c_ms
+    once()                                    # workspace and plans
+    g_ms, c_ms = once()
+    st = im.statistics()
+    samples = (st["gridded_records"] + st["compressed_records"]) * 4
+    return {"value": samples / (c_ms * 1e-3), "unit": "samples/s", "gridder_value": samples / (g_ms * 1e-3),
+            "gridder_ms": g_ms, "calls_ms": c_ms, "records": int(n_rec), "chunk_records": REF_CHUNK,
+            "sample": "the cpu_baseline sample in chunks of %d records: the records and chunking of the "
+                      "reference arm's reference_gpu leg" % REF_CHUNK}
 
 
 def cpu_sample_records(args, spec, nt):
