@@ -1129,6 +1129,9 @@ def reference_sample_gpu(args, spec, uvw_d, chans, kern, dl, torch, nt, dev):
                            trial_support=spec["trial_support"], max_support=spec["max_support"], kernels=kern,
                            gridder=args.gridder)
     gev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+    for e in gev:             # torch creates the CUDA event on first record
+        e.record()
+    im.gridder_events = gev
     bounds = list(range(0, n_rec, REF_CHUNK)) + [n_rec]
     chunks = [(uvw_d[:, a:b].contiguous(), freq[a:b].contiguous(), vis[a:b].contiguous(),
                weights[a:b].contiguous(), flags[a:b].contiguous()) for a, b in zip(bounds[:-1], bounds[1:])]
@@ -1137,7 +1140,6 @@ def reference_sample_gpu(args, spec, uvw_d, chans, kern, dl, torch, nt, dev):
         im.reset()
         g_ms, c_ms = 0.0, 0.0
         for c in chunks:
-            im.gridder_events = gev
             c0, c1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             c0.record()
             im.grid_device(*c)
