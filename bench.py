@@ -555,7 +555,7 @@ def main():
     # 4096^2), measured with ncu (dram__bytes_read.sum + dram__bytes_write.sum,
     # one pass; profiles/k_grid7_mid4096_8h_dram.md); other workloads and
     # gridders were not captured
-    gridder = args.gridder or 7
+    gridder = args.gridder or 8
     traffic = (GRIDDER_TRAFFIC.get(gridder) if (spec["name"] == "mid" and spec["hours"] == 8.0 and R == 29030400)
                else None)
     props = torch.cuda.get_device_properties(dev)

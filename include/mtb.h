@@ -163,17 +163,18 @@ typedef struct mtb_grid_params {
                                   FP32 delta's rounding past the 1e-5 image bound           */
     int gridder_threads;       /* 0: 256; threads of a gridder block, which grids one work
                                   item at a time (256 or 512)                              */
-    int gridder;               /* 0: default (7, or 3 with gridder_threads 512);
+    int gridder;               /* 0: default (8, or 3 with gridder_threads 512);
                                   3: k_grid3 (block-wide staging of each work item);
                                   5: k_grid5 (two item buffers refilled by one warp, no
                                   block barriers; items of at most 256 records);
                                   7: k_grid7 (every warp streams its own jobs -- one work
                                   item against 128 slots of its support box -- with no
                                   block barriers; items of at most 512 records);
-                                  8: k_grid7 with 256 slots per job (8 per lane: twice
-                                  the packed FMAs per record handled, 12 warps per SM).
-                                  A gridder that could not complete sets the normaliser
-                                  to NaN                                                   */
+                                  8: k_grid7 with tap pairs (a lane's slots are two pairs
+                                  of neighbouring columns, each pair's taps fetched by one
+                                  16-byte copy from a pair table; needs one support per
+                                  bucket, else 7 runs).  A gridder that could not complete
+                                  sets the normaliser to NaN                               */
     int flags_u8;              /* 0: d_flags is int32 [R][P] (the reference's layout); 1: it
                                   is one byte per flag, uint8 [R][P] (0 = keep, non-zero = flagged;
                                   a quarter of the bytes to move), passed cast to int *    */

@@ -270,7 +270,7 @@ __global__ void k_gather(int R, const unsigned *__restrict__ skeys, const int *_
                          const float2 *__restrict__ vis, const float *__restrict__ weights,
                          const F *__restrict__ flags, int4 *__restrict__ wpos, void *__restrict__ wvis,
                          BucketTable bt, int nx, const int *__restrict__ conv_info, const int *__restrict__ pbase,
-                         int nw, int psf) {
+                         int nw, int psf, int vpairs) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < R; i += gridDim.x * blockDim.x) {
         if (skeys[i] == kNoKey) continue;
         int g = sidx[i];
@@ -297,9 +297,13 @@ __global__ void k_gather(int R, const unsigned *__restrict__ skeys, const int *_
             const int rxm = (M - q.x % M) % M, rym = (M - q.y % M) % M;
             wpos[i] = make_int4(q.y * nx + q.x, rxm | (rym << 16), padded_index(q.z, q.w, conv_info, pbase, nw),
                                 q.w);
+            // {re, im, -im, re}: two packed FMAs per expanded tap; vpairs (the
+            // tap-pair gridder): {re, re, im, im}
             float4 *o = (float4 *)wvis + (size_t)i * P;
 #pragma unroll
-            for (int p = 0; p < P; p++) o[p] = make_float4(acc[p].x, acc[p].y, -acc[p].y, acc[p].x);
+            for (int p = 0; p < P; p++)
+                o[p] = vpairs ? make_float4(acc[p].x, acc[p].x, acc[p].y, acc[p].y)
+                              : make_float4(acc[p].x, acc[p].y, -acc[p].y, acc[p].x);
         } else {
             wpos[i] = q;
             float2 *o = (float2 *)wvis + (size_t)i * P;
@@ -736,6 +740,55 @@ __global__ void k_pad_expand(const float2 *__restrict__ t, const int *__restrict
         for (int x = lane; x <= S; x += 32) {
             const float2 c = x < S ? t[src + x] : make_float2(0.f, 0.f);
             t2[dst + x] = make_float4(c.x, c.x, c.y, c.y);
+        }
+    }
+}
+
+// The pair table of the tap-pair gridder, in k_pad_expand's layout (S + 1
+// 16-byte entries per sub-kernel row): entry k < (S + 1) / 2 holds taps
+// (2k, 2k + 1) and entry (S + 1) / 2 + k taps (2k + 1, 2k + 2), each {re, im};
+// a tap index S stands for tap 0 (the neighbour of column S - 1 under Romein's
+// wrap with one support per bucket), and the pair starting at column S is zero.
+__global__ void k_pad_pairs(const float2 *__restrict__ t, const int *__restrict__ conv_info,
+                            const int *__restrict__ pbase, int nw, int rows, float4 *__restrict__ t2) {
+    const int lane = threadIdx.x & 31;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int per = (rows + nwarps - 1) / nwarps;
+    const int r0 = warp * per, r1 = min(rows, r0 + per);
+    if (r0 >= r1) return;
+    const int *rbase = pbase + nw;
+    int lo = 0, hi = nw - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(&rbase[mid]) <= r0) lo = mid;
+        else hi = mid - 1;
+    }
+    int k = lo;
+    int S = __ldg(&conv_info[2 * k]), rb = __ldg(&rbase[k]), next = __ldg(&rbase[k + 1]);
+    size_t cbase = (size_t)__ldg(&conv_info[2 * k + 1]), pb = (size_t)__ldg(&pbase[k]);
+    for (int row = r0; row < r1; row++) {
+        while (row >= next) {     // next plane (rbase[nw] is the total, so this ends)
+            k++;
+            S = __ldg(&conv_info[2 * k]);
+            rb = next;
+            next = __ldg(&rbase[k + 1]);
+            cbase = (size_t)__ldg(&conv_info[2 * k + 1]);
+            pb = (size_t)__ldg(&pbase[k]);
+        }
+        const int rel = row - rb;        // sub * S + y
+        const int sub = rel / S, y = rel - sub * S;
+        const size_t src = cbase + (size_t)rel * S;
+        const size_t dst = pb + (size_t)sub * S * (S + 1) + (size_t)y * (S + 1);
+        const int half = (S + 1) >> 1;
+        for (int x = lane; x <= S; x += 32) {
+            const int c0 = x < half ? 2 * x : 2 * (x - half) + 1;    // first column of the pair
+            float2 a = make_float2(0.f, 0.f), b = make_float2(0.f, 0.f);
+            if (c0 < S) {
+                a = t[src + c0];
+                b = t[src + (c0 + 1 < S ? c0 + 1 : 0)];
+            }
+            t2[dst + x] = make_float4(a.x, a.y, b.x, b.y);
         }
     }
 }
@@ -1177,26 +1230,39 @@ __global__ void __launch_bounds__(kG3Threads, 2) k_grid5(Grid2Args a, int *err) 
 // Jobs are ordered by segment (image, support bucket), largest support
 // first, so the longest jobs are handed out first.
 //
-// Two shapes (G7Cfg): gridder 7, 4 slots per lane (128 per job), taps 4
-// records ahead, 8-warp blocks, 2 per SM; gridder 8, 8 slots per lane (256 per
-// job: twice the packed FMAs per record for the same record handling), taps 2
-// records ahead, 4-warp blocks, 3 per SM (the doubled accumulators cost
-// registers; the smaller rings keep 12 warps' within the SM's shared memory).
-template <int KS_, int D_, int WARPS_, int MINB_>
+// Two shapes (G7Cfg).  Gridder 7: 4 slots per lane (128 per job), each tap
+// copied on its own as {re, re, im, im}; 8-warp blocks, 2 per SM.  Gridder 8
+// (tap pairs): the 4 slots of a lane are two pairs of neighbouring box
+// columns (a, a + 1), whose taps sit side by side in a pair table, so one
+// 16-byte copy fetches both (the per-lane tap copies are this kernel's
+// measured limit: halving their number made it 21 % faster); the taps stay
+// compact {re, im}, the visibilities come as {re, re, im, im} and each slot
+// keeps two packed sums (re·{re, im}, im·{re, im} of the tap), combined at
+// its flush; 4-warp blocks, 4 per SM (127 registers: the doubled sums fit
+// without spilling).  The
+// pair table (k_pad_pairs) holds, for every sub-kernel row, the pairs
+// (tap 2k, tap 2k + 1) and (tap 2k + 1, tap 2k + 2), so a pair starting at
+// any column is one aligned 16-byte entry; the pair at the last column holds
+// tap 0 as its second tap, the neighbour of column S - 1 under Romein's wrap,
+// which is why gridder 8 needs one support per bucket (the host uses gridder
+// 7 otherwise).
+template <int KS_, int D_, int WARPS_, int MINB_, bool PAIRS_>
 struct G7Cfg {
+    static constexpr bool PAIRS = PAIRS_;
     static constexpr int KS = KS_;                       // slots per lane
     static constexpr int D = D_;                         // taps fetched this many records ahead
     static constexpr int Warps = WARPS_;                 // warps per block
     static constexpr int Threads = 32 * WARPS_;
     static constexpr int MinBlocks = MINB_;              // blocks per SM the registers are capped for
     static constexpr int RR = 2 * D_ + 1 <= 8 ? 8 : 16;  // record-ring entries (records fetched 2D ahead)
+    static constexpr int NF = PAIRS_ ? KS_ / 2 : KS_;     // tap copies per lane and record
     static constexpr int PartSlots = 32 * KS_;           // slots of one job
     static constexpr int TapStride = D_ * KS_ * 32;      // tap-ring / FIFO entries per warp
     static_assert(RR >= 2 * D_ + 1, "the record ring holds every record in flight");
     static_assert((D_ & (D_ - 1)) == 0, "ring indices are masked");
 };
-using G7Narrow = G7Cfg<4, 4, 8, 2>;    // gridder 7
-using G7Wide = G7Cfg<8, 2, 4, 3>;      // gridder 8
+using G7Narrow = G7Cfg<4, 4, 8, 2, false>;   // gridder 7
+using G7Pairs = G7Cfg<4, 4, 4, 4, true>;     // gridder 8, the default
 static const int kG7Chunk = 512;       // records of one work item
 
 // Jobs [job0, next.job0) are items [item0, item0 + n) x wu parts of modulus m.
@@ -1223,7 +1289,8 @@ struct G7SegSrc {
 // One block of kMaxBuckets threads: the segments of every image in image
 // order (the order of the concatenated item list), buckets by descending
 // modulus within an image.
-__global__ void k_g7_segments(G7SegSrc src, int nimages, int part_slots, G7Segment *__restrict__ segs,
+// pairs: jobs hold 64 column pairs ((M + 1) / 2 per box row) instead of 128 slots.
+__global__ void k_g7_segments(G7SegSrc src, int nimages, int pairs, G7Segment *__restrict__ segs,
                               int *__restrict__ n_segs) {
     using Scan = cub::BlockScan<int, kMaxBuckets>;
     __shared__ typename Scan::TempStorage tmp;
@@ -1241,7 +1308,7 @@ __global__ void k_g7_segments(G7SegSrc src, int nimages, int part_slots, G7Segme
             m = src.M[j][bb];
             if (m <= 0 || cnt <= 0) cnt = 0;
         }
-        const int wu = cnt ? (m * m + part_slots - 1) / part_slots : 0;
+        const int wu = cnt ? (pairs ? (((m + 1) >> 1) * m + 63) / 64 : (m * m + 127) / 128) : 0;
         int idx, njob, aggr_seg, aggr_job;
         Scan(tmp).ExclusiveSum(cnt ? 1 : 0, idx, aggr_seg);
         __syncthreads();
@@ -1328,7 +1395,9 @@ __global__ void k_mark_runs(const int4 *__restrict__ items, const int *__restric
 template <class C, int P, bool UNIFORM, bool EXACT>
 __device__ __forceinline__ void grid_job7(const GridJobDesc &J, const int first, const int N, const int M,
                                           const int part, float4 *tring, int *fifo, float4 *rring) {
-    constexpr int KS = C::KS, D = C::D, RR = C::RR, E = 1 + P;
+    constexpr int KS = C::KS, D = C::D, RR = C::RR, E = 1 + P, NF = C::NF;
+    constexpr bool PR = C::PAIRS;
+    static_assert(!PR || UNIFORM, "tap pairs need one support per bucket");
     const int lane = threadIdx.x & 31;
     const float4 *const tab = J.table2;
     float *const ggrid = EXACT ? nullptr : J.grid;
@@ -1337,14 +1406,31 @@ __device__ __forceinline__ void grid_job7(const GridJobDesc &J, const int first,
     const int MM = M * M;
     // box position (qa, qb) of every slot of this lane; qb = -1: no slot
     int qa[KS], qb[KS];
-    int nb[KS];                  // copy size of each slot's tap: 16, or 0 outside the box
+    int nb[NF];                  // bytes of each tap copy: 16, 8 (a pair's second column is off the box), 0
+    if constexpr (PR) {
+        // pair jp: box columns (2 pc, 2 pc + 1) of box row b, (M + 1) / 2 pairs per row
+        const int PW = (M + 1) >> 1;
 #pragma unroll
-    for (int j = 0; j < KS; j++) {
-        const int q = part * C::PartSlots + j * 32 + lane;
-        const int b = q / M;
-        qa[j] = q - b * M;
-        qb[j] = q < MM ? b : -1;
-        nb[j] = q < MM ? 16 : 0;
+        for (int jp = 0; jp < NF; jp++) {
+            const int pq = part * (32 * NF) + jp * 32 + lane;
+            const int b = pq / PW;
+            const int pc = pq - b * PW;
+            const bool in = b < M, two = 2 * pc + 1 < M;
+            qa[2 * jp] = 2 * pc;
+            qb[2 * jp] = in ? b : -1;
+            qa[2 * jp + 1] = 2 * pc + 1;
+            qb[2 * jp + 1] = in && two ? b : -1;
+            nb[jp] = in ? (two ? 16 : 8) : 0;
+        }
+    } else {
+#pragma unroll
+        for (int j = 0; j < KS; j++) {
+            const int q = part * C::PartSlots + j * 32 + lane;
+            const int b = q / M;
+            qa[j] = q - b * M;
+            qb[j] = q < MM ? b : -1;
+            nb[j] = q < MM ? 16 : 0;
+        }
     }
     // record ring: lane 0 copies the record, lanes 1..P its visibilities
     const int rflag = lane <= P ? 1 : 0;
@@ -1359,11 +1445,29 @@ __device__ __forceinline__ void grid_job7(const GridJobDesc &J, const int first,
                      : "memory");
     };
     auto rec = [&](int k) { return *(const int4 *)(rring + (k & (RR - 1)) * E); };
-    // look-ahead: row base of every slot for the run being fetched
-    const float4 *src[KS];
+    // look-ahead: source of every tap copy for the run being fetched
+    const float4 *src[NF];
     auto pgeom = [&](int k, const int4 r) {   // record k opens a run: geometry of its slots
         const int rxm = r.y & 0xFFFF, rym = r.y >> 16, S = r.w & 0xFFFF;
         int *const f = fifo + (k & (D - 1)) * KS * 32;
+        if constexpr (PR) {
+            // pair table row: (S + 1) / 2 pairs starting at even columns, then
+            // (S + 1) / 2 starting at odd columns (S == M)
+#pragma unroll
+            for (int jp = 0; jp < NF; jp++) {
+                int sx = qa[2 * jp] + rxm;
+                sx -= (sx >= M) ? M : 0;
+                int sy = qb[2 * jp] + rym;
+                sy -= (sy >= M) ? M : 0;
+                int sx1 = sx + 1;
+                sx1 -= (sx1 >= M) ? M : 0;
+                const bool ok = qb[2 * jp] >= 0;
+                src[jp] = tab + (ok ? sy * (S + 1) + (sx & 1) * ((S + 1) >> 1) + (sx >> 1) : 0);
+                f[2 * jp * 32] = ok ? r.x + sy * gnx + sx : -1;
+                f[(2 * jp + 1) * 32] = qb[2 * jp + 1] >= 0 ? r.x + sy * gnx + sx1 : -1;
+            }
+            return;
+        }
 #pragma unroll
         for (int j = 0; j < KS; j++) {
             int sx = qa[j] + rxm;
@@ -1380,7 +1484,7 @@ __device__ __forceinline__ void grid_job7(const GridJobDesc &J, const int first,
     auto tfetch = [&](int k, int z) {
         const unsigned d = tdst + (unsigned)((k & (D - 1)) * KS * 32) * 16;
 #pragma unroll
-        for (int j = 0; j < KS; j++) {
+        for (int j = 0; j < NF; j++) {
             const bool in = in_bounds((long long)(src[j] - tab) + z, J.table2_elems, kSiteTapStreaming);
             cp_async16_zfill_n(d + j * 32 * 16, in ? src[j] + z : tab, in ? nb[j] : 0);
         }
@@ -1408,12 +1512,28 @@ __device__ __forceinline__ void grid_job7(const GridJobDesc &J, const int first,
     }
     int last[KS];
     float2 acc[KS][P];
+    float2 accb[PR ? KS : 1][P];   // tap pairs: the sums of {re, im} of the tap times im of the visibility
 #pragma unroll
     for (int j = 0; j < KS; j++) {
         last[j] = -1;
 #pragma unroll
-        for (int p = 0; p < P; p++) acc[j][p] = make_float2(0.f, 0.f);
+        for (int p = 0; p < P; p++) {
+            acc[j][p] = make_float2(0.f, 0.f);
+            if (PR) accb[PR ? j : 0][p] = make_float2(0.f, 0.f);
+        }
     }
+    // slot j's sums as {re, im} per polarisation, flushed to its last cell
+    auto flush_slot = [&](int j) {
+        if constexpr (PR) {
+            float2 v[P];
+#pragma unroll
+            for (int p = 0; p < P; p++)
+                v[p] = make_float2(acc[j][p].x - accb[j][p].y, accb[j][p].x + acc[j][p].y);
+            flush2<P>(ggrid, gdelta, last[j], J.cells, v);
+        } else {
+            flush2<P>(ggrid, gdelta, last[j], J.cells, acc[j]);
+        }
+    };
     // One record: accumulate record i (two packed FMAs per tap and
     // polarisation; ConvolutionGridder.cu:153-181: to += vis * wt, no
     // conjugate); TAP: fetch the taps of record i + D; REC: refill the record
@@ -1430,14 +1550,30 @@ __device__ __forceinline__ void grid_job7(const GridJobDesc &J, const int first,
             wp[p] = make_float2(q.z, q.w);
         }
         const float4 *c4 = tring + (i & (D - 1)) * KS * 32;
+        if constexpr (PR) {
+            // visibilities {re, re, im, im}: vp = (re, re), wp = (im, im)
 #pragma unroll
-        for (int j = 0; j < KS; j++) {
-            const float4 c = c4[j * 32];
-            const float2 cre = make_float2(c.x, c.y), cim = make_float2(c.z, c.w);
+            for (int jp = 0; jp < NF; jp++) {
+                const float4 c = c4[jp * 32];
+                const float2 t0 = make_float2(c.x, c.y), t1 = make_float2(c.z, c.w);
 #pragma unroll
-            for (int p = 0; p < P; p++) {
-                acc[j][p] = __ffma2_rn(cre, vp[p], acc[j][p]);
-                acc[j][p] = __ffma2_rn(cim, wp[p], acc[j][p]);
+                for (int p = 0; p < P; p++) {
+                    acc[2 * jp][p] = __ffma2_rn(t0, vp[p], acc[2 * jp][p]);
+                    accb[2 * jp][p] = __ffma2_rn(t0, wp[p], accb[2 * jp][p]);
+                    acc[2 * jp + 1][p] = __ffma2_rn(t1, vp[p], acc[2 * jp + 1][p]);
+                    accb[2 * jp + 1][p] = __ffma2_rn(t1, wp[p], accb[2 * jp + 1][p]);
+                }
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j < KS; j++) {
+                const float4 c = c4[j * 32];
+                const float2 cre = make_float2(c.x, c.y), cim = make_float2(c.z, c.w);
+#pragma unroll
+                for (int p = 0; p < P; p++) {
+                    acc[j][p] = __ffma2_rn(cre, vp[p], acc[j][p]);
+                    acc[j][p] = __ffma2_rn(cim, wp[p], acc[j][p]);
+                }
             }
         }
         if (decltype(TAP)::value) tfetch(i + D, rec(i + D).z);
@@ -1463,7 +1599,7 @@ __device__ __forceinline__ void grid_job7(const GridJobDesc &J, const int first,
             if (chg) {
 #pragma unroll
                 for (int j = 0; j < KS; j++)
-                    if (cell[j] >= 0 && cell[j] != last[j] && last[j] >= 0) flush2<P>(ggrid, gdelta, last[j], J.cells, acc[j]);
+                    if (cell[j] >= 0 && cell[j] != last[j] && last[j] >= 0) flush_slot(j);
             }
             // Reset of the flushed slots by a packed multiply with 0 (1 keeps
             // the sum): branch-free, so the accumulators keep their registers
@@ -1477,7 +1613,10 @@ __device__ __forceinline__ void grid_job7(const GridJobDesc &J, const int first,
                 const bool c = cell[j] >= 0 && cell[j] != last[j];
                 const float kf = c ? 0.f : 1.f;
 #pragma unroll
-                for (int p = 0; p < P; p++) acc[j][p] = __fmul2_rn(acc[j][p], make_float2(kf, kf));
+                for (int p = 0; p < P; p++) {
+                    acc[j][p] = __fmul2_rn(acc[j][p], make_float2(kf, kf));
+                    if (PR) accb[PR ? j : 0][p] = __fmul2_rn(accb[PR ? j : 0][p], make_float2(kf, kf));
+                }
                 last[j] = c ? cell[j] : last[j];
             }
             cend = i + max(1, rec(i).w >> 16);
@@ -1508,7 +1647,7 @@ __device__ __forceinline__ void grid_job7(const GridJobDesc &J, const int first,
     __syncwarp();              // the rings are reused by the next job
 #pragma unroll
     for (int j = 0; j < KS; j++)
-        if (last[j] >= 0) flush2<P>(ggrid, gdelta, last[j], J.cells, acc[j]);
+        if (last[j] >= 0) flush_slot(j);
 }
 
 template <class C, int P, bool UNIFORM, bool EXACT>
@@ -1542,13 +1681,20 @@ static size_t grid7_smem() {
 }
 
 // UNIFORM kernel when every image of the launch has one support per bucket
+// (always, for the tap-pair shape: the host chooses it only then)
 template <class C, int P>
 static int launch_grid7c(const Grid7Args &a, cudaStream_t st) {
     bool uniform = true;
     for (int j = 0; j < kMaxBatch && a.jobs[j].wpos; j++) uniform = uniform && a.jobs[j].uniform;
     const bool exact = a.jobs[0].dgrid != nullptr;
-    auto kern = uniform ? (exact ? k_grid7<C, P, true, true> : k_grid7<C, P, true, false>)
-                        : (exact ? k_grid7<C, P, false, true> : k_grid7<C, P, false, false>);
+    void (*kern)(Grid7Args);
+    if constexpr (C::PAIRS) {
+        if (!uniform) return MTB_ERR_BAD_PARAM;
+        kern = exact ? k_grid7<C, P, true, true> : k_grid7<C, P, true, false>;
+    } else {
+        kern = uniform ? (exact ? k_grid7<C, P, true, true> : k_grid7<C, P, true, false>)
+                       : (exact ? k_grid7<C, P, false, true> : k_grid7<C, P, false, false>);
+    }
     const size_t smem = grid7_smem<C, P>();
     MTB_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
@@ -1559,12 +1705,10 @@ static int launch_grid7c(const Grid7Args &a, cudaStream_t st) {
     return MTB_OK;
 }
 
-// Slots of one job of the streaming gridder `which` (7 or 8).
-static int g7_part_slots(int which) { return which == 8 ? G7Wide::PartSlots : G7Narrow::PartSlots; }
-
+// pairs: the tap-pair shape (gridder 8, one support per bucket), else gridder 7
 template <int P>
-static int launch_grid7(const Grid7Args &a, int which, cudaStream_t st) {
-    return which == 8 ? launch_grid7c<G7Wide, P>(a, st) : launch_grid7c<G7Narrow, P>(a, st);
+static int launch_grid7(const Grid7Args &a, bool pairs, cudaStream_t st) {
+    return pairs ? launch_grid7c<G7Pairs, P>(a, st) : launch_grid7c<G7Narrow, P>(a, st);
 }
 
 template <int P>
@@ -1756,11 +1900,17 @@ static long long wait_cycles() {
 static int gridder_of(const mtb_grid_params *p) {
     if (p->gridder != 0) return p->gridder;
     if (p->gridder_threads == 512) return 3;
-    return 7;
+    return 8;
 }
 
 // The per-warp streaming gridders (k_grid7 in its two shapes).
 static bool streaming(int which) { return which == 7 || which == 8; }
+
+// The tap-pair shape runs when it is asked for and every record's support is
+// its bucket's modulus (one support per bucket); otherwise gridder 7 does.
+static bool pairs_of(const mtb_grid_params *p) {
+    return p->merge != 1 && gridder_of(p) == 8 && p->support_bucket <= 1;
+}
 
 // Work items shorter than this many records multiply the flushes into each
 // cell: with the FP32 per-call delta grid, 37-record items took the first
@@ -1918,14 +2068,15 @@ static void launch_preprocess(const mtb_grid_params *p, int blocks, cudaStream_t
 template <int P, bool DIRECT>
 static void launch_gather(const mtb_grid_params *p, int blocks, cudaStream_t st, int R, const GridSpace &s,
                           const float2 *vis, const float *weights, const int *flags, const GridPlan &plan,
-                          const int *conv_info, const int *pbase, int nw) {
+                          const int *conv_info, const int *pbase, int nw, bool pairs = false) {
     if (p->flags_u8)
         k_gather<P, DIRECT, unsigned char><<<blocks, 256, 0, st>>>(
             R, s.skeys, s.sidx, s.pos, s.meta, vis, weights, (const unsigned char *)flags, s.wpos, s.wvis, plan.bt,
-            p->nx, conv_info, pbase, nw, p->psf);
+            p->nx, conv_info, pbase, nw, p->psf, pairs ? 1 : 0);
     else
         k_gather<P, DIRECT, int><<<blocks, 256, 0, st>>>(R, s.skeys, s.sidx, s.pos, s.meta, vis, weights, flags,
-                                                         s.wpos, s.wvis, plan.bt, p->nx, conv_info, pbase, nw, p->psf);
+                                                         s.wpos, s.wvis, plan.bt, p->nx, conv_info, pbase, nw, p->psf,
+                                                         pairs ? 1 : 0);
 }
 
 // Everything of one mtb_grid call before the gridder kernels: preprocessing,
@@ -1936,7 +2087,7 @@ template <int P>
 static int prepare_grid(const mtb_grid_params *p, const GridPlan &plan, const float2 *table, size_t table_elems,
                         size_t padded, const int *conv_info, const float *conv_sums, const float *uvw,
                         const float *freq, const float2 *vis, const float *weights, const int *flags, int R,
-                        bool compensated, GridSpace &s, cudaStream_t st) {
+                        bool compensated, GridSpace &s, cudaStream_t st, bool pairs) {
     const int T = oversample_T(p->sampling);
     const int sms = sm_count();
     MTB_CUDA_TRY(cudaMemsetAsync(s.norm_acc, 0, 4 * sizeof(double), st));
@@ -1977,7 +2128,7 @@ static int prepare_grid(const mtb_grid_params *p, const GridPlan &plan, const fl
     }
     k_pad_bases<<<1, 1, 0, st>>>(conv_info, p->wplanes, T, s.pbase);
     MTB_LAUNCHED();
-    launch_gather<P, true>(p, blocks, st, R, s, vis, weights, flags, plan, conv_info, s.pbase, p->wplanes);
+    launch_gather<P, true>(p, blocks, st, R, s, vis, weights, flags, plan, conv_info, s.pbase, p->wplanes, pairs);
     MTB_LAUNCHED();
     if (streaming(gridder_of(p))) {
         // one warp per work item; the item count is on the device: cover the
@@ -1991,7 +2142,10 @@ static int prepare_grid(const mtb_grid_params *p, const GridPlan &plan, const fl
         // the expanded padded table the direct gridders read
         const int rows = plan.table_rows;
         const int pb = (int)std::min<size_t>(((size_t)rows + 7) / 8, (size_t)sms * 16);
-        k_pad_expand<<<pb > 0 ? pb : 1, 256, 0, st>>>(table, conv_info, s.pbase, p->wplanes, rows, s.table2);
+        if (pairs)
+            k_pad_pairs<<<pb > 0 ? pb : 1, 256, 0, st>>>(table, conv_info, s.pbase, p->wplanes, rows, s.table2);
+        else
+            k_pad_expand<<<pb > 0 ? pb : 1, 256, 0, st>>>(table, conv_info, s.pbase, p->wplanes, rows, s.table2);
         MTB_LAUNCHED();
         (void)table_elems;
         (void)padded;
@@ -2064,8 +2218,9 @@ static int run_grid(const mtb_grid_params *p, const GridPlan &plan, const float2
                     float *grid, float *grid_lo, float *normalizer, mtb_grid_stats *stats, GridSpace &s,
                     cudaStream_t st) {
     const bool direct = p->merge != 1;
+    const bool pairs = pairs_of(p);
     MTB_TRY(prepare_grid<P>(p, plan, table, table_elems, padded, conv_info, conv_sums, uvw, freq, vis, weights,
-                            flags, R, direct && grid_lo != nullptr, s, st));
+                            flags, R, direct && grid_lo != nullptr, s, st, pairs));
     if (p->gridder_start_event) MTB_CUDA_TRY(cudaEventRecord((cudaEvent_t)p->gridder_start_event, st));
     if (!direct) {
         GridArgs a;
@@ -2111,7 +2266,7 @@ static int run_grid(const mtb_grid_params *p, const GridPlan &plan, const float2
         src.bounds[0] = s.bounds;
         src.n_items[0] = s.n_items;
         src.M[0] = s.moduli;
-        k_g7_segments<<<1, kMaxBuckets, 0, st>>>(src, 1, g7_part_slots(which), s.segs, s.n_segs);
+        k_g7_segments<<<1, kMaxBuckets, 0, st>>>(src, 1, pairs ? 1 : 0, s.segs, s.n_segs);
         MTB_LAUNCHED();
         MTB_CUDA_TRY(cudaMemsetAsync(s.counter7, 0, sizeof(int), st));
         Grid7Args g7;
@@ -2121,7 +2276,7 @@ static int run_grid(const mtb_grid_params *p, const GridPlan &plan, const float2
         g7.n_segs = s.n_segs;
         g7.counter = s.counter7;
         g7.jobs[0] = g2.jobs[0];
-        MTB_TRY(launch_grid7<P>(g7, which, st));
+        MTB_TRY(launch_grid7<P>(g7, pairs, st));
     } else if (which == 5) {
         MTB_TRY(launch_grid5<P>(g2, s.err, st));
     } else {
@@ -2337,6 +2492,14 @@ static int run_batch(const mtb_grid_job *jobs, int njobs, const GridPlan *plans,
     Grid2Args g2;
     g2.njobs = njobs;
     g2.wait_cycles = wait_cycles();
+    // tap pairs only when every image qualifies (the tables and visibility
+    // layout of one launch are alike)
+    bool pairs = true;
+    for (int j = 0; j < njobs; j++) {
+        mtb_grid_params pj = jobs[j].params;
+        pj.merge = 0;
+        pairs = pairs && pairs_of(&pj);
+    }
     for (int j = 0; j < njobs; j++) {
         const mtb_grid_job &J = jobs[j];
         mtb_grid_params p = J.params;
@@ -2348,7 +2511,7 @@ static int run_batch(const mtb_grid_job *jobs, int njobs, const GridPlan *plans,
         const size_t te = table_elems_of(&p, J.h_conv_info), pe = padded_elems_of(&p, J.h_conv_info);
         MTB_TRY(prepare_grid<P>(&p, plans[j], (const float2 *)J.d_table, te, pe, J.d_conv_info, J.d_conv_sums,
                                 J.d_uvw, J.d_freq, (const float2 *)J.d_vis, J.d_weights, J.d_flags, J.nrecords,
-                                J.d_grid_lo != nullptr, spaces[j], st));
+                                J.d_grid_lo != nullptr, spaces[j], st, pairs));
         q.n_items[j] = spaces[j].n_items;
     }
     const mtb_grid_params &p0 = jobs[0].params;
@@ -2370,7 +2533,7 @@ static int run_batch(const mtb_grid_job *jobs, int njobs, const GridPlan *plans,
             src.n_items[j] = jobs[j].nrecords > 0 ? spaces[j].n_items : nullptr;
             src.M[j] = spaces[j].moduli;
         }
-        k_g7_segments<<<1, kMaxBuckets, 0, st>>>(src, njobs, g7_part_slots(which), segs, spaces[0].n_segs);
+        k_g7_segments<<<1, kMaxBuckets, 0, st>>>(src, njobs, pairs ? 1 : 0, segs, spaces[0].n_segs);
         MTB_LAUNCHED();
         MTB_CUDA_TRY(cudaMemsetAsync(spaces[0].counter7, 0, sizeof(int), st));
         Grid7Args g7;
@@ -2380,7 +2543,7 @@ static int run_batch(const mtb_grid_job *jobs, int njobs, const GridPlan *plans,
         g7.n_segs = spaces[0].n_segs;
         g7.counter = spaces[0].counter7;
         for (int j = 0; j < njobs; j++) g7.jobs[j] = g2.jobs[j];
-        MTB_TRY(launch_grid7<P>(g7, which, st));
+        MTB_TRY(launch_grid7<P>(g7, pairs, st));
     } else if (gridder_of(&p0) == 5) {
         MTB_TRY(launch_grid5<P>(g2, spaces[0].err, st));
         if (check_gridder() && !capturing(st)) {
