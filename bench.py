@@ -270,7 +270,9 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
-GRIDDER_TRAFFIC = {7: 5.018e9}   # bytes per launch, one 8 h mid-size channel (ncu)
+# bytes per gridder launch, one 8 h mid-size channel (ncu: profiles/k_grid7_pairs_mid4096_8h_dram.md
+# for the default tap-pair shape, profiles/k_grid7_mid4096_8h_dram.md for gridder 7)
+GRIDDER_TRAFFIC = {8: 5.017e9, 7: 5.018e9}
 REF_CHUNK = 1000000   # records per WImager chunk: mt-imager's default `records` (mtimager.properties:47-48)
 
 
@@ -553,8 +555,7 @@ def main():
     achieved = flops_per_step / (gridder_ms * 1e-3) / 1e12
     # DRAM bytes of one gridder launch over one channel of this workload (8 h,
     # 4096^2), measured with ncu (dram__bytes_read.sum + dram__bytes_write.sum,
-    # one pass; profiles/k_grid7_mid4096_8h_dram.md); other workloads and
-    # gridders were not captured
+    # one pass; GRIDDER_TRAFFIC); other workloads and gridders were not captured
     gridder = args.gridder or 8
     traffic = (GRIDDER_TRAFFIC.get(gridder) if (spec["name"] == "mid" and spec["hours"] == 8.0 and R == 29030400)
                else None)
