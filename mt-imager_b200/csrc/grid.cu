@@ -1436,12 +1436,12 @@ __device__ __forceinline__ void grid_job7(const GridJobDesc &J, const int first,
     const int rflag = lane <= P ? 1 : 0;
     const char *const rsrc = lane == 0 ? (const char *)(J.wpos + first)
                                        : (const char *)(J.wvis4 + (size_t)first * P + (lane <= P ? lane - 1 : 0));
-    const int rstride = lane == 0 ? 16 : 16 * P;
+    const int rsh = lane == 0 ? 4 : (P == 4 ? 6 : (P == 2 ? 5 : 4));   // log2 of the bytes per record of the source
     const unsigned rdst = (unsigned)__cvta_generic_to_shared(rring) + (unsigned)lane * 16;
     auto rfetch = [&](int r) {
         asm volatile("{\n .reg .pred p;\n setp.ne.b32 p, %2, 0;\n @p cp.async.cg.shared.global [%0], [%1], 16;\n}" ::"r"(
                          rdst + (unsigned)((r & (RR - 1)) * E) * 16),
-                     "l"(rsrc + (size_t)r * rstride), "r"(rflag)
+                     "l"(rsrc + ((size_t)r << rsh)), "r"(rflag)
                      : "memory");
     };
     auto rec = [&](int k) { return *(const int4 *)(rring + (k & (RR - 1)) * E); };
