@@ -66,6 +66,12 @@ struct BucketTable {
     int half;                    // odd supports per bucket
     int M[kMaxBuckets];          // modulus (largest support) of each bucket, 0 = empty
     int tile[kMaxBuckets];       // grid tile edge used for the bucket's keys
+    // A record's sort key packs {bucket, tile row, tile column} into the low
+    // xbits + ybits + bbits bits, bucket most significant; the bit counts
+    // hold the largest tile column, tile row and bucket number + 1, so the
+    // kNoKey sentinel (all ones) sorts after every record when the sort
+    // covers only those bits.
+    int xbits, ybits, bbits;
 };
 
 __device__ __forceinline__ int bucket_of(int S, int half) { return (S - 1) / (2 * half); }
@@ -182,7 +188,7 @@ __global__ void k_compress(int R, int nx, const int4 *__restrict__ pos, int *__r
         } else if (m & 1) {
             int b = bucket_of(q.w, bt.half);
             int t = bt.tile[b];
-            key = ((unsigned)b << 24) | ((unsigned)(q.y / t) << 12) | (unsigned)(q.x / t);
+            key = ((unsigned)b << (bt.xbits + bt.ybits)) | ((unsigned)(q.y / t) << bt.xbits) | (unsigned)(q.x / t);
             st[0] += 1;
             st[2] += s2;
         }
@@ -208,19 +214,24 @@ __global__ void k_chunk_counts(const unsigned *__restrict__ ukeys, const int *__
     }
 }
 
-// Work items: {first record (bin order), record count, bin key}.
+// Work items: {first record (bin order), record count, bin key}, the key
+// widened from the packed sort key to bucket << 24 | tile row << 12 | tile
+// column, the layout the gridders decode.
 __global__ void k_make_items(const unsigned *__restrict__ ukeys, const int *__restrict__ counts,
                              const int *__restrict__ run_start, const int *__restrict__ item_start,
                              const int *__restrict__ nchunks, const int *__restrict__ num_runs, int chunk,
-                             int4 *__restrict__ items) {
+                             int xbits, int ybits, int4 *__restrict__ items) {
     int n = *num_runs;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         int c = nchunks[i];
         int base = item_start[i], s0 = run_start[i], cnt = counts[i];
+        const unsigned k = ukeys[i];
+        const unsigned key = ((k >> (xbits + ybits)) << 24) | (((k >> xbits) & ((1u << ybits) - 1u)) << 12) |
+                             (k & ((1u << xbits) - 1u));
         for (int j = 0; j < c; j++) {
             int a = s0 + j * chunk;
             int len = min(chunk, s0 + cnt - a);
-            items[base + j] = make_int4(a, len, (int)ukeys[i], 0);
+            items[base + j] = make_int4(a, len, (int)key, 0);
         }
     }
 }
@@ -1985,6 +1996,11 @@ static int make_plan(const mtb_grid_params *p, const int *h_conv_info, GridPlan 
         g->bt.n = std::max(g->bt.n, b + 1);
     }
     for (int b = 0; b < kMaxBuckets; b++) g->bt.tile[b] = tile;
+    // bits that hold 0..v
+    auto bits = [](int v) { int n = 0; while (n < 31 && (1 << n) <= v) n++; return n; };
+    g->bt.xbits = bits((p->nx - 1) / tile);   // corners stay below nx - S, ny - S
+    g->bt.ybits = bits((p->ny - 1) / tile);
+    g->bt.bbits = bits(g->bt.n);              // bucket numbers stay below 2^bbits - 1
     if (rows > 0x7FFFFFFFLL) return MTB_ERR_BAD_SHAPE;
     g->table_rows = (int)rows;
     return MTB_OK;
@@ -2101,11 +2117,11 @@ static int prepare_grid(const mtb_grid_params *p, const GridPlan &plan, const fl
     MTB_LAUNCHED();
     k_compress<<<blocks, 256, 0, st>>>(R, p->nx, s.pos, s.meta, s.keys, s.iota, plan.bt, s.stats);
     MTB_LAUNCHED();
-    int end_bit = 24;
-    while ((1 << (end_bit - 24)) < plan.bt.n) end_bit++;
-    // the kNoKey sentinel needs every bit: sort the full 32 bits
+    // only the packed key's bits: 20 for a 4096² grid of 32² tiles and 32
+    // buckets, three 8-bit digit passes instead of four
+    const int end_bit = plan.bt.xbits + plan.bt.ybits + plan.bt.bbits;
     size_t cb = s.cub_bytes;
-    MTB_CUDA_TRY(cub::DeviceRadixSort::SortPairs(s.cub, cb, s.keys, s.skeys, s.iota, s.sidx, R, 0, 32, st));
+    MTB_CUDA_TRY(cub::DeviceRadixSort::SortPairs(s.cub, cb, s.keys, s.skeys, s.iota, s.sidx, R, 0, end_bit, st));
     cb = s.cub_bytes;
     MTB_CUDA_TRY(cub::DeviceRunLengthEncode::Encode(s.cub, cb, s.skeys, s.ukeys, s.counts, s.num_runs, R, st));
     cb = s.cub_bytes;
@@ -2115,7 +2131,7 @@ static int prepare_grid(const mtb_grid_params *p, const GridPlan &plan, const fl
     cb = s.cub_bytes;
     MTB_CUDA_TRY(cub::DeviceScan::ExclusiveSum(s.cub, cb, s.nchunks, s.item_start, R, st));
     k_make_items<<<blocks, 256, 0, st>>>(s.ukeys, s.counts, s.run_start, s.item_start, s.nchunks, s.num_runs,
-                                         plan.chunk, s.items);
+                                         plan.chunk, plan.bt.xbits, plan.bt.ybits, s.items);
     MTB_LAUNCHED();
     k_bucket_bounds<<<blocks, 256, 0, st>>>(s.items, s.item_start, s.nchunks, s.num_runs, s.bounds, plan.bt.n,
                                             s.n_items);
@@ -2123,7 +2139,6 @@ static int prepare_grid(const mtb_grid_params *p, const GridPlan &plan, const fl
     if (p->merge == 1) {
         launch_gather<P, false>(p, blocks, st, R, s, vis, weights, flags, plan, nullptr, nullptr, 0);
         MTB_LAUNCHED();
-        (void)end_bit;
         return MTB_OK;
     }
     k_pad_bases<<<1, 1, 0, st>>>(conv_info, p->wplanes, T, s.pbase);
@@ -2137,7 +2152,6 @@ static int prepare_grid(const mtb_grid_params *p, const GridPlan &plan, const fl
         k_mark_runs<<<wb, 256, 0, st>>>(s.items, s.n_items, s.wpos);
         MTB_LAUNCHED();
     }
-    (void)end_bit;
     {
         // the expanded padded table the direct gridders read
         const int rows = plan.table_rows;
