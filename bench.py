@@ -734,6 +734,19 @@ def run_e2e(args, torch, dev, uvw_d, chans, imagers, images, samples_per_step, w
                 state["back"][c] = record(back)
         state["uvw_free"][n % 2] = record(comp)
 
+    # the host link's own rate, outside the timed region: pinned H2D copies of
+    # one channel's visibilities alone on the copy stream
+    vis_h, vis_d = host[0][1], bufs[0][1]
+    with torch.cuda.stream(copy):
+        vis_d.copy_(vis_h, non_blocking=True)
+        l0, l1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        l0.record(copy)
+        for _ in range(3):
+            vis_d.copy_(vis_h, non_blocking=True)
+        l1.record(copy)
+    torch.cuda.synchronize()
+    link_gbs = 3 * vis_h.numel() * vis_h.element_size() / (l0.elapsed_time(l1) * 1e-3) / 1e9
+
     step(0)
     torch.cuda.synchronize()
     if world > 1:
@@ -756,7 +769,9 @@ def run_e2e(args, torch, dev, uvw_d, chans, imagers, images, samples_per_step, w
     if not check <= 1e-5:
         raise RuntimeError("e2e image differs from the device path: rms/peak %g" % check)
     return {"value": job_throughput(samples_per_step, world, ms), "unit": "samples/s", "h2d_bytes_per_step": int(h2d),
-            "d2h_bytes_per_step": int(d2h), "ms_per_step": ms, "image_check_rms": check}
+            "d2h_bytes_per_step": int(d2h), "ms_per_step": ms, "image_check_rms": check,
+            "h2d_gbs": h2d / (ms * 1e-3) / 1e9, "h2d_link_gbs": link_gbs,
+            "h2d_link_note": "h2d_link_gbs: pinned copies of one channel's visibilities alone, before the timed region"}
 
 
 # ---------------------------------------------------------------- serving --
