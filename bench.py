@@ -370,6 +370,7 @@ def main():
     ap.add_argument("--no-serve", action="store_true", help="skip the request-stream measurement")
     ap.add_argument("--no-oracle", action="store_true", help="skip the FP64 oracle check of the first channel")
     ap.add_argument("--no-cube", action="store_true", help="skip the batched-cubes measurement")
+    ap.add_argument("--no-lsrk", action="store_true", help="skip the TOPO->LSRK frequency measurement")
     ap.add_argument("--no-ref-gpu", action="store_true",
                     help="reference arm: skip timing the reference's own gridding operators on the GPU")
     ap.add_argument("--cube-images", type=int, default=64)
@@ -606,6 +607,11 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu:
         same = reference_sample_gpu(args, spec, uvw, chans, kern, dl, torch, nt, dev)
 
+    # ---- TOPO -> LSRK frequencies of the workload's records (rank 0, one GPU)
+    lsrk = None
+    if rank == 0 and world == 1 and not args.no_lsrk:
+        lsrk = run_lsrk(torch, dev, nt, nbl, freqs)
+
     # ---- batched cubes and the request stream (rank 0, one GPU): the other
     # two configurations of the workload, measured after the main line
     cube, serve = None, None
@@ -652,6 +658,8 @@ def main():
             line["oracle_check"] = oracle
         if cube:
             line["cube"] = cube
+        if lsrk:
+            line["lsrk"] = lsrk
         if serve:
             line["serving"] = serve
         print(json.dumps(line), flush=True)
@@ -1103,6 +1111,52 @@ def run_serve(args, torch, dev):
                        "note": "all requests queued at once; plain = total samples / summed service times"},
         "datagen_s": t_gen,
     }
+
+
+def run_lsrk(torch, dev, nt, nbl, freqs, reps=5):
+    """mtb_lsrk_freq_over_c on the workload's rows: a MeasurementSet-order
+    TIME column (nt times x nbl baselines, 2 s apart), every channel, taken
+    in the baseline-major record order; CUDA events around each call on its
+    stream, outside the timed region.  Algorithmic bytes per call: the time
+    column (8 B per row), the index (4 B per record) and nu/c (4 B per record
+    and channel); the peak is MEASURED_PEAKS.json's copy bandwidth when the
+    file is there.  The oracle checks the records of 24 spread-out times."""
+    from mtb.lsrk import lsrk_freq_over_c
+    from oracle import lsrk_oracle as O
+    site, ra, dec = (5109360.133, 2006852.586, -3238948.127), 2.1, -0.7
+    t0 = 60389.0 * 86400.0
+    times = t0 + 2.0 * np.arange(nt)
+    t_rows = torch.from_numpy(times).to(dev).repeat_interleave(nbl)            # row = t * nbl + b
+    index = torch.arange(nt * nbl, device=dev, dtype=torch.int32).view(nt, nbl).t().contiguous().view(-1)
+    chan = np.asarray(freqs, np.float64)
+    st = torch.cuda.current_stream()
+    out = lsrk_freq_over_c(t_rows, chan, site, ra, dec, index=index)        # warm-up: plan, caches
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(reps)]
+    for a, b in ev:
+        a.record(st)
+        out = lsrk_freq_over_c(t_rows, chan, site, ra, dec, index=index)
+        b.record(st)
+    torch.cuda.synchronize()
+    ms = sorted(a.elapsed_time(b) for a, b in ev)[reps // 2]
+    rows = nt * nbl
+    nbytes = 8 * rows + 4 * rows + 4 * rows * len(chan)
+    pick = np.linspace(0, nt - 1, 24).astype(int)
+    got = out.view(len(chan), nbl, nt)[:, 0, pick].cpu().numpy()               # baseline 0 at the picked times
+    ref = O.lsrk_freq_over_c(times[pick], chan, site, ra, dec)
+    ulps = int(np.abs(got.view(np.int32).astype(np.int64) - ref.view(np.int32).astype(np.int64)).max())
+    same = bool((out.view(len(chan), nbl, nt) == out.view(len(chan), nbl, nt)[:, :1, :]).all())
+    peak, src = None, None
+    pk = os.path.join(os.path.dirname(os.path.abspath(__file__)), "MEASURED_PEAKS.json")
+    if os.path.exists(pk):
+        with open(pk) as fh:
+            peak, src = json.load(fh).get("hbm_gbs"), "MEASURED_PEAKS.json hbm_gbs (copy)"
+    gbs = nbytes / (ms * 1e-3) / 1e9
+    del out, t_rows, index
+    torch.cuda.empty_cache()
+    return {"rows": rows, "channels": len(chan), "ms": ms, "algorithmic_bytes": nbytes, "achieved_gbs": gbs,
+            "peak_gbs": peak, "frac": gbs / peak if peak else None, "peak_source": src,
+            "oracle_max_ulps": ulps, "every_baseline_same_per_time": same,
+            "kernels": "k_lsrk_heads (FP64 velocity per distinct time) + CUB max-scan + k_lsrk_write"}
 
 
 def oracle_check(spec, dl, uvw_d, chan, image_d, kern):

@@ -281,6 +281,42 @@ int mtb_sort_index(const int *antenna1, const int *antenna2, int nrows, int nant
 int mtb_gather_rows(const void *in, size_t in_stride, size_t offset, size_t row_bytes, const int *index, int n,
                     void *out, int threads);
 
+/* ------------------------------------------------ LSRK frequencies (device) */
+/* Observer and epoch of the TOPO -> LSRK conversion. */
+typedef struct mtb_lsrk_params {
+    double site_itrf[3];     /* observatory position, ITRF metres (what MeasTable::Observatory gives) */
+    double ra, dec;          /* phase centre, J2000, radians                                        */
+    double tt_minus_time;    /* TT minus the time scale of time_s, seconds: 69.184 for UTC since
+                                2017-01-01, 32.184 for TAI                                          */
+    double ut1_minus_time;   /* UT1 minus the time scale of time_s, seconds (DUT1 for UTC, < 0.9 s) */
+} mtb_lsrk_params;
+
+/* Workspace bytes of mtb_lsrk_freq_over_c for nrows rows. */
+int mtb_lsrk_workspace_size(int nrows, size_t *bytes);
+
+/* Channel frequencies converted from TOPO to LSRK per record, as nu/c in
+ * float32: the per-record frequency column PreProcessUVW takes.  Replaces
+ * FrequencyConverter (code/mt-imager/lib/components/VisibilityManager/
+ * FrequencyConverter.cpp:112-140), which evaluates casacore's
+ * MFrequency::Convert(TOPO -> LSRK) once per distinct consecutive record time
+ * and stores (float)(nu_LSRK / c).  casacore's measures are not used: the
+ * observer's velocity with respect to the kinematic LSR (Earth rotation,
+ * Earth's barycentric motion from published mean elements, 20 km/s solar
+ * motion towards 18h +30 deg B1900) is computed in FP64 on the device, once
+ * per record whose time differs from the previous record's.
+ *   time_s   device double [nrows]: MJD seconds (the MeasurementSet TIME
+ *            column), in the row order the time-sharing is detected in
+ *   chan_hz  device double [nchan]: TOPO channel frequencies, Hz
+ *   index    device int [n] or NULL: out[.][k] is for row index[k] (the
+ *            baseline-major record order of mtb_sort_index); NULL: n == nrows
+ *            and row k; an index outside [0, nrows) writes NaN
+ *   out      device float [nchan][n]: nu_LSRK / c, m^-1
+ * Enqueued on `stream`; the workspace (mtb_lsrk_workspace_size) is in use
+ * until the stream reaches the end of the call. */
+int mtb_lsrk_freq_over_c(const mtb_lsrk_params *params, const double *time_s, int nrows, const double *chan_hz,
+                         int nchan, const int *index, int n, float *out, void *workspace, size_t workspace_bytes,
+                         mtb_stream_t stream);
+
 /* Gridder knobs the autotuner chooses among (fields of mtb_grid_params). */
 typedef struct mtb_grid_tuning {
     int tile;             /* bin tile edge                                            */

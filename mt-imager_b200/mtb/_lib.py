@@ -39,7 +39,7 @@ EXPORTS = (
     "mtb_taper_kernel_build", "mtb_grid_batch_workspace_size", "mtb_grid_batch",
     "mtb_grid_autotune_workspace_size", "mtb_grid_autotune", "mtb_grid_autotune_candidate_count", "mtb_sort_index", "mtb_gather_rows", "mtb_fits_create", "mtb_fits_write_channel", "mtb_fits_close",
     "mtb_engine_create", "mtb_engine_submit", "mtb_engine_wait", "mtb_engine_cancel", "mtb_engine_request_bytes",
-    "mtb_engine_destroy", "mtb_bounds_status",
+    "mtb_engine_destroy", "mtb_bounds_status", "mtb_lsrk_workspace_size", "mtb_lsrk_freq_over_c",
 )
 
 
@@ -54,6 +54,11 @@ class WKernelParams(ctypes.Structure):
     _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("l_increment", ctypes.c_double),
                 ("m_increment", ctypes.c_double), ("wplanes", ctypes.c_int), ("sampling", ctypes.c_int),
                 ("trial_support", ctypes.c_int), ("max_support", ctypes.c_int), ("w_max", ctypes.c_double)]
+
+
+class LsrkParams(ctypes.Structure):
+    _fields_ = [("site_itrf", ctypes.c_double * 3), ("ra", ctypes.c_double), ("dec", ctypes.c_double),
+                ("tt_minus_time", ctypes.c_double), ("ut1_minus_time", ctypes.c_double)]
 
 
 class WKernelInfo(ctypes.Structure):
@@ -178,6 +183,8 @@ def load(path: str = LIB_PATH):
     L.mtb_bounds_status.argtypes = [ctypes.POINTER(i), ctypes.POINTER(ctypes.c_uint)]
     L.mtb_engine_request_bytes.argtypes = [p, ctypes.POINTER(ImageRequest), ctypes.POINTER(sz)]
     L.mtb_engine_destroy.argtypes = [p]
+    L.mtb_lsrk_workspace_size.argtypes = [i, ctypes.POINTER(sz)]
+    L.mtb_lsrk_freq_over_c.argtypes = [ctypes.POINTER(LsrkParams), p, i, p, i, p, i, p, p, sz, p]
     _lib = L
     return L
 

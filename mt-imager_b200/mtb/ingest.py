@@ -15,12 +15,17 @@ main-table columns:
 * ``flag``                    bool [R][nchan][npol]
 * ``chan_freq``               float64 [nchan] Hz
 * ``n_antennas``              int (optional; max antenna id + 1 otherwise)
+* ``time``                    float64 [R] MJD seconds (optional; the MS TIME column)
+* ``site_itrf``               float64 [3] observatory ITRF metres (optional)
+* ``phase_dir``               float64 [2] phase centre RA, Dec J2000 radians (optional)
 
 Rows may be in any order (a MeasurementSet is usually time-major);
 autocorrelations are dropped.  The sort and the column gathers run in the
 library (mtb_sort_index, mtb_gather_rows: host code, threads, no GPU).
-Frequencies are taken as given (no TOPO->LSRK conversion, which needs
-casacore's measures): nu/c of a record is chan_freq / c.
+``RecordFile.channel`` takes the frequencies as given (nu/c of a record is
+chan_freq / c); ``RecordFile.lsrk_freq_over_c`` converts them from TOPO to
+LSRK per record on the GPU (mtb.lsrk, FrequencyConverter's part) when the
+file holds the time, site and phase-centre columns.
 """
 from __future__ import annotations
 
@@ -92,6 +97,11 @@ class RecordFile:
             raise ValueError("flag must match data, weight must be [R][npol]")
         if self.chan_freq.shape != (self.nchan,):
             raise ValueError("chan_freq must be [nchan]")
+        self.time = np.ascontiguousarray(z["time"], np.float64) if "time" in z else None
+        self.site_itrf = np.asarray(z["site_itrf"], np.float64) if "site_itrf" in z else None
+        self.phase_dir = np.asarray(z["phase_dir"], np.float64) if "phase_dir" in z else None
+        if self.time is not None and self.time.shape != (R,):
+            raise ValueError("time must be [R]")
         self.index = sort_index(self.antenna1, self.antenna2, self.n_antennas)
         self.nrec = int(self.index.size)
         self._uvw_sorted = None
@@ -120,6 +130,18 @@ class RecordFile:
         freq = np.full(self.nrec, self.chan_freq[chan] / C_LIGHT, np.float32)
         return freq, vis, self.weights(), flags
 
+    def lsrk_freq_over_c(self, device="cuda", stream=None, **kw):
+        """float32 device tensor [nchan][nrec]: every channel's nu/c converted
+        from TOPO to LSRK per record, in record order (FrequencyConverter:
+        the conversion runs over the rows in file order, where equal
+        consecutive times share one evaluation, and the result is taken in
+        the sort index's order)."""
+        if self.time is None or self.site_itrf is None or self.phase_dir is None:
+            raise ValueError("the record file has no time, site_itrf or phase_dir column")
+        from .lsrk import lsrk_freq_over_c
+        return lsrk_freq_over_c(self.time, self.chan_freq, self.site_itrf, self.phase_dir[0], self.phase_dir[1],
+                                index=self.index, device=device, stream=stream, **kw)
+
     def chunks(self, chan, chunk_records):
         """(uvw, freq, vis, weights, flags) of one channel in record chunks."""
         uvw = self.uvw()
@@ -129,10 +151,12 @@ class RecordFile:
             yield (np.ascontiguousarray(uvw[:, a:b]), freq[a:b], vis[a:b], wts[a:b], flags[a:b])
 
 
-def write_record_file(path, obs, autocorrelations=True):
+def write_record_file(path, obs, autocorrelations=True, time_s=None, site_itrf=None, phase_dir=None):
     """Write a synthetic observation (mtb.synth, baseline-major) as a record
     file in time-major row order, the usual MeasurementSet order, with an
-    autocorrelation row per antenna and time (dropped again on ingest)."""
+    autocorrelation row per antenna and time (dropped again on ingest).
+    ``time_s`` (MJD seconds per time sample), ``site_itrf`` and ``phase_dir``
+    add the columns the TOPO -> LSRK conversion needs."""
     from .synth import baseline_order
     n_ant = obs.meta["n_ant"]
     pairs = baseline_order(n_ant)
@@ -164,5 +188,15 @@ def write_record_file(path, obs, autocorrelations=True):
         na1[cross], na2[cross] = a1, a2
         nuvw[cross], ndata[cross], nflag[cross], nweight[cross] = uvw, data, flag, weight
         a1, a2, uvw, data, flag, weight = na1, na2, nuvw, ndata, nflag, nweight
+    extra = {}
+    if time_s is not None:
+        time_s = np.asarray(time_s, np.float64)
+        if time_s.shape != (nt,):
+            raise ValueError("time_s needs one time per time sample")
+        extra["time"] = np.repeat(time_s, a1.size // nt)
+    if site_itrf is not None:
+        extra["site_itrf"] = np.asarray(site_itrf, np.float64)
+    if phase_dir is not None:
+        extra["phase_dir"] = np.asarray(phase_dir, np.float64)
     np.savez(path, antenna1=a1, antenna2=a2, uvw=uvw, data=data, weight=weight, flag=flag,
-             chan_freq=np.asarray(obs.freqs_hz, np.float64), n_antennas=n_ant)
+             chan_freq=np.asarray(obs.freqs_hz, np.float64), n_antennas=n_ant, **extra)
