@@ -456,12 +456,18 @@ def main():
     # (per row and polarisation) and hands the same array to each channel
     # (MSVisibilityDataSetAsync.cpp:262-271)
     weights = torch.ones((R, 4), dtype=torch.float32, device=dev)
+    # nu/c of every record and channel comes from the TIME column (MS row
+    # order: row = t * nbl + b, 2 s apart) through the TOPO -> LSRK conversion
+    # (mtb_lsrk_freq_over_c), taken in the baseline-major record order
+    # (record k = b * nt + t) -- once per step, on the device
+    mscol = lsrk_inputs(torch, dev, spec, nbl, nt, freqs)
+    nu = torch.empty((len(freqs), R), dtype=torch.float32, device=dev)
+    mscol["run"](mscol["time"], mscol["index"], nu)
     for c, f in enumerate(freqs):
         vis = make_vis(uvw, f, srcs, torch, gen)
         # one byte per flag (mtb_grid_params.flags_u8): a quarter of the int32 layout's bytes to move
         flags = (torch.rand(R, device=dev, generator=gen) < spec["flag"]).to(torch.uint8)[:, None].repeat(1, 4).contiguous()
-        freq = torch.full((R,), f / C_LIGHT, dtype=torch.float32, device=dev)
-        chans.append((freq, vis, weights, flags))
+        chans.append((nu[c], vis, weights, flags))
     torch.cuda.synchronize()
     t_gen = time.perf_counter() - t_gen
 
@@ -493,6 +499,7 @@ def main():
     streams = [main_stream] + [torch.cuda.Stream(device=dev) for _ in range(max(1, args.streams) - 1)]
 
     def step(record_latency=True):
+        mscol["run"](mscol["time"], mscol["index"], nu)
         begin = torch.cuda.Event()
         begin.record(main_stream)
         for st in streams[1:]:
@@ -587,7 +594,7 @@ def main():
             dist.all_reduce(flag, op=dist.ReduceOp.MIN)
             fits = bool(flag.item())
         if fits:
-            e2e = run_e2e(args, torch, dev, uvw, chans, imagers, images, samples_per_step, world, dist)
+            e2e = run_e2e(args, torch, dev, uvw, chans, imagers, images, samples_per_step, world, dist, mscol)
         else:
             e2e = {"value": None, "skipped": "pinned host copies of %d ranks (%.0f GB) exceed 60 %% of the host's "
                                           "available memory" % (local_ranks, pinned * local_ranks / 1e9)}
@@ -634,7 +641,8 @@ def main():
             "warmup": max(3, args.warmup), "ms_per_step": ms_per_step, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32 (FP64 coordinates and w-phase)",
             "data": "synthetic (seeded earth-rotation tracks, point-source sky; one weights array shared by the "
-                    "channels, as the MS WEIGHT column)",
+                    "channels, as the MS WEIGHT column; nu/c of every record and channel converted TOPO -> LSRK "
+                    "from the TIME column on the device every step)",
             "config": {"workload": workload_name(spec), "records_per_channel": R, "channels": len(freqs),
                        "image": n, "cell_arcsec": dl / ARCSEC, "wplanes": spec["wplanes"],
                        "sampling": spec["sampling"], "supports": [int(sup.min()), int(sup.max())],
@@ -667,11 +675,13 @@ def main():
         dist.destroy_process_group()
 
 
-def run_e2e(args, torch, dev, uvw_d, chans, imagers, images, samples_per_step, world, dist):
+def run_e2e(args, torch, dev, uvw_d, chans, imagers, images, samples_per_step, world, dist, mscol):
     """Same metric through the public API from pinned host buffers: per step
     the H2D copy of every channel's records (and of the arrays the channels
-    share: uvw and the weights) and the D2H of every image are inside the
-    timed region.  H2D copies run on a side stream,
+    share: uvw, the weights, the TIME column and the record order) and the
+    D2H of every image are inside the timed region; nu/c of every channel is
+    computed on the device from the TIME column (mtb_lsrk_freq_over_c), as
+    the MeasurementSet holds no per-record frequency column.  H2D copies run on a side stream,
     double-buffered against the compute of the previous channel; each image's
     D2H runs on a third stream once it is finalised.  Steps follow each other
     without a device drain (a streaming imager): events guard every buffer
@@ -684,8 +694,12 @@ def run_e2e(args, torch, dev, uvw_d, chans, imagers, images, samples_per_step, w
     shared_w = all(ch[2] is chans[0][2] for ch in chans)
     host_uvw = pinned(uvw_d)
     host_w = pinned(chans[0][2]) if shared_w else None
-    # per channel: freq, vis, flags (and weights when the channels do not share them)
-    host = [[pinned(t) for t in ((f, v, fl) if shared_w else (f, v, w, fl))] for (f, v, w, fl) in chans]
+    host_time, host_index = pinned(mscol["time"]), pinned(mscol["index"])
+    time_bufs = [torch.empty_like(mscol["time"]) for _ in range(2)]
+    index_bufs = [torch.empty_like(mscol["index"]) for _ in range(2)]
+    nu_bufs = [torch.empty((len(chans), uvw_d.shape[1]), dtype=torch.float32, device=dev) for _ in range(2)]
+    # per channel: vis, flags (and weights when the channels do not share them)
+    host = [[pinned(t) for t in ((v, fl) if shared_w else (v, w, fl))] for (f, v, w, fl) in chans]
     out_host = [torch.empty(im.shape, dtype=im.dtype, pin_memory=True) for im in images]
     bufs = [[torch.empty(t.shape, dtype=t.dtype, device=dev) for t in host[0]] for _ in range(2)]
     uvw_bufs = [torch.empty_like(uvw_d) for _ in range(2)]
@@ -693,28 +707,52 @@ def run_e2e(args, torch, dev, uvw_d, chans, imagers, images, samples_per_step, w
     copy = torch.cuda.Stream(device=dev)
     back = torch.cuda.Stream(device=dev)
     comp = torch.cuda.current_stream(dev)
-    h2d = host_uvw.numel() * 4 + (host_w.numel() * 4 if shared_w else 0) + \
-        sum(sum(t.numel() * t.element_size() for t in hc) for hc in host)
+    h2d = host_uvw.numel() * 4 + (host_w.numel() * 4 if shared_w else 0) + host_time.numel() * 8 + \
+        host_index.numel() * 4 + sum(sum(t.numel() * t.element_size() for t in hc) for hc in host)
     d2h = sum(o.numel() * 4 for o in out_host)
     ref_image = images[-1].clone()          # the device path's image of the last channel
     # events: buffer pair free (last gridding that read it done), uvw buffer
     # free, image c read back
-    state = dict(seq=0, free=[None, None], uvw_free=[None, None], back=[None] * len(host))
+    state = dict(seq=0, free=[None, None], uvw_free=[None, None], back=[None] * len(host), shared={})
 
     def record(stream):
         e = torch.cuda.Event()
         e.record(stream)
         return e
 
-    def step(n):
-        ub = uvw_bufs[n % 2]
-        wb = w_bufs[n % 2] if shared_w else None
+    def shared_pairs(p):
+        pairs = [(time_bufs[p], host_time), (index_bufs[p], host_index), (uvw_bufs[p], host_uvw)]
+        return pairs + ([(w_bufs[p], host_w)] if shared_w else [])
+
+    def shared_copy(n, part=0, parts=1):
+        """H2D of step n's shared arrays (TIME, record order, uvw, weights)
+        into the buffers of its parity once step n - 2 has released them,
+        whole or as slice `part` of `parts` of every array."""
+        p = n % 2
         with torch.cuda.stream(copy):
-            if state["uvw_free"][n % 2] is not None:
-                copy.wait_event(state["uvw_free"][n % 2])
-            ub.copy_(host_uvw, non_blocking=True)
-            if shared_w:
-                wb.copy_(host_w, non_blocking=True)
+            if part == 0 and state["uvw_free"][p] is not None:
+                copy.wait_event(state["uvw_free"][p])
+            for dst, src in shared_pairs(p):
+                d, h = dst.view(-1), src.view(-1)
+                a, b = d.numel() * part // parts, d.numel() * (part + 1) // parts
+                d[a:b].copy_(h[a:b], non_blocking=True)
+            if part == parts - 1:
+                state["shared"][n] = record(copy)
+
+    def step(n, prefetch_next):
+        """Step n; with prefetch_next, step n + 1's shared arrays follow this
+        step's channel copies on the copy stream in slices (one after each
+        channel from the second on), so that no whole-array copy stands
+        between one step's last channel and the next step's first."""
+        p = n % 2
+        ub = uvw_bufs[p]
+        wb = w_bufs[p] if shared_w else None
+        tb, ib, nub = time_bufs[p], index_bufs[p], nu_bufs[p]
+        nch = len(host)
+        if n not in state["shared"]:
+            shared_copy(n)
+        comp.wait_event(state["shared"].pop(n))
+        mscol["run"](tb, ib, nub)
         for c, hc in enumerate(host):
             k = state["seq"] % 2
             state["seq"] += 1
@@ -725,13 +763,15 @@ def run_e2e(args, torch, dev, uvw_d, chans, imagers, images, samples_per_step, w
                 for dst, src in zip(b, hc):
                     dst.copy_(src, non_blocking=True)
                 ready = record(copy)
+            if prefetch_next and (nch == 1 or c >= 1):
+                shared_copy(n + 1, 0 if nch == 1 else c - 1, 1 if nch == 1 else nch - 1)
             comp.wait_event(ready)
             im = imagers[c]
             im.reset()
             if shared_w:
-                im.grid_device(ub, b[0], b[1], wb, b[2])
+                im.grid_device(ub, nub[c], b[0], wb, b[1])
             else:
-                im.grid_device(ub, *b)
+                im.grid_device(ub, nub[c], *b)
             state["free"][k] = record(comp)
             if state["back"][c] is not None:
                 comp.wait_event(state["back"][c])      # images[c] of the last step is on the host
@@ -740,11 +780,11 @@ def run_e2e(args, torch, dev, uvw_d, chans, imagers, images, samples_per_step, w
             with torch.cuda.stream(back):
                 out_host[c].copy_(images[c], non_blocking=True)
                 state["back"][c] = record(back)
-        state["uvw_free"][n % 2] = record(comp)
+        state["uvw_free"][p] = record(comp)
 
     # the host link's own rate, outside the timed region: pinned H2D copies of
     # one channel's visibilities alone on the copy stream
-    vis_h, vis_d = host[0][1], bufs[0][1]
+    vis_h, vis_d = host[0][0], bufs[0][0]
     with torch.cuda.stream(copy):
         vis_d.copy_(vis_h, non_blocking=True)
         l0, l1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -755,15 +795,17 @@ def run_e2e(args, torch, dev, uvw_d, chans, imagers, images, samples_per_step, w
     torch.cuda.synchronize()
     link_gbs = 3 * vis_h.numel() * vis_h.element_size() / (l0.elapsed_time(l1) * 1e-3) / 1e9
 
-    step(0)
+    step(0, False)
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     a.record()
+    # every timed step's shared arrays are copied inside the timed region:
+    # step 1 its own, steps 2..K by their predecessors
     for n in range(1, args.e2e_steps + 1):
-        step(n)
+        step(n, n < args.e2e_steps)
     for e in state["back"]:
         comp.wait_event(e)
     b.record()
@@ -1111,6 +1153,29 @@ def run_serve(args, torch, dev):
                        "note": "all requests queued at once; plain = total samples / summed service times"},
         "datagen_s": t_gen,
     }
+
+
+LSRK_SITE = (5109360.133, 2006852.586, -3238948.127)   # ITRF metres of a site at latitude -30.7 deg
+LSRK_T0 = 60389.0 * 86400.0                              # MJD seconds of the first time sample
+
+
+def lsrk_inputs(torch, dev, spec, nbl, nt, freqs):
+    """The TIME column of the workload's rows in MeasurementSet order (row =
+    t * nbl + b, spec["dt"] apart), the record order that takes them to the
+    baseline-major records (record b * nt + t is row t * nbl + b), the
+    channel frequencies, and a call that writes nu/c [nchan][R] from them on
+    the current stream with a reused workspace."""
+    from mtb.lsrk import lsrk_freq_over_c, lsrk_workspace_bytes
+    times = LSRK_T0 + spec["dt"] * torch.arange(nt, dtype=torch.float64, device=dev)
+    time_rows = times.repeat_interleave(nbl)
+    index = torch.arange(nt * nbl, device=dev, dtype=torch.int32).view(nt, nbl).t().contiguous().view(-1)
+    chan = torch.tensor(np.asarray(freqs, np.float64), device=dev)
+    ws = torch.empty(lsrk_workspace_bytes(nt * nbl), dtype=torch.uint8, device=dev)
+    ra, dec = 1.2, math.radians(spec["dec"])
+
+    def run(time_s, idx, out):
+        return lsrk_freq_over_c(time_s, chan, LSRK_SITE, ra, dec, index=idx, device=dev, out=out, workspace=ws)
+    return {"time": time_rows, "index": index, "run": run}
 
 
 def run_lsrk(torch, dev, nt, nbl, freqs, reps=5):

@@ -32,6 +32,7 @@
 // "head", the reference's `time_storage[recordNo] != last_time` test)
 // evaluates the velocity once; an inclusive max-scan hands every record its
 // head; a last kernel writes nu/c per channel in the caller's record order.
+#include <algorithm>
 #include <cmath>
 
 #include <cub/cub.cuh>
@@ -135,21 +136,6 @@ __device__ V3 moon_position(double T) {
     return ecl_to_eq({r * cos(bet) * cos(lam), r * cos(bet) * sin(lam), r * sin(bet)});
 }
 
-// Barycentric J2000 equatorial position of the Earth (au).
-__device__ V3 earth_position(double T) {
-    V3 emb = kepler_position(0, T);
-    double mtot = 1.0;
-    V3 sun = {0, 0, 0};   // -sum(m_p r_p) over the bodies, heliocentric, in units of the Sun's mass
-    for (int b = 0; b < 5; b++) {
-        const double m = 1.0 / kSunOverMass[b];
-        const V3 p = b == 0 ? emb : kepler_position(b, T);
-        sun = sub(sun, scale(p, m));
-        mtot += m;
-    }
-    sun = scale(sun, 1.0 / mtot);
-    return sub(add(emb, sun), scale(moon_position(T), kMoonFraction));
-}
-
 // IAU 1976 precession matrix from epoch jd0 to epoch jd1 (rows: x, y, z of
 // the target frame in the source frame's coordinates).
 __device__ void precession(double jd0, double jd1, double m[3][3]) {
@@ -180,79 +166,178 @@ __device__ __forceinline__ V3 mul_t(const double m[3][3], V3 v) {
             m[0][2] * v.x + m[1][2] * v.y + m[2][2] * v.z};
 }
 
-// nu_LSRK / nu_TOPO at one record time (MJD seconds of the caller's scale).
-__device__ double doppler_factor(const mtb_lsrk_params &p, double time_s) {
+// Sun / body mass of the barycentre's bodies, summed once: 1 + sum(m_b / M_sun)
+__device__ __forceinline__ double total_mass() {
+    double m = 1.0;
+#pragma unroll
+    for (int b = 0; b < 5; b++) m += 1.0 / kSunOverMass[b];
+    return m;
+}
+
+// One warp per distinct time: the terms of the observer's velocity (m/s,
+// J2000 equator) are spread over lanes and summed by shuffles.
+//   lanes 0..9:   body b = lane / 2 at T + h (even lane) or T - h (odd): its
+//                 heliocentric position times its weight in the Earth's
+//                 barycentric position (EMB: 1 - m/M, the others: -m/M, the
+//                 Sun's barycentric offset), +-1/(2h) for the central difference
+//   lanes 10, 11: the Moon at T + h, T - h, weight -m_Moon / (m_E + m_M)
+//   lane 12:      the site's rotation velocity (GMST, precession date -> J2000)
+//   lane 13:      the solar motion, 20 km/s towards the B1900 apex
+// Lane 0 turns the sum into nu_LSRK / nu_TOPO for the phase centre.
+__device__ double observer_term(const mtb_lsrk_params &p, double time_s, int lane, V3 &v) {
     const double jd_tt = 2400000.5 + (time_s + p.tt_minus_time) / kDay;
-    const double jd_ut1 = 2400000.5 + (time_s + p.ut1_minus_time) / kDay;
     const double T = (jd_tt - kJ2000) / 36525.0;
-    // Earth's barycentric velocity (m/s), J2000 equator
     const double h = kHalfStepDays / 36525.0;
-    const V3 ve = scale(sub(earth_position(T + h), earth_position(T - h)), kAU / (2.0 * kHalfStepDays * kDay));
-    // the site's rotation velocity in the mean equator of date, then in J2000
-    const double du = jd_ut1 - kJ2000, Tu = du / 36525.0;
-    double gmst = fmod(280.46061837 + 360.98564736629 * du + 0.000387933 * Tu * Tu - Tu * Tu * Tu / 38710000.0, 360.0);
-    gmst *= kDeg;
-    const double omega = 360.98564736629 * kDeg / kDay;
-    const double cg = cos(gmst), sg = sin(gmst);
-    const V3 r = {cg * p.site_itrf[0] - sg * p.site_itrf[1], sg * p.site_itrf[0] + cg * p.site_itrf[1], p.site_itrf[2]};
-    double P[3][3];
-    precession(kJ2000, jd_tt, P);
-    const V3 vd = mul_t(P, {-omega * r.y, omega * r.x, 0.0});
-    // the Sun's motion with respect to the LSRK
-    double Q[3][3];
-    precession(kB1900, kJ2000, Q);
-    const double a0 = 270.0 * kDeg, d0 = 30.0 * kDeg;
-    const V3 apex = mul(Q, {cos(d0) * cos(a0), cos(d0) * sin(a0), sin(d0)});
-    const V3 v = add(add(ve, vd), scale(apex, kLsrSpeed));
+    const double dscale = kAU / (2.0 * kHalfStepDays * kDay);   // au per 2h -> m/s
+    v = {0.0, 0.0, 0.0};
+    if (lane < 10) {
+        const int b = lane >> 1;
+        const double sgn = (lane & 1) ? -1.0 : 1.0;
+        const double w = (b == 0 ? 1.0 : 0.0) - 1.0 / (kSunOverMass[b] * total_mass());
+        v = scale(kepler_position(b, T + sgn * h), sgn * w * dscale);
+    } else if (lane < 12) {
+        const double sgn = lane == 10 ? 1.0 : -1.0;
+        v = scale(moon_position(T + sgn * h), -sgn * kMoonFraction * dscale);
+    } else if (lane == 12) {
+        const double jd_ut1 = 2400000.5 + (time_s + p.ut1_minus_time) / kDay;
+        const double du = jd_ut1 - kJ2000, Tu = du / 36525.0;
+        double gmst =
+            fmod(280.46061837 + 360.98564736629 * du + 0.000387933 * Tu * Tu - Tu * Tu * Tu / 38710000.0, 360.0);
+        gmst *= kDeg;
+        const double omega = 360.98564736629 * kDeg / kDay;
+        const double cg = cos(gmst), sg = sin(gmst);
+        const V3 r = {cg * p.site_itrf[0] - sg * p.site_itrf[1], sg * p.site_itrf[0] + cg * p.site_itrf[1],
+                      p.site_itrf[2]};
+        double P[3][3];
+        precession(kJ2000, jd_tt, P);
+        v = mul_t(P, {-omega * r.y, omega * r.x, 0.0});
+    } else if (lane == 13) {
+        double Q[3][3];
+        precession(kB1900, kJ2000, Q);
+        const double a0 = 270.0 * kDeg, d0 = 30.0 * kDeg;
+        v = scale(mul(Q, {cos(d0) * cos(a0), cos(d0) * sin(a0), sin(d0)}), kLsrSpeed);
+    }
+    // butterfly sum: lane pairs first, so each body's central difference is
+    // formed before the bodies are added
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        v.x += __shfl_xor_sync(0xFFFFFFFFu, v.x, o);
+        v.y += __shfl_xor_sync(0xFFFFFFFFu, v.y, o);
+        v.z += __shfl_xor_sync(0xFFFFFFFFu, v.z, o);
+    }
     const V3 n = {cos(p.dec) * cos(p.ra), cos(p.dec) * sin(p.ra), sin(p.dec)};
     const double bn = dot(v, n) / kC, b2 = dot(v, v) / (kC * kC);
     return sqrt(1.0 - b2) / (1.0 + bn);
 }
 
-// heads: a record whose time differs from the previous record's evaluates
-// its factor; marks = its own index there, 0 elsewhere (scanned with max next)
-__global__ void k_lsrk_heads(mtb_lsrk_params p, const double *__restrict__ time_s, int nrows, int *__restrict__ marks,
-                             double *__restrict__ factor) {
-    const int r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= nrows) return;
-    const double t = time_s[r];
-    const bool head = r == 0 || !(t == time_s[r - 1]);
-    marks[r] = head ? r : 0;
-    if (head) factor[r] = doppler_factor(p, t);
+__device__ __forceinline__ bool is_head(const double *__restrict__ time_s, int r) {
+    return r == 0 || !(time_s[r] == time_s[r - 1]);   // the reference's last_time test
 }
 
-struct MaxInt {
-    __host__ __device__ __forceinline__ int operator()(int a, int b) const { return a > b ? a : b; }
-};
+// flags: 1 where a row starts a run of equal times (a head)
+__global__ void k_lsrk_flags(const double *__restrict__ time_s, int nrows, int *__restrict__ flags) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r < nrows) flags[r] = is_head(time_s, r) ? 1 : 0;
+}
 
-// out[c][k] = (float)(chan_hz[c] * factor(row) / c) for row = index[k]
-// (k itself without an index); a row outside [0, nrows) gives NaN
+// rank = inclusive count of heads: the head of row r is heads[rank[r] - 1]
+__global__ void k_lsrk_heads(const double *__restrict__ time_s, int nrows, const int *__restrict__ rank,
+                             int *__restrict__ heads, int *__restrict__ nheads) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= nrows) return;
+    if (is_head(time_s, r)) heads[rank[r] - 1] = r;
+    if (r == nrows - 1) *nheads = rank[r];
+}
+
+// one warp per head (grid-stride over the device-side head count)
+__global__ void k_lsrk_eval(mtb_lsrk_params p, const double *__restrict__ time_s, const int *__restrict__ heads,
+                            const int *__restrict__ nheads, double *__restrict__ factor) {
+    const int lane = threadIdx.x & 31;
+    const int nw = gridDim.x * (blockDim.x >> 5);
+    const int nh = *nheads;
+    for (int h = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); h < nh; h += nw) {
+        V3 v;
+        const double f = observer_term(p, time_s[heads[h]], lane, v);
+        if (lane == 0) factor[h] = f;
+    }
+}
+
+// x / c rounded to nearest: the product with the rounded reciprocal and one
+// residual correction (Brisebarre, Muller and Raina, "Accelerating correctly
+// rounded floating-point division when the divisor is known in advance",
+// IEEE Trans. Computers 53(8), 2004); the residual x - q0 c is exact under FMA
+__device__ __forceinline__ double div_c(double x) {
+    constexpr double inv = 1.0 / kC;
+    const double q0 = x * inv;
+    const double e = fma(-q0, kC, x);
+    return fma(e, inv, q0);
+}
+
+// out[c][k] = (float)(chan_hz[c] * factor / c) for row = index[k] (k itself
+// without an index); a row outside [0, nrows) gives NaN.  VEC: 4 consecutive
+// records per thread, one 16-byte store per channel (n a multiple of 4 and
+// out 16-byte aligned); the four rows' gathers are independent loads in
+// flight together.  Streaming stores: the output is not read again here.
+__device__ __forceinline__ float lsrk_value(const double *__restrict__ chan_hz, int c, double f, bool ok) {
+    return ok ? (float)div_c(chan_hz[c] * f) : __int_as_float(0x7fc00000);
+}
+
+template <bool VEC>
 __global__ void k_lsrk_write(const double *__restrict__ chan_hz, int nchan, const int *__restrict__ index, int n,
-                             int nrows, const int *__restrict__ hidx, const double *__restrict__ factor,
+                             int nrows, const int *__restrict__ rank, const double *__restrict__ factor,
                              float *__restrict__ out) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= n) return;
-    const int row = index ? index[k] : k;
-    const bool ok = row >= 0 && row < nrows;
-    const double f = ok ? factor[hidx[row]] : 0.0;
-    for (int c = 0; c < nchan; c++)
-        out[(size_t)c * n + k] = ok ? (float)(chan_hz[c] * f / kC) : __int_as_float(0x7fc00000);
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if constexpr (VEC) {
+        const int k0 = 4 * t;
+        if (k0 >= n) return;
+        int row[4];
+        bool ok[4];
+        double f[4];
+        if (index) {
+            const int4 r4 = *reinterpret_cast<const int4 *>(index + k0);
+            row[0] = r4.x, row[1] = r4.y, row[2] = r4.z, row[3] = r4.w;
+        } else {
+#pragma unroll
+            for (int j = 0; j < 4; j++) row[j] = k0 + j;
+        }
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            ok[j] = row[j] >= 0 && row[j] < nrows;
+            f[j] = ok[j] ? factor[rank[row[j]] - 1] : 0.0;
+        }
+        for (int c = 0; c < nchan; c++) {
+            const float4 v = make_float4(lsrk_value(chan_hz, c, f[0], ok[0]), lsrk_value(chan_hz, c, f[1], ok[1]),
+                                         lsrk_value(chan_hz, c, f[2], ok[2]), lsrk_value(chan_hz, c, f[3], ok[3]));
+            __stcs(reinterpret_cast<float4 *>(out + (size_t)c * n + k0), v);
+        }
+    } else {
+        const int k = t;
+        if (k >= n) return;
+        const int row = index ? index[k] : k;
+        const bool ok = row >= 0 && row < nrows;
+        const double f = ok ? factor[rank[row] - 1] : 0.0;
+        for (int c = 0; c < nchan; c++) __stcs(out + (size_t)c * n + k, lsrk_value(chan_hz, c, f, ok));
+    }
 }
 
 struct Carve {
-    int *marks;     // head records: their own index, else 0
-    int *hidx;      // the head of every record (max-scan of marks)
-    double *factor;
+    int *flags;     // 1 at head rows
+    int *rank;      // inclusive count of heads
+    int *heads;     // head rows in order
+    int *nheads;    // head count (device)
+    double *factor; // nu_LSRK / nu_TOPO per head
     void *cub;
     size_t cub_bytes;
 };
 
 static int carve(int nrows, void *ws, size_t ws_bytes, Carve &c, size_t *total) {
     size_t cub_bytes = 0;
-    MTB_CUDA_TRY(cub::DeviceScan::InclusiveScan(nullptr, cub_bytes, (int *)nullptr, (int *)nullptr, MaxInt{}, nrows));
+    MTB_CUDA_TRY(cub::DeviceScan::InclusiveSum(nullptr, cub_bytes, (int *)nullptr, (int *)nullptr, nrows));
     Arena a(ws, ws_bytes);
-    c.marks = a.take<int>((size_t)nrows);
-    c.hidx = a.take<int>((size_t)nrows);
+    c.flags = a.take<int>((size_t)nrows);
+    c.rank = a.take<int>((size_t)nrows);
+    c.heads = a.take<int>((size_t)nrows);
+    c.nheads = a.take<int>(1);
     c.factor = a.take<double>((size_t)nrows);
     c.cub = a.take<char>(cub_bytes);
     c.cub_bytes = cub_bytes;
@@ -290,10 +375,24 @@ extern "C" int mtb_lsrk_freq_over_c(const mtb_lsrk_params *params, const double 
     MTB_TRY(carve(nrows, workspace, workspace_bytes, c, nullptr));
     cudaStream_t st = (cudaStream_t)stream;
     const int T = 256;
-    k_lsrk_heads<<<(nrows + T - 1) / T, T, 0, st>>>(p, time_s, nrows, c.marks, c.factor);
+    const int rb = (nrows + T - 1) / T;
+    k_lsrk_flags<<<rb, T, 0, st>>>(time_s, nrows, c.flags);
     MTB_LAUNCHED();
-    MTB_CUDA_TRY(cub::DeviceScan::InclusiveScan(c.cub, c.cub_bytes, c.marks, c.hidx, MaxInt{}, nrows, st));
-    k_lsrk_write<<<(n + T - 1) / T, T, 0, st>>>(chan_hz, nchan, index, n, nrows, c.hidx, c.factor, out);
+    MTB_CUDA_TRY(cub::DeviceScan::InclusiveSum(c.cub, c.cub_bytes, c.flags, c.rank, nrows, st));
+    k_lsrk_heads<<<rb, T, 0, st>>>(time_s, nrows, c.rank, c.heads, c.nheads);
+    MTB_LAUNCHED();
+    int dev = 0, sms = 148;
+    MTB_CUDA_TRY(cudaGetDevice(&dev));
+    MTB_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const int eval_blocks = std::min((nrows + 3) / 4, sms * 16);   // 4 warps per block, one head per warp
+    k_lsrk_eval<<<eval_blocks, 128, 0, st>>>(p, time_s, c.heads, c.nheads, c.factor);
+    MTB_LAUNCHED();
+    // 16-byte rows: n a multiple of 4, out and index 16-byte aligned
+    const bool vec = n % 4 == 0 && ((uintptr_t)out & 15) == 0 && ((uintptr_t)index & 15) == 0;
+    if (vec)
+        k_lsrk_write<true><<<(n / 4 + T - 1) / T, T, 0, st>>>(chan_hz, nchan, index, n, nrows, c.rank, c.factor, out);
+    else
+        k_lsrk_write<false><<<(n + T - 1) / T, T, 0, st>>>(chan_hz, nchan, index, n, nrows, c.rank, c.factor, out);
     MTB_LAUNCHED();
     return MTB_OK;
 }

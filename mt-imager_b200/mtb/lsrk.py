@@ -25,7 +25,7 @@ TT_MINUS_UTC = 69.184
 
 
 def lsrk_freq_over_c(time_s, chan_hz, site_itrf, ra, dec, index=None, tt_minus_time=TT_MINUS_UTC,
-                     ut1_minus_time=0.0, device="cuda", stream=None):
+                     ut1_minus_time=0.0, device="cuda", stream=None, out=None, workspace=None):
     """float32 tensor [nchan][n] on `device`: nu_LSRK / c per channel and record.
 
     time_s     MJD seconds per row (MeasurementSet TIME), [nrows]
@@ -34,6 +34,10 @@ def lsrk_freq_over_c(time_s, chan_hz, site_itrf, ra, dec, index=None, tt_minus_t
     ra, dec    phase centre, J2000 radians
     index      rows in output order (e.g. ``RecordFile.index``), or None for
                every row in its own order
+    out        optional float32 device tensor [nchan][n] to write into
+    workspace  optional uint8 device tensor of at least
+               ``lsrk_workspace_bytes(nrows)`` bytes (reused between calls on
+               one stream)
     """
     _require_cuda(device)
     lib = L.load()
@@ -53,10 +57,25 @@ def lsrk_freq_over_c(time_s, chan_hz, site_itrf, ra, dec, index=None, tt_minus_t
         p.site_itrf[k] = float(site[k])
     p.ra, p.dec = float(ra), float(dec)
     p.tt_minus_time, p.ut1_minus_time = float(tt_minus_time), float(ut1_minus_time)
-    nbytes = ctypes.c_size_t(0)
-    L.check(lib.mtb_lsrk_workspace_size(nrows, ctypes.byref(nbytes)), "mtb_lsrk_workspace_size")
-    ws = torch.empty(max(1, nbytes.value), dtype=torch.uint8, device=device)
-    out = torch.empty((nchan, n), dtype=torch.float32, device=device)
+    nbytes = lsrk_workspace_bytes(nrows)
+    if workspace is None:
+        workspace = torch.empty(max(1, nbytes), dtype=torch.uint8, device=device)
+    elif workspace.numel() * workspace.element_size() < nbytes or not workspace.is_cuda:
+        raise ValueError("workspace needs %d device bytes" % nbytes)
+    if out is None:
+        out = torch.empty((nchan, n), dtype=torch.float32, device=device)
+    elif (tuple(out.shape) != (nchan, n) or out.dtype != torch.float32 or not out.is_contiguous()
+          or not out.is_cuda):
+        raise ValueError("out must be a contiguous float32 device tensor [%d][%d]" % (nchan, n))
+    ws = workspace
     L.check(lib.mtb_lsrk_freq_over_c(ctypes.byref(p), _ptr(t), nrows, _ptr(ch), nchan, _ptr(idx), n, _ptr(out),
-                                     _ptr(ws), nbytes.value, _stream(stream)), "mtb_lsrk_freq_over_c")
+                                     _ptr(ws), ws.numel() * ws.element_size(), _stream(stream)),
+            "mtb_lsrk_freq_over_c")
     return out
+
+
+def lsrk_workspace_bytes(nrows):
+    """Device workspace bytes of one conversion over nrows rows."""
+    nbytes = ctypes.c_size_t(0)
+    L.check(L.load().mtb_lsrk_workspace_size(int(nrows), ctypes.byref(nbytes)), "mtb_lsrk_workspace_size")
+    return nbytes.value
