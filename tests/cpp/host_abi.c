@@ -5,7 +5,8 @@
  * calls the host-side entry points: the baseline-major record order of
  * mt-imager's visibility ingest (SortIndex.cpp:46-87) on a hand-made antenna
  * table, a column gather in that order (SortedStorage.h:205-246), the status
- * strings, and parameter refusals that happen before any device work.
+ * strings, and parameter refusals that happen before any device work
+ * (grid, engine, FITS and TOPO -> LSRK entry points).
  * Prints "ok" and exits 0 when every check holds.
  */
 #include <stdio.h>
@@ -88,6 +89,22 @@ int main(void)
     CHECK(mtb_engine_cancel(NULL, 1) == MTB_ERR_NULL);
     CHECK(strcmp(mtb_status_string(MTB_ERR_CANCELLED), "request cancelled") == 0);
     CHECK(mtb_fits_create(NULL, NULL, NULL) != MTB_OK);
+
+    /* TOPO -> LSRK conversion: the parameter block from C and its refusals */
+    mtb_lsrk_params lp;
+    memset(&lp, 0, sizeof(lp));
+    lp.site_itrf[0] = 5109360.133;
+    lp.site_itrf[1] = 2006852.586;
+    lp.site_itrf[2] = -3238948.127;
+    lp.ra = 1.2;
+    lp.dec = -0.8;
+    lp.tt_minus_time = 69.184;
+    size_t lws = 0;
+    CHECK(mtb_lsrk_workspace_size(-1, &lws) == MTB_ERR_BAD_PARAM);
+    CHECK(mtb_lsrk_freq_over_c(NULL, NULL, 1, NULL, 1, NULL, 1, NULL, NULL, 0, NULL) == MTB_ERR_NULL);
+    CHECK(mtb_lsrk_freq_over_c(&lp, NULL, 4, NULL, 1, NULL, 3, NULL, NULL, 0, NULL) == MTB_ERR_BAD_PARAM);
+    CHECK(mtb_lsrk_freq_over_c(&lp, NULL, 4, NULL, 0, NULL, 4, NULL, NULL, 0, NULL) == MTB_OK);
+    CHECK(mtb_lsrk_freq_over_c(&lp, NULL, 4, NULL, 2, NULL, 4, NULL, NULL, 0, NULL) == MTB_ERR_NULL);
 
     printf("ok\n");
     return 0;
