@@ -1613,22 +1613,27 @@ __device__ __forceinline__ void grid_job7(const GridJobDesc &J, const int first,
                     if (cell[j] >= 0 && cell[j] != last[j] && last[j] >= 0) flush_slot(j);
             }
             // Reset of the flushed slots by a packed multiply with 0 (1 keeps
-            // the sum): branch-free, so the accumulators keep their registers
-            // through the loop (an assignment under the branch above made the
-            // compiler copy every accumulator once per record).  It differs
-            // from an assignment only for a non-finite sum, which has already
-            // gone to the grid, where the inverse FFT spreads it over the whole
-            // image either way.
+            // the sum), so the accumulators keep their registers through the
+            // loop (an assignment under the branch above made the compiler
+            // copy every accumulator once per record; a select instead of the
+            // multiply measured 3.8 % slower).  It differs from an assignment
+            // only for a non-finite sum, which has already gone to the grid,
+            // where the inverse FFT spreads it over the whole image either
+            // way.  Skipped, warp-uniformly, when no lane's cell changes (a
+            // run that moves only across box rows the warp does not hold):
+            // 1.5 % faster on the 8 h mid-size channel.
+            if (__any_sync(0xFFFFFFFFu, chg)) {
 #pragma unroll
-            for (int j = 0; j < KS; j++) {
-                const bool c = cell[j] >= 0 && cell[j] != last[j];
-                const float kf = c ? 0.f : 1.f;
+                for (int j = 0; j < KS; j++) {
+                    const bool c = cell[j] >= 0 && cell[j] != last[j];
+                    const float kf = c ? 0.f : 1.f;
 #pragma unroll
-                for (int p = 0; p < P; p++) {
-                    acc[j][p] = __fmul2_rn(acc[j][p], make_float2(kf, kf));
-                    if (PR) accb[PR ? j : 0][p] = __fmul2_rn(accb[PR ? j : 0][p], make_float2(kf, kf));
+                    for (int p = 0; p < P; p++) {
+                        acc[j][p] = __fmul2_rn(acc[j][p], make_float2(kf, kf));
+                        if (PR) accb[PR ? j : 0][p] = __fmul2_rn(accb[PR ? j : 0][p], make_float2(kf, kf));
+                    }
+                    last[j] = c ? cell[j] : last[j];
                 }
-                last[j] = c ? cell[j] : last[j];
             }
             cend = i + max(1, rec(i).w >> 16);
         }
