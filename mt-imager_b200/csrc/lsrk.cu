@@ -184,7 +184,7 @@ __device__ __forceinline__ double total_mass() {
 //   lane 12:      the site's rotation velocity (GMST, precession date -> J2000)
 //   lane 13:      the solar motion, 20 km/s towards the B1900 apex
 // Lane 0 turns the sum into nu_LSRK / nu_TOPO for the phase centre.
-__device__ double observer_term(const mtb_lsrk_params &p, double time_s, int lane, V3 &v) {
+__device__ double warp_doppler_factor(const mtb_lsrk_params &p, double time_s, int lane, V3 &v) {
     const double jd_tt = 2400000.5 + (time_s + p.tt_minus_time) / kDay;
     const double T = (jd_tt - kJ2000) / 36525.0;
     const double h = kHalfStepDays / 36525.0;
@@ -257,7 +257,7 @@ __global__ void k_lsrk_eval(mtb_lsrk_params p, const double *__restrict__ time_s
     const int nh = *nheads;
     for (int h = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); h < nh; h += nw) {
         V3 v;
-        const double f = observer_term(p, time_s[heads[h]], lane, v);
+        const double f = warp_doppler_factor(p, time_s[heads[h]], lane, v);
         if (lane == 0) factor[h] = f;
     }
 }
