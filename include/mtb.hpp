@@ -10,6 +10,10 @@
  *                      compensated) and normaliser that chunks are gridded into,
  *                      then the Stokes image (WImager.cpp:167-290,
  *                      ImageFinalizer.cpp:31-65)
+ *   mtb::FrequencyConverter
+ *                      FrequencyConverter: nu/c per record and channel converted
+ *                      TOPO -> LSRK from the TIME column
+ *                      (VisibilityManager/FrequencyConverter.cpp:112-140)
  * Unlike the C ABI, these classes own their device memory: allocations are
  * stream-ordered (cudaMallocAsync / cudaFreeAsync on the object's stream), and
  * every call only enqueues work on that stream.  Errors throw mtb::Error.
@@ -246,6 +250,33 @@ private:
     bool fresh_ = true;
     std::unique_ptr<ImagerBuffers> own_;
     ImagerBuffers *b_ = nullptr;
+};
+
+// TOPO -> LSRK nu/c of every record and channel from the MeasurementSet TIME
+// column (mtb_lsrk_freq_over_c).  The workspace grows to the largest row count
+// seen and is reused; every call only enqueues work on the stream.
+class FrequencyConverter {
+public:
+    FrequencyConverter(const mtb_lsrk_params &params, cudaStream_t stream) : p_(params), s_(stream) {}
+
+    // time: device double [nrows] (MJD seconds, row order); chan_hz: device
+    // double [nchan]; index: device int [n] record order (nullptr: n == nrows);
+    // out: device float [nchan][n]
+    void convert(const double *time, int nrows, const double *chan_hz, int nchan, const int *index, int n,
+                 float *out) {
+        size_t need = 0;
+        check(mtb_lsrk_workspace_size(nrows, &need), "mtb_lsrk_workspace_size");
+        if (ws_.size() < need) ws_ = DeviceArray<unsigned char>(need, s_);
+        check(mtb_lsrk_freq_over_c(&p_, time, nrows, chan_hz, nchan, index, n, out, ws_.data(), ws_.bytes(),
+                                   (mtb_stream_t)s_),
+              "mtb_lsrk_freq_over_c");
+    }
+    const mtb_lsrk_params &params() const { return p_; }
+
+private:
+    mtb_lsrk_params p_;
+    cudaStream_t s_;
+    DeviceArray<unsigned char> ws_;
 };
 
 }  // namespace mtb

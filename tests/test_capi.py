@@ -106,9 +106,9 @@ def test_c_program_uses_the_abi(tmp_path, mtblib):
 
 
 def test_cpp_host_classes_compile():
-    """include/mtb.hpp (the C++ classes over the C ABI) and the C++ program
-    that uses them compile with g++ -std=c++17 on a machine without a GPU;
-    running the program is a GPU test."""
+    """include/mtb.hpp (the C++ classes over the C ABI) and the C++ programs
+    that use them compile with g++ -std=c++17 on a machine without a GPU;
+    running the programs is a GPU test."""
     import shutil
     import subprocess
     import pytest
@@ -116,8 +116,9 @@ def test_cpp_host_classes_compile():
     if shutil.which(cxx) is None:
         pytest.skip("no C++ compiler")
     cuda = os.environ.get("CUDA_HOME", "/usr/local/cuda")
-    r = subprocess.run([cxx, "-std=c++17", "-Wall", "-Werror", "-fsyntax-only",
-                        os.path.join(ROOT, "tests", "cpp", "image_one.cpp"),
-                        "-I", os.path.join(ROOT, "include"), "-I", os.path.join(cuda, "include")],
-                       capture_output=True, text=True, timeout=120)
-    assert r.returncode == 0, r.stderr
+    for prog in ("image_one.cpp", "lsrk_one.cpp"):
+        r = subprocess.run([cxx, "-std=c++17", "-Wall", "-Werror", "-fsyntax-only",
+                            os.path.join(ROOT, "tests", "cpp", prog),
+                            "-I", os.path.join(ROOT, "include"), "-I", os.path.join(cuda, "include")],
+                           capture_output=True, text=True, timeout=120)
+        assert r.returncode == 0, (prog, r.stderr)

@@ -188,3 +188,36 @@ def test_record_file_lsrk_frequencies_follow_the_record_order(tmp_path):
     got = rf.lsrk_freq_over_c().cpu().numpy()
     ref = O.lsrk_freq_over_c(rf.time, rf.chan_freq, MEERKAT, 0.3, 0.9, index=rf.index)
     assert got.shape == (rf.nchan, rf.nrec) and _ulps(got, ref).max() <= 1
+
+
+@pytest.mark.gpu
+def test_cpp_frequency_converter(tmp_path):
+    """tests/cpp/lsrk_one.cpp converts through mtb::FrequencyConverter
+    (include/mtb.hpp); its nu/c equals the oracle's to 1 ulp."""
+    import os
+    import subprocess
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    cxx = os.environ.get("CXX", "g++")
+    cuda = os.environ.get("CUDA_HOME", "/usr/local/cuda")
+    lib = os.path.join(root, "mt-imager_b200")
+    exe = tmp_path / "lsrk_one"
+    subprocess.run([cxx, "-std=c++17", "-O2", os.path.join(root, "tests", "cpp", "lsrk_one.cpp"), "-o", str(exe),
+                    "-I", os.path.join(root, "include"), "-I", os.path.join(cuda, "include"), "-L", lib, "-lmtb",
+                    "-L", os.path.join(cuda, "lib64"), "-lcudart", "-Wl,-rpath," + lib,
+                    "-Wl,-rpath," + os.path.join(cuda, "lib64")], check=True)
+    rng = np.random.default_rng(12)
+    t = np.repeat(MJD_2024_03_20 + 6.0 * np.arange(40), 9)
+    chan = np.array([1.31e9, 1.42e9, 1.49e9])
+    index = rng.permutation(t.size).astype(np.int32)
+    inp = tmp_path / "in.bin"
+    with open(inp, "wb") as f:
+        np.array([t.size, chan.size, index.size, 1], np.int32).tofile(f)
+        np.array(list(MEERKAT) + [0.7, -0.9, 69.184, 0.1], np.float64).tofile(f)
+        t.astype(np.float64).tofile(f)
+        chan.tofile(f)
+        index.tofile(f)
+    out = tmp_path / "out.bin"
+    subprocess.run([str(exe), str(inp), str(out)], check=True)
+    got = np.fromfile(out, np.float32).reshape(chan.size, index.size)
+    ref = O.lsrk_freq_over_c(t, chan, MEERKAT, 0.7, -0.9, 69.184, 0.1, index=index)
+    assert _ulps(got, ref).max() <= 1
