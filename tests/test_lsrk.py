@@ -64,6 +64,18 @@ def test_factor_is_a_doppler_shift_of_the_observer_velocity():
     assert np.isclose(O.doppler_factor(t, MEERKAT, ra + np.pi, -dec), np.sqrt((1 + beta) / (1 - beta)), rtol=1e-14)
 
 
+def test_time_scale_offsets():
+    """tt_minus_time and ut1_minus_time only move the epoch: shifting the
+    record time and both offsets against each other changes nothing; one
+    second of UT1 turns the site by 7.3e-5 rad, a few cm/s of its velocity."""
+    t = MJD_2024_03_20 + 1234.5
+    a = O.doppler_factor(t, MEERKAT, 1.0, 0.2, tt_minus_time=69.184, ut1_minus_time=0.3)
+    b = O.doppler_factor(t + 10.0, MEERKAT, 1.0, 0.2, tt_minus_time=59.184, ut1_minus_time=-9.7)
+    assert abs(a - b) < 1e-15
+    c = O.doppler_factor(t, MEERKAT, 1.0, 0.2, tt_minus_time=69.184, ut1_minus_time=1.3)
+    assert 1e-13 < abs(c - a) < 1e-9
+
+
 def test_oracle_evaluates_once_per_run_of_equal_times():
     t = np.repeat(MJD_2024_03_20 + 10.0 * np.arange(4), 3)
     out = O.lsrk_freq_over_c(t, [1.4e9], MEERKAT, 1.0, -0.5)
