@@ -357,6 +357,7 @@ def main():
     ap.add_argument("--channels", type=int, default=16)
     ap.add_argument("--hours", type=float, default=8.0)
     ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--e2e-slots", type=int, default=2, help="device buffer sets the e2e leg's channel copies rotate over")
     ap.add_argument("--streams", type=int, default=1, help="CUDA streams the channels of a step alternate over")
     ap.add_argument("--cpu-records", type=int, default=0, help="records for the CPU baseline sample")
     ap.add_argument("--ref-baselines", type=int, default=560)
@@ -701,7 +702,8 @@ def run_e2e(args, torch, dev, uvw_d, chans, imagers, images, samples_per_step, w
     # per channel: vis, flags (and weights when the channels do not share them)
     host = [[pinned(t) for t in ((v, fl) if shared_w else (v, w, fl))] for (f, v, w, fl) in chans]
     out_host = [torch.empty(im.shape, dtype=im.dtype, pin_memory=True) for im in images]
-    bufs = [[torch.empty(t.shape, dtype=t.dtype, device=dev) for t in host[0]] for _ in range(2)]
+    nslots = max(2, args.e2e_slots)
+    bufs = [[torch.empty(t.shape, dtype=t.dtype, device=dev) for t in host[0]] for _ in range(nslots)]
     uvw_bufs = [torch.empty_like(uvw_d) for _ in range(2)]
     w_bufs = [torch.empty_like(chans[0][2]) for _ in range(2)] if shared_w else None
     copy = torch.cuda.Stream(device=dev)
@@ -713,7 +715,7 @@ def run_e2e(args, torch, dev, uvw_d, chans, imagers, images, samples_per_step, w
     ref_image = images[-1].clone()          # the device path's image of the last channel
     # events: buffer pair free (last gridding that read it done), uvw buffer
     # free, image c read back
-    state = dict(seq=0, free=[None, None], uvw_free=[None, None], back=[None] * len(host), shared={})
+    state = dict(seq=0, free=[None] * nslots, uvw_free=[None, None], back=[None] * len(host), shared={})
 
     def record(stream):
         e = torch.cuda.Event()
@@ -754,7 +756,7 @@ def run_e2e(args, torch, dev, uvw_d, chans, imagers, images, samples_per_step, w
         comp.wait_event(state["shared"].pop(n))
         mscol["run"](tb, ib, nub)
         for c, hc in enumerate(host):
-            k = state["seq"] % 2
+            k = state["seq"] % nslots
             state["seq"] += 1
             b = bufs[k]
             with torch.cuda.stream(copy):
