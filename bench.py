@@ -356,7 +356,7 @@ def main():
     ap.add_argument("--config", default="mid", choices=["mid", "small", "serve", "cube"])
     ap.add_argument("--channels", type=int, default=16)
     ap.add_argument("--hours", type=float, default=8.0)
-    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--e2e-slots", type=int, default=2, help="device buffer sets the e2e leg's channel copies rotate over")
     ap.add_argument("--streams", type=int, default=1, help="CUDA streams the channels of a step alternate over")
     ap.add_argument("--cpu-records", type=int, default=0, help="records for the CPU baseline sample")
@@ -408,7 +408,7 @@ def main():
     import torch
     import torch.distributed as dist
     from mtb import _lib as L
-    from mtb.imager import WProjectionImager, build_wkernels, wkernel_params
+    from mtb.imager import WProjectionImager, build_wkernels, pack_flags, wkernel_params
 
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
@@ -462,13 +462,17 @@ def main():
     # (mtb_lsrk_freq_over_c), taken in the baseline-major record order
     # (record k = b * nt + t) -- once per step, on the device
     mscol = lsrk_inputs(torch, dev, spec, nbl, nt, freqs)
+    packed = []
     nu = torch.empty((len(freqs), R), dtype=torch.float32, device=dev)
     mscol["run"](mscol["time"], mscol["index"], nu)
     for c, f in enumerate(freqs):
         vis = make_vis(uvw, f, srcs, torch, gen)
-        # one byte per flag (mtb_grid_params.flags_u8): a quarter of the int32 layout's bytes to move
+        # one byte per flag (mtb_grid_params.flags_u8 = 1) for the checks and
+        # samples outside the timed region; the timed step and the e2e leg
+        # take the same flags packed one bit per flag (flags_u8 = 2)
         flags = (torch.rand(R, device=dev, generator=gen) < spec["flag"]).to(torch.uint8)[:, None].repeat(1, 4).contiguous()
         chans.append((nu[c], vis, weights, flags))
+        packed.append(pack_flags(flags))
     torch.cuda.synchronize()
     t_gen = time.perf_counter() - t_gen
 
@@ -505,7 +509,7 @@ def main():
         begin.record(main_stream)
         for st in streams[1:]:
             st.wait_event(begin)
-        for c, (im, (freq, vis, weights, flags)) in enumerate(zip(imagers, chans)):
+        for c, (im, (freq, vis, weights, _), flags) in enumerate(zip(imagers, chans, packed)):
             st = streams[c % len(streams)]
             with torch.cuda.stream(st):
                 if record_latency:
@@ -595,7 +599,8 @@ def main():
             dist.all_reduce(flag, op=dist.ReduceOp.MIN)
             fits = bool(flag.item())
         if fits:
-            e2e = run_e2e(args, torch, dev, uvw, chans, imagers, images, samples_per_step, world, dist, mscol)
+            e2e = run_e2e(args, torch, dev, uvw, chans, imagers, images, samples_per_step, world, dist, mscol,
+                          packed)
         else:
             e2e = {"value": None, "skipped": "pinned host copies of %d ranks (%.0f GB) exceed 60 %% of the host's "
                                           "available memory" % (local_ranks, pinned * local_ranks / 1e9)}
@@ -648,7 +653,7 @@ def main():
                        "image": n, "cell_arcsec": dl / ARCSEC, "wplanes": spec["wplanes"],
                        "sampling": spec["sampling"], "supports": [int(sup.min()), int(sup.max())],
                        "samples_per_step": samples_per_step, "l2": "inputs larger than L2 (1.6 GB per channel)",
-                       "flags": "uint8 [R][4] (flags_u8)", "streams": args.streams,
+                       "flags": "bit-packed, uint8 [R*4/8] (flags_u8 = 2)", "streams": args.streams,
                        "parallelism": "replicas" if world > 1 else "single GPU"},
             "images_per_s": len(freqs) * world / (ms_per_step * 1e-3),
             "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
@@ -676,7 +681,7 @@ def main():
         dist.destroy_process_group()
 
 
-def run_e2e(args, torch, dev, uvw_d, chans, imagers, images, samples_per_step, world, dist, mscol):
+def run_e2e(args, torch, dev, uvw_d, chans, imagers, images, samples_per_step, world, dist, mscol, packed):
     """Same metric through the public API from pinned host buffers: per step
     the H2D copy of every channel's records (and of the arrays the channels
     share: uvw, the weights, the TIME column and the record order) and the
@@ -699,8 +704,9 @@ def run_e2e(args, torch, dev, uvw_d, chans, imagers, images, samples_per_step, w
     time_bufs = [torch.empty_like(mscol["time"]) for _ in range(2)]
     index_bufs = [torch.empty_like(mscol["index"]) for _ in range(2)]
     nu_bufs = [torch.empty((len(chans), uvw_d.shape[1]), dtype=torch.float32, device=dev) for _ in range(2)]
-    # per channel: vis, flags (and weights when the channels do not share them)
-    host = [[pinned(t) for t in ((v, fl) if shared_w else (v, w, fl))] for (f, v, w, fl) in chans]
+    # per channel: vis, bit-packed flags (and weights when the channels do not share them)
+    host = [[pinned(t) for t in ((v, fl) if shared_w else (v, w, fl))]
+            for (f, v, w, _), fl in zip(chans, packed)]
     out_host = [torch.empty(im.shape, dtype=im.dtype, pin_memory=True) for im in images]
     nslots = max(2, args.e2e_slots)
     bufs = [[torch.empty(t.shape, dtype=t.dtype, device=dev) for t in host[0]] for _ in range(nslots)]
@@ -797,19 +803,23 @@ def run_e2e(args, torch, dev, uvw_d, chans, imagers, images, samples_per_step, w
     torch.cuda.synchronize()
     link_gbs = 3 * vis_h.numel() * vis_h.element_size() / (l0.elapsed_time(l1) * 1e-3) / 1e9
 
-    step(0, False)
+    # steady streaming: every step queues the next step's shared arrays behind
+    # its channel copies, so the timed region holds K sets of them (those of
+    # steps 2..K+1; step 1's came with the warm-up step), every copy ending
+    # inside it
+    step(0, True)
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     a.record()
-    # every timed step's shared arrays are copied inside the timed region:
-    # step 1 its own, steps 2..K by their predecessors
-    for n in range(1, args.e2e_steps + 1):
-        step(n, n < args.e2e_steps)
+    K = args.e2e_steps
+    for n in range(1, K + 1):
+        step(n, True)
     for e in state["back"]:
         comp.wait_event(e)
+    comp.wait_event(state["shared"].pop(K + 1))
     b.record()
     torch.cuda.synchronize()
     ms = max_over_ranks(a.elapsed_time(b) / args.e2e_steps, world, dist, torch, dev)

@@ -177,7 +177,10 @@ typedef struct mtb_grid_params {
                                   sets the normaliser to NaN                               */
     int flags_u8;              /* 0: d_flags is int32 [R][P] (the reference's layout); 1: it
                                   is one byte per flag, uint8 [R][P] (0 = keep, non-zero = flagged;
-                                  a quarter of the bytes to move), passed cast to int *    */
+                                  a quarter of the bytes to move); 2: one bit per flag, flag
+                                  i = r*P + p in bit i % 8 of byte i / 8 (ceil(R*P/8) bytes, 1 =
+                                  flagged; a thirty-second of the bytes); 1 and 2 passed cast
+                                  to int *; other values are refused                       */
     int no_grid_lo;            /* 0: the workspace holds the per-call delta grid compensated
                                   calls (d_grid_lo set) accumulate in: 8 bytes per cell and
                                   polarisation (FP32), 16 with exact_delta or with work

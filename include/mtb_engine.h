@@ -56,7 +56,8 @@ typedef struct mtb_image_request {
     long long uvw_row_stride;     /* floats between the u, v and w rows of uvw (a slice of
                                      a longer uvw array); 0: nrecords                      */
     int flags_u8;                 /* 1: flags is uint8 [R][P] (one byte per flag), passed
-                                     cast to int *; 0: int32 [R][P]                        */
+                                     cast to int *; 0: int32 [R][P]; other values (the
+                                     bit-packed flags mtb_grid takes) are refused          */
 } mtb_image_request;
 
 typedef struct mtb_image_result {

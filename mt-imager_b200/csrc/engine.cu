@@ -289,6 +289,7 @@ int check_request(const mtb_image_request *r) {
     if (r->nrecords > 0 && (!r->uvw || !r->freq || !r->vis || !r->weights || !r->flags)) return MTB_ERR_NULL;
     if (r->pol_type != MTB_POL_LINEAR && r->pol_type != MTB_POL_CIRCULAR) return MTB_ERR_BAD_PARAM;
     if (r->uvw_row_stride != 0 && r->uvw_row_stride < r->nrecords) return MTB_ERR_BAD_SHAPE;
+    if (r->flags_u8 != 0 && r->flags_u8 != 1) return MTB_ERR_BAD_PARAM;   // whole bytes: chunks start anywhere
     return MTB_OK;
 }
 

@@ -77,10 +77,22 @@ struct BucketTable {
 __device__ __forceinline__ int bucket_of(int S, int half) { return (S - 1) / (2 * half); }
 
 // ------------------------------------------------------------- preprocess --
-// F: flag element type, int (the reference's layout) or unsigned char
-template <int P, typename F>
+// Flag readers: flag i = r * P + p of the caller's array is set (flagged).
+// FlagArray: one int (the reference's layout) or one byte per flag;
+// FlagBits: one bit per flag, bit i % 8 of byte i / 8 (mtb_grid_params.flags_u8 = 2)
+template <typename F>
+struct FlagArray {
+    const F *f;
+    __device__ __forceinline__ bool operator()(size_t i) const { return __ldg(f + i) != 0; }
+};
+struct FlagBits {
+    const unsigned char *f;
+    __device__ __forceinline__ bool operator()(size_t i) const { return (__ldg(f + (i >> 3)) >> (i & 7)) & 1u; }
+};
+
+template <int P, typename FR>
 __global__ void k_preprocess(int R, const float *__restrict__ uvw, const float *__restrict__ freq,
-                             const float *__restrict__ weights, const F *__restrict__ flags,
+                             const float *__restrict__ weights, const FR flags,
                              const int *__restrict__ conv_info, const float *__restrict__ conv_sums,
                              int nw, double w_inc, int s, int T, int nx, int ny, double du, double dv,
                              int4 *__restrict__ pos, int *__restrict__ meta, double *__restrict__ norm_acc,
@@ -96,7 +108,7 @@ __global__ void k_preprocess(int R, const float *__restrict__ uvw, const float *
         for (int p = 0; p < P; p++) {
             // any non-zero flag is a flagged sample; the reference weights by
             // 1 - flag (WProjPreProcessUVW.cu:84-106), which agrees for 0 / 1
-            fl[p] = flags[(size_t)r * P + p] != 0 ? 1 : 0;
+            fl[p] = flags((size_t)r * P + p) ? 1 : 0;
             wt[p] = weights[(size_t)r * P + p];
             if (fl[p] == 0) grid = true;
         }
@@ -275,11 +287,11 @@ __device__ __forceinline__ int padded_index(int ci, int S, const int *__restrict
     return __ldg(&pbase[lo]) + sub * S * (S + 1);
 }
 
-template <int P, bool DIRECT, typename F>
+template <int P, bool DIRECT, typename FR>
 __global__ void k_gather(int R, const unsigned *__restrict__ skeys, const int *__restrict__ sidx,
                          const int4 *__restrict__ pos, const int *__restrict__ meta,
                          const float2 *__restrict__ vis, const float *__restrict__ weights,
-                         const F *__restrict__ flags, int4 *__restrict__ wpos, void *__restrict__ wvis,
+                         const FR flags, int4 *__restrict__ wpos, void *__restrict__ wvis,
                          BucketTable bt, int nx, const int *__restrict__ conv_info, const int *__restrict__ pbase,
                          int nw, int psf, int vpairs) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < R; i += gridDim.x * blockDim.x) {
@@ -296,7 +308,7 @@ __global__ void k_gather(int R, const unsigned *__restrict__ skeys, const int *_
             for (int p = 0; p < P; p++) {
                 const float2 v = psf ? make_float2(1.0f, 0.0f) : vis[(size_t)r * P + p];
                 float wgt = weights[(size_t)r * P + p];
-                float keep = flags[(size_t)r * P + p] != 0 ? 0.0f : 1.0f;
+                float keep = flags((size_t)r * P + p) ? 0.0f : 1.0f;
                 acc[p].x += v.x * wgt * keep;
                 acc[p].y += v.y * wgt * keep * im;
             }
@@ -1973,6 +1985,7 @@ static int check_params(const mtb_grid_params *p) {
     if (!(p->u_increment > 0.0) || !(p->v_increment > 0.0) || !(p->w_sq_increment > 0.0)) return MTB_ERR_BAD_PARAM;
     if (p->tile < 0 || p->support_bucket < 0 || p->max_chunk < 0) return MTB_ERR_BAD_PARAM;
     if (p->merge < 0 || p->merge > 2) return MTB_ERR_BAD_PARAM;
+    if (p->flags_u8 < 0 || p->flags_u8 > 2) return MTB_ERR_BAD_PARAM;
     if (p->bulk_min_support != 0) return MTB_ERR_BAD_PARAM;   // reserved (no bulk-copy gridder)
     if (p->gridder_threads != 0 && p->gridder_threads != 256 && p->gridder_threads != 512) return MTB_ERR_BAD_PARAM;
     if (p->gridder != 0 && p->gridder != 3 && p->gridder != 5 && !streaming(p->gridder)) return MTB_ERR_BAD_PARAM;
@@ -2069,35 +2082,58 @@ static bool check_gridder() {
     return v == 1;
 }
 
-// k_preprocess / k_gather with the caller's flag element type: int32 (the
-// reference's layout) or bytes (mtb_grid_params.flags_u8).
+// k_preprocess / k_gather with the caller's flag layout: int32 (the
+// reference's layout), bytes or bits (mtb_grid_params.flags_u8 = 0, 1, 2).
+template <int P, typename FR>
+static void launch_preprocess_fr(const mtb_grid_params *p, int blocks, cudaStream_t st, int R, const float *uvw,
+                                 const float *freq, const float *weights, FR flags, const int *conv_info,
+                                 const float *conv_sums, int T, int4 *pos, int *meta, double *norm_acc,
+                                 float *convsum_out) {
+    k_preprocess<P, FR><<<blocks, 256, 0, st>>>(R, uvw, freq, weights, flags, conv_info, conv_sums, p->wplanes,
+                                                p->w_sq_increment, p->sampling, T, p->nx, p->ny, p->u_increment,
+                                                p->v_increment, pos, meta, norm_acc, convsum_out);
+}
+
 template <int P>
 static void launch_preprocess(const mtb_grid_params *p, int blocks, cudaStream_t st, int R, const float *uvw,
                               const float *freq, const float *weights, const int *flags, const int *conv_info,
                               const float *conv_sums, int T, int4 *pos, int *meta, double *norm_acc,
                               float *convsum_out) {
-    if (p->flags_u8)
-        k_preprocess<P, unsigned char><<<blocks, 256, 0, st>>>(
-            R, uvw, freq, weights, (const unsigned char *)flags, conv_info, conv_sums, p->wplanes, p->w_sq_increment,
-            p->sampling, T, p->nx, p->ny, p->u_increment, p->v_increment, pos, meta, norm_acc, convsum_out);
+    const unsigned char *fb = (const unsigned char *)flags;
+    if (p->flags_u8 == 2)
+        launch_preprocess_fr<P>(p, blocks, st, R, uvw, freq, weights, FlagBits{fb}, conv_info, conv_sums, T, pos,
+                                meta, norm_acc, convsum_out);
+    else if (p->flags_u8)
+        launch_preprocess_fr<P>(p, blocks, st, R, uvw, freq, weights, FlagArray<unsigned char>{fb}, conv_info,
+                                conv_sums, T, pos, meta, norm_acc, convsum_out);
     else
-        k_preprocess<P, int><<<blocks, 256, 0, st>>>(R, uvw, freq, weights, flags, conv_info, conv_sums, p->wplanes,
-                                                     p->w_sq_increment, p->sampling, T, p->nx, p->ny, p->u_increment,
-                                                     p->v_increment, pos, meta, norm_acc, convsum_out);
+        launch_preprocess_fr<P>(p, blocks, st, R, uvw, freq, weights, FlagArray<int>{flags}, conv_info, conv_sums, T,
+                                pos, meta, norm_acc, convsum_out);
+}
+
+template <int P, bool DIRECT, typename FR>
+static void launch_gather_fr(const mtb_grid_params *p, int blocks, cudaStream_t st, int R, const GridSpace &s,
+                             const float2 *vis, const float *weights, FR flags, const GridPlan &plan,
+                             const int *conv_info, const int *pbase, int nw, bool pairs) {
+    k_gather<P, DIRECT, FR><<<blocks, 256, 0, st>>>(R, s.skeys, s.sidx, s.pos, s.meta, vis, weights, flags, s.wpos,
+                                                    s.wvis, plan.bt, p->nx, conv_info, pbase, nw, p->psf,
+                                                    pairs ? 1 : 0);
 }
 
 template <int P, bool DIRECT>
 static void launch_gather(const mtb_grid_params *p, int blocks, cudaStream_t st, int R, const GridSpace &s,
                           const float2 *vis, const float *weights, const int *flags, const GridPlan &plan,
                           const int *conv_info, const int *pbase, int nw, bool pairs = false) {
-    if (p->flags_u8)
-        k_gather<P, DIRECT, unsigned char><<<blocks, 256, 0, st>>>(
-            R, s.skeys, s.sidx, s.pos, s.meta, vis, weights, (const unsigned char *)flags, s.wpos, s.wvis, plan.bt,
-            p->nx, conv_info, pbase, nw, p->psf, pairs ? 1 : 0);
+    const unsigned char *fb = (const unsigned char *)flags;
+    if (p->flags_u8 == 2)
+        launch_gather_fr<P, DIRECT>(p, blocks, st, R, s, vis, weights, FlagBits{fb}, plan, conv_info, pbase, nw,
+                                    pairs);
+    else if (p->flags_u8)
+        launch_gather_fr<P, DIRECT>(p, blocks, st, R, s, vis, weights, FlagArray<unsigned char>{fb}, plan, conv_info,
+                                    pbase, nw, pairs);
     else
-        k_gather<P, DIRECT, int><<<blocks, 256, 0, st>>>(R, s.skeys, s.sidx, s.pos, s.meta, vis, weights, flags,
-                                                         s.wpos, s.wvis, plan.bt, p->nx, conv_info, pbase, nw, p->psf,
-                                                         pairs ? 1 : 0);
+        launch_gather_fr<P, DIRECT>(p, blocks, st, R, s, vis, weights, FlagArray<int>{flags}, plan, conv_info, pbase,
+                                    nw, pairs);
 }
 
 // Everything of one mtb_grid call before the gridder kernels: preprocessing,

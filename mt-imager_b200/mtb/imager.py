@@ -52,13 +52,32 @@ def _is_byte_flags(flags):
     return dt in (np.uint8, np.bool_, torch.uint8, torch.bool)
 
 
-def _flags_u8(flags):
-    """mtb_grid_params.flags_u8 for a device flag tensor (int32 or uint8)."""
+def _flags_u8(flags, R, P):
+    """mtb_grid_params.flags_u8 for a device flag tensor: int32 [R][P] -> 0,
+    uint8 [R][P] -> 1, uint8 [ceil(R*P/8)] bit-packed (pack_flags) -> 2."""
     if flags.dtype == torch.uint8:
+        if flags.dim() == 1 and flags.numel() == (R * P + 7) // 8 and flags.numel() != R * P:
+            return 2
+        if flags.numel() != R * P:
+            raise ValueError("uint8 flags must be [R][P] bytes or ceil(R*P/8) packed bytes")
         return 1
     if flags.dtype == torch.int32:
         return 0
     raise TypeError("flags must be int32 or uint8 on the device")
+
+
+def pack_flags(flags):
+    """One bit per flag (mtb_grid_params.flags_u8 = 2): flags [R][P] (any
+    dtype; non-zero = flagged) -> uint8 [ceil(R*P/8)], flag i = r*P + p in bit
+    i % 8 of byte i / 8.  A torch tensor stays on its device; numpy gives numpy."""
+    if isinstance(flags, torch.Tensor):
+        bits = (flags.reshape(-1) != 0).to(torch.uint8)
+        pad = (-bits.numel()) % 8
+        if pad:
+            bits = torch.cat([bits, bits.new_zeros(pad)])
+        w = torch.tensor([1, 2, 4, 8, 16, 32, 64, 128], dtype=torch.uint8, device=bits.device)
+        return (bits.view(-1, 8) * w).sum(dim=1, dtype=torch.uint8).contiguous()
+    return np.packbits(np.asarray(flags).reshape(-1) != 0, bitorder="little")
 
 
 @dataclasses.dataclass
@@ -245,7 +264,7 @@ class WProjectionImager:
         k = self.build_kernels()
         R = int(freq.numel())
         gp = self.grid_params(self._fresh)
-        gp.flags_u8 = _flags_u8(flags)
+        gp.flags_u8 = _flags_u8(flags, R, self.npol)
         ws, nbytes = self._workspace(R, gp)
         st = L.check(self.lib.mtb_grid(ctypes.byref(gp), _ptr(k.table), _ptr(k.d_conv_info),
                                        k.conv_info.ctypes.data_as(ctypes.c_void_p), _ptr(k.conv_sums),
@@ -292,7 +311,7 @@ def _batch_jobs(entries):
         k = im.build_kernels()
         gp = im.grid_params(im._fresh)
         J = jobs[j]
-        gp.flags_u8 = _flags_u8(flags)
+        gp.flags_u8 = _flags_u8(flags, int(freq.numel()), im.npol)
         J.params = gp
         J.d_table, J.d_conv_info = _ptr(k.table), _ptr(k.d_conv_info)
         J.h_conv_info = k.conv_info.ctypes.data_as(ctypes.c_void_p)

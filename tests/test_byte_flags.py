@@ -1,5 +1,6 @@
 """Flags given as one byte per flag (mtb_grid_params.flags_u8,
-mtb_image_request.flags_u8) grid exactly like the reference's int32 flags:
+mtb_image_request.flags_u8) or one bit per flag (flags_u8 = 2, mtb_grid and
+mtb_grid_batch) grid exactly like the reference's int32 flags:
 through mtb_grid, mtb_preprocess_uvw, mtb_grid_batch (the two formats mixed in
 one batch) and the request engine.  The preprocessing outputs are compared
 bit for bit; images to 1e-6 of the peak (with the FP64 per-call delta grid
@@ -114,6 +115,39 @@ def test_batch_mixes_flag_formats():
     grid_batch(entries)
     for (im, *_), img1 in zip(entries, single):
         assert same(im.finalize().cpu().numpy(), img1)
+
+
+def test_packed_bit_flags_equal_bytes():
+    """One bit per flag (flags_u8 = 2, mtb.imager.pack_flags) grids exactly
+    like one byte per flag, through mtb_grid on an odd record count (the last
+    byte half used) and through mtb_grid_batch beside byte flags."""
+    from mtb.imager import pack_flags
+    dev = torch.device("cuda")
+    t = lambda a, dt: torch.from_numpy(np.ascontiguousarray(a)).to(dev, dt)  # noqa: E731
+    obs, setup = case(seed=36)
+    R = obs.nrec - 1                                 # R * P / 8 not whole
+    args = (obs.uvw[:, :R], obs.freq_over_c(0)[:R], obs.vis[0][:R], obs.weights[0][:R])
+    fl = obs.flags[0][:R].astype(np.uint8)
+    ref = imager(setup)
+    ref.grid_chunk(*args, fl)
+    a = ref.finalize().cpu().numpy()
+    im = imager(setup)
+    bits = pack_flags(t(fl, torch.uint8))
+    assert bits.numel() == (R * 4 + 7) // 8
+    im.grid_device(t(args[0], torch.float32), t(args[1], torch.float32), t(args[2], torch.complex64),
+                   t(args[3], torch.float32), bits)
+    assert im.statistics() == ref.statistics()
+    assert same(im.finalize().cpu().numpy(), a)
+    cs = [case(seed=37), case(seed=38, nx=96)]
+    single = [image(o, st, o.flags[0])[0] for o, st in cs]
+    entries = []
+    for i, (o, st) in enumerate(cs):
+        f = t(o.flags[0], torch.uint8)
+        entries.append((imager(st), t(o.uvw, torch.float32), t(o.freq_over_c(0), torch.float32),
+                        t(o.vis[0], torch.complex64), t(o.weights[0], torch.float32), pack_flags(f) if i else f))
+    grid_batch(entries)
+    for (im2, *_), img1 in zip(entries, single):
+        assert same(im2.finalize().cpu().numpy(), img1)
 
 
 def test_engine_byte_flags_equal_int32():
