@@ -5,9 +5,11 @@ The oracle (oracle/lsrk_oracle.py) is held to known answers on the CPU: the
 J2000 direction of the standard solar motion (18h03m50.2s +30d00m16.8s),
 the Earth's barycentric velocity at J2000.0 as the JPL DE405 ephemeris gives
 it (-0.017202, -0.002904, -0.001259 au/day), the annual range of the Earth's
-speed (29.29-30.29 km/s) and the diurnal speed of a site on the equator
-(465.1 m/s).  casacore's own conversion cannot run here, so parity with the
-reference is unpinned beyond these answers.  The GPU tests compare the
+speed (29.29-30.29 km/s), the diurnal speed of a site on the equator
+(465.1 m/s), and the Earth's velocity from the Astronomical Almanac's
+low-precision Sun formula, a second published method.  casacore's own
+conversion cannot run here, so parity with the reference is unpinned beyond
+these answers.  The GPU tests compare the
 device path with the oracle: nu/c in float32 equal to the oracle's or one
 unit in the last place away (FP64 sin/cos of the two libraries differ in
 their last bits, which moves a rounding only next to a tie)."""
@@ -41,6 +43,31 @@ def test_apex_of_solar_motion_in_j2000():
 def test_earth_velocity_at_j2000_matches_de405():
     v = O.earth_velocity(O.J2000) / O.AU * O.DAY      # au/day
     assert np.allclose(v, [-0.017202, -0.002904, -0.001259], atol=1e-5)   # 17 m/s
+
+
+def test_earth_velocity_agrees_with_the_almanac_sun():
+    """A second, independent published formula: the Astronomical Almanac's
+    low-precision geocentric Sun (mean longitude and anomaly, two-term
+    equation of centre, of-date equator), differentiated and precessed to
+    J2000, gives the Earth's velocity within 40 m/s and 0.08 deg of the
+    oracle's over 30 years; it leaves out the Earth's monthly motion about the
+    Earth-Moon barycentre and the Sun's motion about the barycentre (each up
+    to ~13 m/s), which the oracle carries."""
+    def sun(jd):
+        n = jd - 2451545.0
+        g = np.radians(357.528 + 0.9856003 * n)
+        lam = np.radians(280.460 + 0.9856474 * n + 1.915 * np.sin(g) + 0.020 * np.sin(2 * g))
+        r = 1.00014 - 0.01671 * np.cos(g) - 0.00014 * np.cos(2 * g)
+        eps = np.radians(23.439 - 0.0000004 * n)
+        return np.array([r * np.cos(lam), r * np.cos(eps) * np.sin(lam), r * np.sin(eps) * np.sin(lam)])
+    for d in np.arange(0.0, 30 * 365.25, 41.7):
+        jd = O.J2000 + d
+        v1 = O.earth_velocity(jd)
+        v2 = -(sun(jd + 0.01) - sun(jd - 0.01)) / 0.02 * O.AU / O.DAY
+        v2 = O.precession_matrix(O.J2000, jd).T @ v2
+        assert abs(np.linalg.norm(v1) - np.linalg.norm(v2)) < 40.0
+        cosang = v1 @ v2 / (np.linalg.norm(v1) * np.linalg.norm(v2))
+        assert np.degrees(np.arccos(min(1.0, cosang))) < 0.08
 
 
 def test_earth_speed_annual_range():
